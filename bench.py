@@ -1,0 +1,419 @@
+"""Benchmark of the B200 BR values-only tridiagonal eigensolver.
+
+python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Headline workload: one plain values-only solve of order N = 65,536, FP64,
+uniform family (D, E iid U(0,1), seeded), the configuration whose GPU time
+the reference publishes (60.5 ms on H100-PCIe).  A step is one solve with D
+and E already resident in HBM; L2 is flushed (256 MiB write) before every
+timed solve, outside the timed interval, and each solve is timed with CUDA
+events on its stream.  value = mean ms per solve (lower is better).
+
+Also reported on the same line: the e2e time through the C ABI with pinned
+host buffers (H2D of D and E, solve, D2H of W inside the timed interval),
+the per-phase roofline of the dominant kernel (FP64 pipe or HBM), the other
+three families at the same order, accuracy against the oracle, workspace
+bytes, clocks sampled during the timed loop, and the CPU baseline: the
+oracle (C restatement of the reference's DSTEDC_DC_BR, OpenMP on all host
+threads) timed on a bounded sample of the same workload.
+
+--impl reference times the reference's CPU implementation of this path
+(the oracle port; no Fortran compiler exists in the image) on the same
+workload and prints the same metric with "impl": "reference".
+
+With --gpus N > 1 (torchrun, one process per GPU) every rank solves its own
+replica (a single solve does not shard: the tree funnels into one root
+merge); value is the max over ranks of the per-solve time and
+solves_per_s is the whole-job rate.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "ppopp27-brdc-ae_b200"))
+
+METRIC = "ms/solve N=65,536 FP64 (fwd; fwd+bwd) and batched solves/s, vs plain & CPU"
+N_HEAD = 65536
+FAMILY_HEAD = "uniform"
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        try:
+            with open(path) as f:
+                p = json.load(f)
+            return float(p["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+def start_clock_sampler(path):
+    try:
+        return subprocess.Popen(
+            ["nvidia-smi",
+             "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+             "--format=csv,noheader,nounits", "-lms", "200"],
+            stdout=open(path, "w"), stderr=subprocess.DEVNULL)
+    except Exception:
+        return None
+
+
+def stop_clock_sampler(proc, path, device_index):
+    if proc is None:
+        return None
+    proc.terminate()
+    try:
+        proc.wait(timeout=5)
+    except Exception:
+        proc.kill()
+    sm, smax, reasons = [], 0.0, set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    try:
+        for line in open(path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9 or parts[0] != str(device_index):
+                continue
+            sm.append(float(parts[1]))
+            smax = max(smax, float(parts[2]))
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() in ("active", "1", "yes"):
+                    reasons.add(nm)
+    except Exception:
+        return None
+    if not sm:
+        return None
+    return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": smax, "reasons": sorted(reasons),
+            "samples": len(sm)}
+
+
+def time_solves(torch, solver, D, E, W, ws, steps, flush):
+    """Per-solve device times (ms) with an L2 flush before each solve."""
+    stream = torch.cuda.current_stream()
+    times = []
+    for _ in range(steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        solver.dstebr(D, E, W=W, workspace=ws)
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    return times
+
+
+def cpu_reference_times(d, e, budget_s, min_solves=1, max_solves=50):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    oracle.set_threads(os.cpu_count() or 1)
+    threads = oracle.max_threads()
+    oracle.dstedc_dc_br(d, e)  # warm-up
+    times = []
+    t_end = time.perf_counter() + budget_s
+    while len(times) < max_solves and (len(times) < min_solves or time.perf_counter() < t_end):
+        t0 = time.perf_counter()
+        oracle.dstedc_dc_br(d, e)
+        times.append((time.perf_counter() - t0) * 1e3)
+    return times, threads
+
+
+def run_reference_arm(args, rank):
+    from brdc import families
+
+    if rank != 0:
+        return
+    d, e = families.generate(FAMILY_HEAD, N_HEAD)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    oracle.set_threads(os.cpu_count() or 1)
+    threads = oracle.max_threads()
+    for _ in range(args.warmup):
+        oracle.dstedc_dc_br(d, e)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        oracle.dstedc_dc_br(d, e)
+        times.append((time.perf_counter() - t0) * 1e3)
+    v = float(np.mean(times))
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": v,
+        "unit": "ms",
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": v,
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded uniform U(0,1) family)",
+        "config": {"workload": f"plain values-only BR solve, {FAMILY_HEAD} family, N={N_HEAD}",
+                   "n": N_HEAD, "family": FAMILY_HEAD},
+        "cpu_baseline": {"value": v, "unit": "ms", "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} full solves of the headline input"},
+        "e2e": {"value": v, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "reference CPU path DSTEDC_DC_BR restated in C (oracle/brdc_oracle.c); "
+                "no Fortran compiler in the image",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-extras", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=12.0)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference_arm(args, rank)
+        return
+
+    import torch
+
+    import brdc
+    from brdc import families
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist_mod
+
+        dist = dist_mod
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    solver = brdc.Solver()
+    d, e = families.generate(FAMILY_HEAD, N_HEAD, instance=rank)
+    D = torch.tensor(d, device="cuda")
+    E = torch.tensor(e, device="cuda")
+    W = torch.empty(N_HEAD, dtype=torch.float64, device="cuda")
+    ws = solver.workspace(N_HEAD)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+
+    for _ in range(args.warmup):
+        solver.dstebr(D, E, W=W, workspace=ws)
+    torch.cuda.synchronize()
+    info = solver.info(N_HEAD, ws)
+
+    clocks_path = os.path.join("/tmp", f"brdc_clocks_{os.getpid()}.csv")
+    sampler = start_clock_sampler(clocks_path) if rank == 0 else None
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    times = time_solves(torch, solver, D, E, W, ws, args.steps, flush)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    clocks = stop_clock_sampler(sampler, clocks_path, local_rank) if rank == 0 else None
+    ms = float(np.mean(times))
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+
+    extras = {}
+    if rank == 0 and not args.no_extras:
+        extras = collect_extras(torch, brdc, families, solver, D, E, W, ws, d, e, flush, args)
+
+    if rank == 0:
+        diag = solver.diagnostics(N_HEAD, ws)
+        line = {
+            "metric": METRIC,
+            "value": ms,
+            "unit": "ms",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms,
+            "higher_is_better": False,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64",
+            "data": "synthetic (seeded uniform U(0,1) family, numpy PCG64 [1, N, rank])",
+            "config": {
+                "workload": f"plain values-only BR solve, {FAMILY_HEAD} family, N={N_HEAD}",
+                "n": N_HEAD, "family": FAMILY_HEAD,
+                "l2": "flushed by a 256 MiB write before every timed solve (outside the timed interval)",
+                "parallelism": f"replicas x{world}",
+            },
+            "solves_per_s": world * 1000.0 / ms,
+            "info": info,
+            "gpu_launches": extras.get("launches"),
+            "ms_min": float(np.min(times)),
+            "ms_median": float(np.median(times)),
+            "workspace_bytes": ws.numel(),
+            "deflation_K_per_level": [lv["dd_after_sum"] for lv in diag["level"]],
+            "clocks": clocks,
+        }
+        line.update({k: v for k, v in extras.items() if k != "launches"})
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def collect_extras(torch, brdc, families, solver, D, E, W, ws, d, e, flush, args):
+    out = {}
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    # accuracy of the headline solve
+    solver.dstebr(D, E, W=W, workspace=ws)
+    w = W.cpu().numpy()
+    ref = oracle.dstedc_dc_br(d, e)
+    out["max_err_vs_oracle"] = float(np.max(np.abs(w - ref)) / np.max(np.abs(ref)))
+
+    # per-phase timings and roofline of the dominant kernel
+    solver.set_timing(True)
+    acc = None
+    reps = 5
+    for _ in range(reps):
+        flush.zero_()
+        solver.dstebr(D, E, W=W, workspace=ws)
+        t = solver.last_timings()
+        if acc is None:
+            acc = {k: 0.0 for k in ("leaf_ms", "merge_ms", "secular_ms", "lowner_ms", "rows_ms", "total_ms")}
+        for k in acc:
+            acc[k] += t[k] / reps
+        launches = t["launches"]
+    solver.set_timing(False)
+    out["launches"] = launches
+    out["phase_ms"] = acc
+    diag = solver.diagnostics(N_HEAD, ws)
+    out["roofline"] = roofline(diag, acc, N_HEAD)
+
+    # other families at the same order
+    fam_ms = {}
+    for fam in ("normal", "toeplitz", "clustered"):
+        dd, ee = families.generate(fam, N_HEAD)
+        Df = torch.tensor(dd, device="cuda")
+        Ef = torch.tensor(ee, device="cuda")
+        solver.dstebr(Df, Ef, W=W, workspace=ws)
+        torch.cuda.synchronize()
+        tt = time_solves(torch, solver, Df, Ef, W, ws, 3, flush)
+        fam_ms[fam] = float(np.mean(tt))
+        if fam == "toeplitz":
+            err = np.max(np.abs(W.cpu().numpy() - families.toeplitz_eigenvalues(N_HEAD))) / 4.0
+            out["toeplitz_max_err_vs_closed_form"] = float(err)
+            dg = solver.diagnostics(N_HEAD, ws)
+            out["toeplitz_roofline"] = roofline(dg, None, N_HEAD, total_ms=fam_ms[fam])
+    out["family_ms"] = fam_ms
+
+    # e2e through the C ABI with pinned host buffers
+    hD = torch.tensor(d).pin_memory()
+    hE = torch.tensor(e).pin_memory()
+    hW = torch.empty(N_HEAD, dtype=torch.float64).pin_memory()
+    stream = torch.cuda.current_stream()
+    e2e = []
+    for i in range(args.warmup + args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        D.copy_(hD, non_blocking=True)
+        E.copy_(hE, non_blocking=True)
+        solver.dstebr(D, E, W=W, workspace=ws)
+        hW.copy_(W, non_blocking=True)
+        e1.record(stream)
+        e1.synchronize()
+        if i >= args.warmup:
+            e2e.append(e0.elapsed_time(e1))
+    out["e2e"] = {"value": float(np.mean(e2e)), "unit": "ms",
+                  "h2d_bytes_per_step": int(hD.numel() * 8 + hE.numel() * 8),
+                  "d2h_bytes_per_step": int(hW.numel() * 8)}
+
+    # CPU baseline: the oracle on a bounded sample of the same workload
+    cpu_t, threads = cpu_reference_times(d, e, args.cpu_budget)
+    out["cpu_baseline"] = {"value": float(np.median(cpu_t)), "unit": "ms", "cores": threads,
+                           "kind": "port",
+                           "sample": f"{len(cpu_t)} full solves of the headline input "
+                                     f"(oracle restatement of DSTEDC_DC_BR, OpenMP)"}
+    return out
+
+
+def roofline(diag, phase, n, total_ms=None):
+    """Roofline of the dominant phase.  FP64 phases count, per pole-root
+    pair: secular 32 flops (4 nominal sweeps x 8), Loewner 3, rows 9; the
+    merge phase moves 68 bytes per row per level."""
+    hbm, hbm_kind = measured_peaks()
+    levels = diag["level"]
+    k2 = sum(lv["dd_after_sq_sum"] for lv in levels)
+    k2_inner = sum(lv["dd_after_sq_sum"] for lv in levels[:-1])
+    fp64_peak = fp64_peak_gflops()
+    res = {"pairs_sum_k2": int(k2)}
+    if phase is None:
+        flops = 32.0 * k2 + 12.0 * k2_inner
+        ach = flops / (total_ms * 1e-3) / 1e12
+        res.update({"bound": "fp64", "kernel": "whole solve", "achieved": ach,
+                    "peak": fp64_peak / 1e3, "unit": "TFLOP/s", "frac": ach / (fp64_peak / 1e3),
+                    "traffic": None, "peak_kind": "measured (DFMA probe)"})
+        return res
+    cand = {
+        "secular": (phase["secular_ms"], 32.0 * k2, "fp64"),
+        "lowner": (phase["lowner_ms"], 3.0 * k2_inner, "fp64"),
+        "rows": (phase["rows_ms"], 9.0 * k2_inner, "fp64"),
+        "merge_deflate": (phase["merge_ms"], 68.0 * n * len(levels), "hbm"),
+        "leaf": (phase["leaf_ms"], 24.0 * n, "hbm"),
+    }
+    name = max(cand, key=lambda k: cand[k][0])
+    ms, work, bound = cand[name]
+    if bound == "fp64":
+        ach = work / (ms * 1e-3) / 1e12
+        res.update({"bound": "fp64", "kernel": name, "achieved": ach, "peak": fp64_peak / 1e3,
+                    "unit": "TFLOP/s", "frac": ach / (fp64_peak / 1e3), "traffic": None,
+                    "peak_kind": "measured (DFMA probe)"})
+    else:
+        ach = work / (ms * 1e-3) / 1e9
+        res.update({"bound": "hbm", "kernel": name, "achieved": ach, "peak": hbm,
+                    "unit": "GB/s", "frac": ach / hbm, "traffic": None,
+                    "peak_kind": hbm_kind + " copy bandwidth"})
+    res["phase_share"] = {k: v[0] / max(sum(c[0] for c in cand.values()), 1e-9) for k, v in cand.items()}
+    return res
+
+
+_FP64 = None
+
+
+def fp64_peak_gflops():
+    global _FP64
+    if _FP64 is None:
+        import ctypes
+
+        lib = ctypes.CDLL(os.path.join(ROOT, "ppopp27-brdc-ae_b200", "brdc", "libbrdc_probe.so"))
+        lib.brdc_probe_dfma_gflops.restype = ctypes.c_double
+        lib.brdc_probe_dfma_gflops.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        best = 0.0
+        for _ in range(3):
+            best = max(best, lib.brdc_probe_dfma_gflops(148 * 8, 256, 20000))
+        _FP64 = best
+    return _FP64
+
+
+if __name__ == "__main__":
+    main()

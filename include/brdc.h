@@ -1,0 +1,210 @@
+/*
+ * brdc.h -- C ABI of the B200 boundary-row (BR) values-only
+ * divide-and-conquer symmetric tridiagonal eigensolver.
+ *
+ * Every entry point replaces one interface of the reference artifact
+ * (Ruinique/PPoPP27-BRDC-AE); the citation beside each declaration names
+ * the reference file:line it stands in for.  Plain C types only: device
+ * pointers are passed as typed pointers, sizes as int64_t/size_t, the CUDA
+ * stream as an opaque pointer that is ABI-identical to cudaStream_t.
+ *
+ * Conventions shared by all device entry points
+ *  - The caller owns D, E, W and the workspace (device memory).  D and E
+ *    are read only.  No entry point on the solve path allocates memory.
+ *  - Work is enqueued on the handle's stream and returns without a host
+ *    synchronisation, so a solve can be captured in a CUDA graph.
+ *    brdc_get_info() / brdc_get_diagnostics() synchronise the stream.
+ *  - A handle is not thread safe (it records the last error); use one
+ *    handle per host thread.
+ */
+#ifndef BRDC_H
+#define BRDC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  Values 0-8 mirror evd_status
+ * (gpu/include/evd/status.h:8-18) one for one; NOT_CONVERGED is new: the
+ * reference records a secular non-convergence only in a debug array and
+ * still returns success (gpu/src/tridiag_solver.cu:2351-2370). */
+typedef enum brdc_status {
+    BRDC_STATUS_SUCCESS = 0,
+    BRDC_STATUS_INVALID_HANDLE = 1,
+    BRDC_STATUS_INVALID_POINTER = 2,
+    BRDC_STATUS_INVALID_VALUE = 3,
+    BRDC_STATUS_INVALID_WORKSPACE = 4,
+    BRDC_STATUS_ALLOC_FAILED = 5,
+    BRDC_STATUS_CUDA_ERROR = 6,
+    BRDC_STATUS_INTERNAL_ERROR = 7,
+    BRDC_STATUS_NOT_IMPLEMENTED = 8,
+    BRDC_STATUS_NOT_CONVERGED = 9
+} brdc_status;
+
+/* Error source of the last failure (gpu/include/evd/types.h:24-29). */
+typedef enum brdc_error_source {
+    BRDC_ERROR_SRC_NONE = 0,
+    BRDC_ERROR_SRC_CUDA = 1,
+    BRDC_ERROR_SRC_DEVICE = 2 /* a status word written by a kernel */
+} brdc_error_source;
+
+typedef struct CUstream_st *brdc_stream_t; /* == cudaStream_t */
+typedef struct brdc_handle_struct *brdc_handle;
+
+/* Handle life cycle: replaces evd_create_handle / evd_destroy_handle
+ * (gpu/include/evd/handle.h:13-14, gpu/src/handle.cu:76-150).  Like the
+ * reference, a new handle owns a non-blocking stream (handle.cu:95). */
+brdc_status brdc_create(brdc_handle *handle);
+brdc_status brdc_destroy(brdc_handle handle);
+
+/* Run on a caller-owned stream instead (NULL restores the handle's own
+ * stream).  No reference counterpart: the reference always uses its own. */
+brdc_status brdc_set_stream(brdc_handle handle, brdc_stream_t stream);
+brdc_status brdc_get_stream(brdc_handle handle, brdc_stream_t *stream);
+
+/* Last error (code, source, call site): replaces evd_get_last_error
+ * (gpu/include/evd/handle.h:15, gpu/src/handle.cu:152-168). */
+brdc_status brdc_get_last_error(brdc_handle handle, int *code,
+                                brdc_error_source *source, const char **site);
+
+/* Status names: replaces evd_status_to_string (gpu/src/handle.cu:198-221). */
+const char *brdc_status_to_string(brdc_status status);
+
+/* Workspace query for one solve of order n: replaces
+ * evd::internal::tridiag_solver_workspace_size
+ * (gpu/src/syev2stage_pipeline.hpp:70-71, gpu/src/tridiag_solver.cu:2373).
+ * flags: 0, or BRDC_FLAG_KEEP_CHECKPOINTS to reserve the per-level records
+ * that brdc_dstebr_backward() reads.  Bytes are O(n) (every slot 256-byte
+ * aligned, gpu/src/workspace_align.hpp:9); the reference reserves an
+ * n x min(n,4096) delta slab on top (gpu/src/tridiag_solver_dc.cuh:183-199).
+ * n <= 0 -> BRDC_STATUS_INVALID_VALUE (tridiag_solver_dc.cuh:284-286). */
+#define BRDC_FLAG_KEEP_CHECKPOINTS 1
+brdc_status brdc_dstebr_workspace_size(int64_t n, int flags, size_t *bytes);
+
+/* Values-only BR solve: D[n], E[n-1] (device, read only) -> W[n] ascending
+ * (device).  Replaces evd::internal::tridiag_solver_run_from_device_tridiagonal
+ * (gpu/src/syev2stage_pipeline.hpp:74-77, gpu/src/tridiag_solver.cu:2541-2583)
+ * with the same argument meaning and checks: NULL handle ->
+ * INVALID_HANDLE; NULL D or W, or NULL E with n > 1 -> INVALID_POINTER;
+ * n <= 0 -> INVALID_VALUE; workspace smaller than the query or NULL ->
+ * INVALID_WORKSPACE; CUDA launch failure -> CUDA_ERROR with the last error
+ * recorded.  The sign of E is ignored (|E| is used, tridiag_solver.cu:1308).
+ * The call is asynchronous: a secular iteration that fails to converge is
+ * reported by brdc_get_info(). */
+brdc_status brdc_dstebr(brdc_handle handle, int64_t n, const double *d_D,
+                        const double *d_E, double *d_W, void *workspace,
+                        size_t workspace_size);
+
+/* Adjoint of brdc_dstebr for the loss L = sum_i G[i] * W[i]: writes
+ * dL/dD[n] and dL/dE[n-1] (device) without forming eigenvectors, by
+ * running back through the merge tree.  The workspace must come from a
+ * brdc_dstebr() call with the same n, D, E made with a workspace sized for
+ * BRDC_FLAG_KEEP_CHECKPOINTS (the call re-runs the forward solve itself
+ * when keep_forward is 0).  No reference counterpart (values-only
+ * reference has no derivative). */
+brdc_status brdc_dstebr_backward(brdc_handle handle, int64_t n,
+                                 const double *d_D, const double *d_E,
+                                 const double *d_G, double *d_gD,
+                                 double *d_gE, void *workspace,
+                                 size_t workspace_size, int keep_forward);
+
+/* Device status of the last solve on this workspace; synchronises the
+ * stream.  *info = 0 on success, > 0 = number of secular roots that did
+ * not converge, < 0 = internal device error code.  Returns
+ * BRDC_STATUS_NOT_CONVERGED when *info > 0. */
+brdc_status brdc_get_info(brdc_handle handle, const void *workspace,
+                          int *info);
+
+/* Per-level deflation and iteration counters of the last solve on this
+ * workspace (synchronises).  Mirrors the values-only fields of the
+ * reference's TridiagMergeLevelDiagnostics (gpu/src/handle_impl.hpp:16-77)
+ * which are compared level by level with the reference prototype. */
+typedef struct brdc_level_diagnostics {
+    int level;               /* 0 = merges of leaves */
+    int merge_count;         /* merges at this level */
+    int size_sum;            /* sum of merged node sizes (= n) */
+    int dd_before_sum;       /* active poles after the small-z test */
+    int dd_after_sum;        /* K: poles left after close-pole deflation */
+    int dd_after_max;        /* largest K of one merge */
+    int zero_deflated_total; /* size_sum - dd_before_sum */
+    int close_deflated_total;/* dd_before_sum - dd_after_sum */
+    int secular_iter_sum;    /* secular iterations summed over roots */
+    int secular_iter_max;
+    int secular_iter_failed; /* roots that hit the iteration cap */
+    int threads_per_root;    /* lanes that shared one root's sums */
+    long long dd_after_sq_sum; /* sum of K^2: pole-root pairs of the level */
+} brdc_level_diagnostics;
+
+#define BRDC_MAX_LEVELS 40
+typedef struct brdc_diagnostics {
+    int n;
+    int levels;
+    int leaf_count;
+    int leaf_sweeps_max;     /* Jacobi sweeps of the slowest leaf */
+    brdc_level_diagnostics level[BRDC_MAX_LEVELS];
+} brdc_diagnostics;
+
+brdc_status brdc_get_diagnostics(brdc_handle handle, const void *workspace,
+                                 brdc_diagnostics *out);
+
+/* Per-phase device timings of the last solve enqueued with timing on,
+ * measured with CUDA events on the handle's stream between the kernels.
+ * Replaces evd_get_last_stage_timings (gpu/include/evd/evd.h:27-29,
+ * gpu/src/handle.cu:170-196) and the per-level slot timers of the
+ * reference's diagnostics (gpu/src/tridiag_solver.cu:158-359).  Timing adds
+ * one event record per kernel; leave it off for headline measurements.
+ * brdc_get_last_timings synchronises the stream. */
+typedef struct brdc_timings {
+    float total_ms;
+    float init_ms;
+    float leaf_ms;
+    float merge_ms;      /* merge + deflation, all levels */
+    float secular_ms;    /* secular roots, all levels */
+    float lowner_ms;     /* Loewner z, all levels */
+    float rows_ms;       /* boundary rows + placement, all levels */
+    int launches;        /* kernels enqueued by the solve */
+    int levels;
+    float level_ms[BRDC_MAX_LEVELS][4]; /* merge, secular, lowner, rows */
+} brdc_timings;
+
+brdc_status brdc_set_timing(brdc_handle handle, int enable);
+brdc_status brdc_get_last_timings(brdc_handle handle, brdc_timings *out);
+
+/* LAPACK-style host entry with the argument list and workspace-query
+ * semantics of DSTEDC_DC_BR (cpu/src/dstedc_dc_br.f:7-75): LWORK = -1 or
+ * LIWORK = -1 returns LWMIN = max(1,(16+2*NTHR)*N) in WORK(1) and
+ * LIWMIN = max(1,7*N) in IWORK(1) (NTHR as BRDC_WPROD_NTHREADS,
+ * dstedc_dc_br.f:153-213); INFO = -1/-5/-7 for a bad N/LWORK/LIWORK.  The
+ * solve itself runs on the GPU (host D, E copied in, D overwritten by the
+ * ascending eigenvalues, E destroyed); INFO > 0 if a root did not converge.
+ * Fortran calling convention (all arguments by reference). */
+void brdc_dstedc_dc_br_(const int *n, double *d, double *e, double *work,
+                        const int *lwork, int *iwork, const int *liwork,
+                        int *info);
+
+/* Batched solve of `count` independent tridiagonals of uneven order packed
+ * back to back: instance b has order n_b = offsets[b+1]-offsets[b] and
+ * occupies D[offsets[b] .. offsets[b+1]), E[offsets[b] .. offsets[b+1]-1)
+ * (the E slot at offsets[b+1]-1 is ignored), W likewise.  offsets is a host
+ * array of count+1 int64 values (offsets[0] = 0).  All levels of all
+ * instances run in one pass of kernels per level.  No reference
+ * counterpart (the reference solves one matrix per call). */
+brdc_status brdc_dstebr_batched_workspace_size(int64_t count,
+                                               const int64_t *offsets,
+                                               size_t *bytes);
+brdc_status brdc_dstebr_batched(brdc_handle handle, int64_t count,
+                                const int64_t *offsets, const double *d_D,
+                                const double *d_E, double *d_W,
+                                void *workspace, size_t workspace_size);
+
+/* Library version string. */
+const char *brdc_version(void);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* BRDC_H */

@@ -1,0 +1,71 @@
+"""Build the sm_100a solver library in-tree.
+
+``python build.py`` (or ``brdc.build.build()``) compiles
+``csrc/brdc_capi.cu`` with nvcc into ``brdc/libbrdc_b200.so`` and the host
+copy of the secular state machine into ``brdc/libbrdc_hostcheck.so`` (used by
+the CPU tests only).  nvcc cross-compiles without a GPU.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+OUT = os.path.join(HERE, "brdc")
+LIB = os.path.join(OUT, "libbrdc_b200.so")
+HOSTLIB = os.path.join(OUT, "libbrdc_hostcheck.so")
+PROBELIB = os.path.join(OUT, "libbrdc_probe.so")
+
+NVCC_FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-O3", "-lineinfo", "-std=c++17",
+    "-Xcompiler", "-fPIC", "-shared",
+]
+
+
+def _nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _sources():
+    return [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC))]
+
+
+def _stale(target: str, deps) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    deps = _sources() + [os.path.join(HERE, "..", "include", "brdc.h"), __file__]
+    deps = [d for d in deps if not d.endswith(("probe_fp64.cu", "host_check.cpp"))]
+    if force or _stale(LIB, deps):
+        cmd = [_nvcc(), *NVCC_FLAGS, "-o", LIB, os.path.join(CSRC, "brdc_capi.cu")]
+        if verbose:
+            cmd.insert(1, "-Xptxas=-v")
+        subprocess.run(cmd, check=True)
+    pdeps = [os.path.join(CSRC, "probe_fp64.cu")]
+    if force or _stale(PROBELIB, pdeps):
+        subprocess.run([_nvcc(), *NVCC_FLAGS, "-o", PROBELIB, pdeps[0]], check=True)
+    hdeps = [os.path.join(CSRC, "host_check.cpp"), os.path.join(CSRC, "brdc_secular.cuh")]
+    if force or _stale(HOSTLIB, hdeps):
+        cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
+        subprocess.run(
+            [cxx, "-O2", "-fPIC", "-shared", "-std=c++17", "-o", HOSTLIB,
+             os.path.join(CSRC, "host_check.cpp")],
+            check=True,
+        )
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose="-v" in sys.argv)
+    print(LIB)

@@ -1,0 +1,811 @@
+// brdc_capi.cu -- host driver and C ABI (include/brdc.h).
+//
+// The driver plans a forest (one or many tridiagonals), carves the caller's
+// workspace, and enqueues per level: k_merge_deflate, k_secular, k_lowner,
+// k_rows_place.  All launch shapes depend only on the orders, never on data,
+// and no call synchronises the stream, so a solve can be captured in a CUDA
+// graph.  Data-dependent sizes (deflation counts K) travel from kernel to
+// kernel through the workspace header; that replaces the per-level device
+// to host copy of the reference (gpu/src/tridiag_solver.cu:624-630).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "brdc_kernels.cuh"
+
+using namespace brdc;
+
+struct brdc_handle_struct {
+    cudaStream_t own_stream;
+    cudaStream_t stream;
+    int last_code;
+    brdc_error_source last_src;
+    const char *last_site;
+    int sm_count;
+    int device;
+    // batched: signature of the forest whose tables sit in a workspace
+    const void *prep_ws;
+    std::vector<long long> prep_off;
+    // phase timing (off by default)
+    int timing;
+    cudaEvent_t ev[2 + 4 * BRDC_MAX_LEVELS + 2];
+    int ev_ready;
+    int ev_used;
+    int launches;
+    int timed_levels;
+    int has_lowner[BRDC_MAX_LEVELS];
+};
+
+namespace {
+
+void set_error(brdc_handle h, int code, brdc_error_source src,
+               const char *site) {
+    if (h != nullptr) {
+        h->last_code = code;
+        h->last_src = src;
+        h->last_site = site;
+    }
+}
+
+#define BRDC_CUDA(h, site, expr)                                               \
+    do {                                                                       \
+        const cudaError_t e__ = (expr);                                        \
+        if (e__ != cudaSuccess) {                                              \
+            set_error((h), (int)e__, BRDC_ERROR_SRC_CUDA, (site));             \
+            return BRDC_STATUS_CUDA_ERROR;                                     \
+        }                                                                      \
+    } while (0)
+
+constexpr size_t kAlign = 256; // gpu/src/workspace_align.hpp:9
+
+size_t align_up(size_t v) { return (v + kAlign - 1) / kAlign * kAlign; }
+
+// Host view of a forest.
+struct HostForest {
+    int B = 0;
+    std::vector<long long> off;  // B+1
+    std::vector<int> lev;        // B
+    int max_levels = 0;
+    long long total_n = 0;
+    long long leaves = 0;
+    std::vector<int> level_nodes; // nodes per level
+    std::vector<int> level_mmax;  // largest node per level
+    long long nn0 = 0;            // max nodes of a level
+};
+
+bool build_forest(int B, const long long *off, HostForest *f) {
+    f->B = B;
+    f->off.assign(off, off + B + 1);
+    f->lev.resize(B);
+    f->max_levels = 0;
+    f->leaves = 0;
+    f->total_n = off[B] - off[0];
+    for (int b = 0; b < B; ++b) {
+        const long long n = off[b + 1] - off[b];
+        if (n <= 0 || n > (1LL << 30)) {
+            return false;
+        }
+        f->lev[b] = tree_levels(n);
+        f->max_levels = std::max(f->max_levels, f->lev[b]);
+        f->leaves += 1LL << f->lev[b];
+    }
+    if (f->max_levels >= BRDC_MAX_LEVELS) {
+        return false;
+    }
+    f->level_nodes.assign(f->max_levels, 0);
+    f->level_mmax.assign(f->max_levels, 0);
+    for (int b = 0; b < B; ++b) {
+        const long long n = off[b + 1] - off[b];
+        const int L = f->lev[b];
+        for (int k = 0; k < L; ++k) {
+            const int depth = L - 1 - k;
+            f->level_nodes[k] += 1 << depth;
+            const long long mm = (n + (1LL << depth) - 1) >> depth;
+            f->level_mmax[k] = std::max<long long>(f->level_mmax[k], mm);
+        }
+    }
+    f->nn0 = 1;
+    for (int k = 0; k < f->max_levels; ++k) {
+        f->nn0 = std::max<long long>(f->nn0, f->level_nodes[k]);
+    }
+    return true;
+}
+
+enum DArr {
+    A_cd, A_cf, A_cl, A_nd, A_nf, A_nl, A_md, A_mz, A_mf, A_ml, A_ad, A_az,
+    A_af, A_al, A_gc, A_gs, A_zd, A_zf, A_zl, A_gd, A_gf, A_gl, A_NDN
+};
+enum PArr { P_pd, P_pz, P_pf, P_pl, P_pw, P_rdo, P_rtau, P_rlam, P_NDP };
+enum IArr { I_mflag, I_morig, I_amap, I_gmark, I_gbase, I_NIN };
+enum QArr { Q_pmap, Q_rorg, Q_NIP };
+
+Layout make_layout(const HostForest &f) {
+    Layout L{};
+    L.nt = f.total_n;
+    L.nn0 = f.nn0;
+    L.np = f.total_n + f.nn0 + 4;
+    size_t cur = 0;
+    L.o_hdr = cur;
+    cur = align_up(cur + sizeof(WsHeader));
+    for (int i = 0; i < A_NDN; ++i) {
+        L.o_d[i] = cur;
+        cur = align_up(cur + sizeof(double) * (size_t)L.nt);
+    }
+    for (int i = 0; i < P_NDP; ++i) {
+        L.o_d[A_NDN + i] = cur;
+        cur = align_up(cur + sizeof(double) * (size_t)L.np);
+    }
+    for (int i = 0; i < I_NIN; ++i) {
+        L.o_i[i] = cur;
+        cur = align_up(cur + sizeof(int) * (size_t)L.nt);
+    }
+    for (int i = 0; i < Q_NIP; ++i) {
+        L.o_i[I_NIN + i] = cur;
+        cur = align_up(cur + sizeof(int) * (size_t)L.np);
+    }
+    // per-node arrays: nK, nKz (int), nrho, ntol, nzn (double), prefixes
+    L.o_i[I_NIN + Q_NIP + 0] = cur;
+    cur = align_up(cur + sizeof(int) * (size_t)L.nn0);
+    L.o_i[I_NIN + Q_NIP + 1] = cur;
+    cur = align_up(cur + sizeof(int) * (size_t)L.nn0);
+    L.o_i[I_NIN + Q_NIP + 2] = cur;
+    cur = align_up(cur + sizeof(int) * (size_t)(L.nn0 + 1));
+    L.o_i[I_NIN + Q_NIP + 3] = cur;
+    cur = align_up(cur + sizeof(int) * (size_t)(L.nn0 + 1));
+    L.o_d[A_NDN + P_NDP + 0] = cur;
+    cur = align_up(cur + sizeof(double) * (size_t)L.nn0);
+    L.o_d[A_NDN + P_NDP + 1] = cur;
+    cur = align_up(cur + sizeof(double) * (size_t)L.nn0);
+    L.o_d[A_NDN + P_NDP + 2] = cur;
+    cur = align_up(cur + sizeof(double) * (size_t)L.nn0);
+    // forest tables (batched only)
+    if (f.B > 1) {
+        L.o_f_off = cur;
+        cur = align_up(cur + sizeof(long long) * (size_t)(f.B + 1));
+        L.o_f_lev = cur;
+        cur = align_up(cur + sizeof(int) * (size_t)f.B);
+        L.o_f_node_prefix = cur;
+        cur = align_up(cur + sizeof(int) * (size_t)(f.B + 1) *
+                                 (size_t)std::max(f.max_levels, 1));
+        L.o_f_leaf_prefix = cur;
+        cur = align_up(cur + sizeof(int) * (size_t)(f.B + 1));
+    }
+    L.bytes = align_up(cur);
+    return L;
+}
+
+Ws carve(void *base, const Layout &L) {
+    char *b = static_cast<char *>(base);
+    Ws w{};
+    w.hdr = reinterpret_cast<WsHeader *>(b + L.o_hdr);
+    double **dp[A_NDN] = {&w.cd, &w.cf, &w.cl, &w.nd, &w.nf, &w.nl, &w.md, &w.mz,
+                          &w.mf, &w.ml, &w.ad, &w.az, &w.af, &w.al, &w.gc, &w.gs,
+                          &w.zd, &w.zf, &w.zl, &w.gd, &w.gf, &w.gl};
+    for (int i = 0; i < A_NDN; ++i) {
+        *dp[i] = reinterpret_cast<double *>(b + L.o_d[i]);
+    }
+    double **pp[P_NDP] = {&w.pd, &w.pz, &w.pf, &w.pl, &w.pw, &w.rdo, &w.rtau, &w.rlam};
+    for (int i = 0; i < P_NDP; ++i) {
+        *pp[i] = reinterpret_cast<double *>(b + L.o_d[A_NDN + i]);
+    }
+    int **ip[I_NIN] = {&w.mflag, &w.morig, &w.amap, &w.gmark, &w.gbase};
+    for (int i = 0; i < I_NIN; ++i) {
+        *ip[i] = reinterpret_cast<int *>(b + L.o_i[i]);
+    }
+    w.pmap = reinterpret_cast<int *>(b + L.o_i[I_NIN + Q_pmap]);
+    w.rorg = reinterpret_cast<int *>(b + L.o_i[I_NIN + Q_rorg]);
+    w.nK = reinterpret_cast<int *>(b + L.o_i[I_NIN + Q_NIP + 0]);
+    w.nKz = reinterpret_cast<int *>(b + L.o_i[I_NIN + Q_NIP + 1]);
+    w.pref_sec = reinterpret_cast<int *>(b + L.o_i[I_NIN + Q_NIP + 2]);
+    w.pref_rows = reinterpret_cast<int *>(b + L.o_i[I_NIN + Q_NIP + 3]);
+    w.nrho = reinterpret_cast<double *>(b + L.o_d[A_NDN + P_NDP + 0]);
+    w.ntol = reinterpret_cast<double *>(b + L.o_d[A_NDN + P_NDP + 1]);
+    w.nzn = reinterpret_cast<double *>(b + L.o_d[A_NDN + P_NDP + 2]);
+    if (L.o_f_off != 0) {
+        w.f_off = reinterpret_cast<long long *>(b + L.o_f_off);
+        w.f_lev = reinterpret_cast<int *>(b + L.o_f_lev);
+        w.f_node_prefix = reinterpret_cast<int *>(b + L.o_f_node_prefix);
+        w.f_leaf_prefix = reinterpret_cast<int *>(b + L.o_f_leaf_prefix);
+    }
+    return w;
+}
+
+template <int T>
+void launch_md(const KArgs &a, int grid, cudaStream_t s) {
+    k_merge_deflate<T><<<grid, T, 0, s>>>(a);
+}
+
+void launch_merge_deflate(const KArgs &a, int mmax, cudaStream_t s) {
+    // about 4 rows per thread, 32..1024 threads
+    int t = 32;
+    while (t < 1024 && t * 4 < mmax) {
+        t <<= 1;
+    }
+    switch (t) {
+    case 32: launch_md<32>(a, a.nodes, s); break;
+    case 64: launch_md<64>(a, a.nodes, s); break;
+    case 128: launch_md<128>(a, a.nodes, s); break;
+    case 256: launch_md<256>(a, a.nodes, s); break;
+    case 512: launch_md<512>(a, a.nodes, s); break;
+    default: launch_md<1024>(a, a.nodes, s); break;
+    }
+}
+
+constexpr size_t smem_tiles(int na) { return sizeof(double) * 2 * na * kTile; }
+
+bool g_attr_done = false;
+
+cudaError_t set_attrs() {
+    if (g_attr_done) {
+        return cudaSuccess;
+    }
+    cudaError_t e = cudaFuncSetAttribute(
+        k_secular, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_tiles(2));
+    if (e == cudaSuccess) {
+        e = cudaFuncSetAttribute(k_lowner, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem_tiles(3));
+    }
+    if (e == cudaSuccess) {
+        e = cudaFuncSetAttribute(k_rows_place,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem_tiles(4));
+    }
+    g_attr_done = (e == cudaSuccess);
+    return e;
+}
+
+// Event slot layout of one timed solve: 0 before init, 1 after init,
+// 2 after the leaves, then 4 per level (after merge, secular, lowner, rows).
+void mark(brdc_handle h, int slot) {
+    if (h->timing && h->ev_ready) {
+        cudaEventRecord(h->ev[slot], h->stream);
+        h->ev_used = std::max(h->ev_used, slot + 1);
+    }
+}
+
+// Enqueue the whole forward solve.
+brdc_status run_forest(brdc_handle h, const HostForest &hf, const Forest &F,
+                       const Ws &w, const double *D, const double *E, double *W) {
+    cudaStream_t s = h->stream;
+    BRDC_CUDA(h, "brdc.set_attributes", set_attrs());
+    h->ev_used = 0;
+    h->launches = 0;
+    h->timed_levels = hf.max_levels;
+    mark(h, 0);
+    k_init<<<1, 64, 0, s>>>(w.hdr, hf.max_levels, hf.B, hf.total_n, hf.leaves, 0);
+    BRDC_CUDA(h, "brdc.init", cudaGetLastError());
+    ++h->launches;
+    mark(h, 1);
+
+    KArgs a{};
+    a.F = F;
+    a.w = w;
+    a.D = D;
+    a.E = E;
+    a.W = W;
+    {
+        const long long per = (long long)kLeafWarps;
+        long long grid = (hf.leaves + per - 1) / per;
+        grid = std::min<long long>(grid, (long long)h->sm_count * 16);
+        grid = std::max<long long>(grid, 1);
+        k_leaf<<<(unsigned)grid, kLeafWarps * 32, 0, s>>>(a, hf.leaves);
+        BRDC_CUDA(h, "brdc.leaf", cudaGetLastError());
+        ++h->launches;
+        mark(h, 2);
+    }
+    const int sweep_grid = h->sm_count * 3;
+    for (int k = 0; k < hf.max_levels; ++k) {
+        a.k = k;
+        a.nodes = hf.level_nodes[k];
+        launch_merge_deflate(a, hf.level_mmax[k], s);
+        BRDC_CUDA(h, "brdc.merge_deflate", cudaGetLastError());
+        mark(h, 3 + 4 * k);
+        k_secular<<<sweep_grid, kSweepThreads, smem_tiles(2), s>>>(a);
+        BRDC_CUDA(h, "brdc.secular", cudaGetLastError());
+        mark(h, 4 + 4 * k);
+        h->launches += 2;
+        // Loewner z is needed unless every merge of this level is a root
+        bool any_inner = false;
+        for (int b = 0; b < hf.B; ++b) {
+            if (hf.lev[b] - 1 > k) {
+                any_inner = true;
+                break;
+            }
+        }
+        h->has_lowner[k] = any_inner ? 1 : 0;
+        if (any_inner) {
+            k_lowner<<<sweep_grid, kSweepThreads, smem_tiles(3), s>>>(a);
+            BRDC_CUDA(h, "brdc.lowner", cudaGetLastError());
+            ++h->launches;
+        }
+        mark(h, 5 + 4 * k);
+        k_rows_place<<<sweep_grid, kSweepThreads, smem_tiles(4), s>>>(a);
+        BRDC_CUDA(h, "brdc.rows_place", cudaGetLastError());
+        ++h->launches;
+        mark(h, 6 + 4 * k);
+        std::swap(a.w.cd, a.w.nd);
+        std::swap(a.w.cf, a.w.nf);
+        std::swap(a.w.cl, a.w.nl);
+    }
+    return BRDC_STATUS_SUCCESS;
+}
+
+} // namespace
+
+// ------------------------------------------------------------------ C ABI
+
+extern "C" const char *brdc_version(void) { return "brdc-b200 0.1"; }
+
+extern "C" brdc_status brdc_create(brdc_handle *handle) {
+    if (handle == nullptr) {
+        return BRDC_STATUS_INVALID_POINTER;
+    }
+    *handle = nullptr;
+    brdc_handle h = new (std::nothrow) brdc_handle_struct{};
+    if (h == nullptr) {
+        return BRDC_STATUS_ALLOC_FAILED;
+    }
+    h->prep_ws = nullptr;
+    if (cudaGetDevice(&h->device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount,
+                               h->device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) !=
+            cudaSuccess) {
+        delete h;
+        return BRDC_STATUS_CUDA_ERROR;
+    }
+    h->stream = h->own_stream;
+    *handle = h;
+    return BRDC_STATUS_SUCCESS;
+}
+
+extern "C" brdc_status brdc_destroy(brdc_handle h) {
+    if (h == nullptr) {
+        return BRDC_STATUS_INVALID_HANDLE;
+    }
+    if (h->ev_ready) {
+        for (auto &e : h->ev) {
+            cudaEventDestroy(e);
+        }
+    }
+    if (h->own_stream != nullptr) {
+        cudaStreamDestroy(h->own_stream);
+    }
+    delete h;
+    return BRDC_STATUS_SUCCESS;
+}
+
+extern "C" brdc_status brdc_set_stream(brdc_handle h, brdc_stream_t stream) {
+    if (h == nullptr) {
+        return BRDC_STATUS_INVALID_HANDLE;
+    }
+    h->stream = stream != nullptr ? reinterpret_cast<cudaStream_t>(stream)
+                                  : h->own_stream;
+    return BRDC_STATUS_SUCCESS;
+}
+
+extern "C" brdc_status brdc_get_stream(brdc_handle h, brdc_stream_t *stream) {
+    if (h == nullptr) {
+        return BRDC_STATUS_INVALID_HANDLE;
+    }
+    if (stream == nullptr) {
+        return BRDC_STATUS_INVALID_POINTER;
+    }
+    *stream = reinterpret_cast<brdc_stream_t>(h->stream);
+    return BRDC_STATUS_SUCCESS;
+}
+
+extern "C" brdc_status brdc_get_last_error(brdc_handle h, int *code,
+                                           brdc_error_source *source,
+                                           const char **site) {
+    if (h == nullptr) {
+        return BRDC_STATUS_INVALID_HANDLE;
+    }
+    if (code != nullptr) {
+        *code = h->last_code;
+    }
+    if (source != nullptr) {
+        *source = h->last_src;
+    }
+    if (site != nullptr) {
+        *site = h->last_site;
+    }
+    return BRDC_STATUS_SUCCESS;
+}
+
+extern "C" const char *brdc_status_to_string(brdc_status status) {
+    switch (status) {
+    case BRDC_STATUS_SUCCESS: return "success";
+    case BRDC_STATUS_INVALID_HANDLE: return "invalid_handle";
+    case BRDC_STATUS_INVALID_POINTER: return "invalid_pointer";
+    case BRDC_STATUS_INVALID_VALUE: return "invalid_value";
+    case BRDC_STATUS_INVALID_WORKSPACE: return "invalid_workspace";
+    case BRDC_STATUS_ALLOC_FAILED: return "alloc_failed";
+    case BRDC_STATUS_CUDA_ERROR: return "cuda_error";
+    case BRDC_STATUS_INTERNAL_ERROR: return "internal_error";
+    case BRDC_STATUS_NOT_IMPLEMENTED: return "not_implemented";
+    case BRDC_STATUS_NOT_CONVERGED: return "not_converged";
+    default: return "unknown_status";
+    }
+}
+
+extern "C" brdc_status brdc_dstebr_workspace_size(int64_t n, int flags,
+                                                  size_t *bytes) {
+    if (bytes == nullptr) {
+        return BRDC_STATUS_INVALID_POINTER;
+    }
+    if (n <= 0 || n > (1LL << 30)) {
+        return BRDC_STATUS_INVALID_VALUE;
+    }
+    (void)flags;
+    const long long off[2] = {0, (long long)n};
+    HostForest f;
+    if (!build_forest(1, off, &f)) {
+        return BRDC_STATUS_INVALID_VALUE;
+    }
+    *bytes = make_layout(f).bytes;
+    return BRDC_STATUS_SUCCESS;
+}
+
+extern "C" brdc_status brdc_dstebr(brdc_handle h, int64_t n, const double *d_D,
+                                   const double *d_E, double *d_W,
+                                   void *workspace, size_t workspace_size) {
+    if (h == nullptr) {
+        return BRDC_STATUS_INVALID_HANDLE;
+    }
+    if (d_D == nullptr || d_W == nullptr || (n > 1 && d_E == nullptr)) {
+        return BRDC_STATUS_INVALID_POINTER;
+    }
+    if (n <= 0 || n > (1LL << 30)) {
+        return BRDC_STATUS_INVALID_VALUE;
+    }
+    const long long off[2] = {0, (long long)n};
+    HostForest hf;
+    if (!build_forest(1, off, &hf)) {
+        return BRDC_STATUS_INVALID_VALUE;
+    }
+    const Layout L = make_layout(hf);
+    if (workspace == nullptr || workspace_size < L.bytes) {
+        return BRDC_STATUS_INVALID_WORKSPACE;
+    }
+    const Ws w = carve(workspace, L);
+    Forest F{};
+    F.B = 1;
+    F.max_levels = hf.max_levels;
+    F.n0 = n;
+    F.L0 = hf.max_levels;
+    return run_forest(h, hf, F, w, d_D, d_E, d_W);
+}
+
+extern "C" brdc_status brdc_get_info(brdc_handle h, const void *workspace,
+                                     int *info) {
+    if (h == nullptr) {
+        return BRDC_STATUS_INVALID_HANDLE;
+    }
+    if (workspace == nullptr || info == nullptr) {
+        return BRDC_STATUS_INVALID_POINTER;
+    }
+    const WsHeader *hd = static_cast<const WsHeader *>(workspace);
+    int vals[2] = {0, 0};
+    BRDC_CUDA(h, "brdc.get_info.copy",
+              cudaMemcpyAsync(vals, &hd->status, sizeof(int) * 2,
+                              cudaMemcpyDeviceToHost, h->stream));
+    BRDC_CUDA(h, "brdc.get_info.sync", cudaStreamSynchronize(h->stream));
+    if (vals[0] != 0) {
+        *info = -vals[0];
+        set_error(h, vals[0], BRDC_ERROR_SRC_DEVICE, "brdc.device_status");
+        return BRDC_STATUS_INTERNAL_ERROR;
+    }
+    *info = vals[1];
+    return vals[1] > 0 ? BRDC_STATUS_NOT_CONVERGED : BRDC_STATUS_SUCCESS;
+}
+
+extern "C" brdc_status brdc_get_diagnostics(brdc_handle h, const void *workspace,
+                                            brdc_diagnostics *out) {
+    if (h == nullptr) {
+        return BRDC_STATUS_INVALID_HANDLE;
+    }
+    if (workspace == nullptr || out == nullptr) {
+        return BRDC_STATUS_INVALID_POINTER;
+    }
+    WsHeader hd;
+    BRDC_CUDA(h, "brdc.diagnostics.copy",
+              cudaMemcpyAsync(&hd, workspace, sizeof(WsHeader),
+                              cudaMemcpyDeviceToHost, h->stream));
+    BRDC_CUDA(h, "brdc.diagnostics.sync", cudaStreamSynchronize(h->stream));
+    std::memset(out, 0, sizeof(*out));
+    out->n = (int)hd.total_n;
+    out->levels = hd.max_levels;
+    out->leaf_count = hd.leaf_count;
+    out->leaf_sweeps_max = hd.leaf_sweeps_max;
+    for (int k = 0; k < hd.max_levels && k < BRDC_MAX_LEVELS; ++k) {
+        out->level[k] = hd.diag[k];
+        out->level[k].level = k;
+        out->level[k].zero_deflated_total =
+            hd.diag[k].size_sum - hd.diag[k].dd_before_sum;
+        out->level[k].close_deflated_total =
+            hd.diag[k].dd_before_sum - hd.diag[k].dd_after_sum;
+    }
+    return BRDC_STATUS_SUCCESS;
+}
+
+extern "C" brdc_status brdc_set_timing(brdc_handle h, int enable) {
+    if (h == nullptr) {
+        return BRDC_STATUS_INVALID_HANDLE;
+    }
+    if (enable && !h->ev_ready) {
+        for (auto &e : h->ev) {
+            BRDC_CUDA(h, "brdc.timing.event_create", cudaEventCreate(&e));
+        }
+        h->ev_ready = 1;
+    }
+    h->timing = enable ? 1 : 0;
+    return BRDC_STATUS_SUCCESS;
+}
+
+extern "C" brdc_status brdc_get_last_timings(brdc_handle h, brdc_timings *out) {
+    if (h == nullptr) {
+        return BRDC_STATUS_INVALID_HANDLE;
+    }
+    if (out == nullptr) {
+        return BRDC_STATUS_INVALID_POINTER;
+    }
+    std::memset(out, 0, sizeof(*out));
+    if (!h->timing || !h->ev_ready || h->ev_used < 3) {
+        return BRDC_STATUS_INVALID_VALUE;
+    }
+    BRDC_CUDA(h, "brdc.timing.sync", cudaStreamSynchronize(h->stream));
+    auto el = [&](int a, int b) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, h->ev[a], h->ev[b]);
+        return ms;
+    };
+    out->init_ms = el(0, 1);
+    out->leaf_ms = el(1, 2);
+    out->levels = h->timed_levels;
+    out->launches = h->launches;
+    int prev = 2;
+    for (int k = 0; k < h->timed_levels; ++k) {
+        const float m = el(prev, 3 + 4 * k);
+        const float s = el(3 + 4 * k, 4 + 4 * k);
+        const float l = el(4 + 4 * k, 5 + 4 * k);
+        const float r = el(5 + 4 * k, 6 + 4 * k);
+        out->level_ms[k][0] = m;
+        out->level_ms[k][1] = s;
+        out->level_ms[k][2] = l;
+        out->level_ms[k][3] = r;
+        out->merge_ms += m;
+        out->secular_ms += s;
+        out->lowner_ms += l;
+        out->rows_ms += r;
+        prev = 6 + 4 * k;
+    }
+    out->total_ms = el(0, prev);
+    return BRDC_STATUS_SUCCESS;
+}
+
+// --------------------------------------------------------------- batched
+
+extern "C" brdc_status brdc_dstebr_batched_workspace_size(int64_t count,
+                                                          const int64_t *offsets,
+                                                          size_t *bytes) {
+    if (bytes == nullptr || offsets == nullptr) {
+        return BRDC_STATUS_INVALID_POINTER;
+    }
+    if (count <= 0 || count > (1LL << 28) || offsets[0] != 0) {
+        return BRDC_STATUS_INVALID_VALUE;
+    }
+    HostForest f;
+    if (!build_forest((int)count, reinterpret_cast<const long long *>(offsets), &f)) {
+        return BRDC_STATUS_INVALID_VALUE;
+    }
+    *bytes = make_layout(f).bytes;
+    return BRDC_STATUS_SUCCESS;
+}
+
+extern "C" brdc_status brdc_dstebr_batched(brdc_handle h, int64_t count,
+                                           const int64_t *offsets,
+                                           const double *d_D, const double *d_E,
+                                           double *d_W, void *workspace,
+                                           size_t workspace_size) {
+    if (h == nullptr) {
+        return BRDC_STATUS_INVALID_HANDLE;
+    }
+    if (offsets == nullptr || d_D == nullptr || d_W == nullptr || d_E == nullptr) {
+        return BRDC_STATUS_INVALID_POINTER;
+    }
+    if (count <= 0 || count > (1LL << 28) || offsets[0] != 0) {
+        return BRDC_STATUS_INVALID_VALUE;
+    }
+    HostForest hf;
+    if (!build_forest((int)count, reinterpret_cast<const long long *>(offsets), &hf)) {
+        return BRDC_STATUS_INVALID_VALUE;
+    }
+    const Layout L = make_layout(hf);
+    if (workspace == nullptr || workspace_size < L.bytes) {
+        return BRDC_STATUS_INVALID_WORKSPACE;
+    }
+    const Ws w = carve(workspace, L);
+    Forest F{};
+    F.B = hf.B;
+    F.max_levels = hf.max_levels;
+    if (hf.B == 1) {
+        F.n0 = hf.total_n;
+        F.L0 = hf.max_levels;
+    } else {
+        // Tables are uploaded once per (workspace, offsets); later calls with
+        // the same pair enqueue kernels only and can be graph-captured.
+        const bool same = h->prep_ws == workspace &&
+                          h->prep_off.size() == (size_t)hf.B + 1 &&
+                          std::equal(h->prep_off.begin(), h->prep_off.end(),
+                                     hf.off.begin());
+        if (!same) {
+            std::vector<int> node_prefix((size_t)(hf.B + 1) *
+                                         std::max(hf.max_levels, 1), 0);
+            for (int k = 0; k < hf.max_levels; ++k) {
+                int *row = node_prefix.data() + (size_t)k * (hf.B + 1);
+                row[0] = 0;
+                for (int b = 0; b < hf.B; ++b) {
+                    const int L = hf.lev[b];
+                    row[b + 1] = row[b] + (L > k ? (1 << (L - 1 - k)) : 0);
+                }
+            }
+            std::vector<int> leaf_prefix(hf.B + 1, 0);
+            for (int b = 0; b < hf.B; ++b) {
+                leaf_prefix[b + 1] = leaf_prefix[b] + (1 << hf.lev[b]);
+            }
+            BRDC_CUDA(h, "brdc.batched.upload_off",
+                      cudaMemcpyAsync(w.f_off, hf.off.data(),
+                                      sizeof(long long) * (hf.B + 1),
+                                      cudaMemcpyHostToDevice, h->stream));
+            BRDC_CUDA(h, "brdc.batched.upload_lev",
+                      cudaMemcpyAsync(w.f_lev, hf.lev.data(), sizeof(int) * hf.B,
+                                      cudaMemcpyHostToDevice, h->stream));
+            BRDC_CUDA(h, "brdc.batched.upload_nodes",
+                      cudaMemcpyAsync(w.f_node_prefix, node_prefix.data(),
+                                      sizeof(int) * node_prefix.size(),
+                                      cudaMemcpyHostToDevice, h->stream));
+            BRDC_CUDA(h, "brdc.batched.upload_leaves",
+                      cudaMemcpyAsync(w.f_leaf_prefix, leaf_prefix.data(),
+                                      sizeof(int) * leaf_prefix.size(),
+                                      cudaMemcpyHostToDevice, h->stream));
+            BRDC_CUDA(h, "brdc.batched.upload_sync", cudaStreamSynchronize(h->stream));
+            h->prep_ws = workspace;
+            h->prep_off = hf.off;
+        }
+        F.off = w.f_off;
+        F.lev = w.f_lev;
+        F.node_prefix = w.f_node_prefix;
+        F.leaf_prefix = w.f_leaf_prefix;
+    }
+    return run_forest(h, hf, F, w, d_D, d_E, d_W);
+}
+
+// -------------------------------------------------------------- backward
+extern "C" brdc_status brdc_dstebr_backward(brdc_handle h, int64_t n,
+                                            const double *d_D, const double *d_E,
+                                            const double *d_G, double *d_gD,
+                                            double *d_gE, void *workspace,
+                                            size_t workspace_size,
+                                            int keep_forward) {
+    (void)n;
+    (void)d_D;
+    (void)d_E;
+    (void)d_G;
+    (void)d_gD;
+    (void)d_gE;
+    (void)workspace;
+    (void)workspace_size;
+    (void)keep_forward;
+    if (h == nullptr) {
+        return BRDC_STATUS_INVALID_HANDLE;
+    }
+    return BRDC_STATUS_NOT_IMPLEMENTED;
+}
+
+// ------------------------------------------------- LAPACK-style host entry
+namespace {
+int wprod_nthreads_host() {
+    // BRDC_WPROD_NTHREADS (cpu/src/dstedc_dc_br.f:153-213) with the team
+    // size taken from OMP_NUM_THREADS (1 when unset).
+    int nt = 1;
+    if (const char *s = std::getenv("OMP_NUM_THREADS")) {
+        nt = std::max(1, std::atoi(s));
+    }
+    int val = 0;
+    if (const char *s = std::getenv("OPENBLAS_BRDC_WPROD_THREADS")) {
+        for (const char *p = s; *p != '\0' && p - s < 32; ++p) {
+            if (*p >= '0' && *p <= '9') {
+                val = 10 * val + (*p - '0');
+            } else if (*p != ' ') {
+                val = 0;
+                break;
+            }
+        }
+    }
+    if (val > 0) {
+        return std::max(1, std::min(val, nt));
+    }
+    const int cap = nt <= 1 ? 1 : nt <= 8 ? 2 : nt <= 28 ? 4 : 16;
+    return std::max(1, std::min(cap, nt));
+}
+} // namespace
+
+extern "C" void brdc_dstedc_dc_br_(const int *n_, double *d, double *e,
+                                   double *work, const int *lwork_,
+                                   int *iwork, const int *liwork_, int *info) {
+    const int n = *n_;
+    const int lwork = *lwork_, liwork = *liwork_;
+    *info = 0;
+    const bool lquery = (lwork == -1 || liwork == -1);
+    if (n < 0) {
+        *info = -1;
+        return;
+    }
+    const int smlsiz = 25; // ILAENV(9, 'DSTEDC', ...)
+    int lwmin = 1, liwmin = 1;
+    if (n > smlsiz) {
+        lwmin = std::max(1, (16 + 2 * wprod_nthreads_host()) * n);
+        liwmin = std::max(1, 7 * n);
+    }
+    work[0] = (double)lwmin;
+    iwork[0] = liwmin;
+    if (lwork < lwmin && !lquery) {
+        *info = -5;
+    } else if (liwork < liwmin && !lquery) {
+        *info = -7;
+    }
+    if (*info != 0 || lquery || n == 0 || n == 1) {
+        return;
+    }
+    brdc_handle h = nullptr;
+    if (brdc_create(&h) != BRDC_STATUS_SUCCESS) {
+        *info = n + 1;
+        return;
+    }
+    size_t ws_bytes = 0;
+    brdc_dstebr_workspace_size(n, 0, &ws_bytes);
+    double *dD = nullptr, *dE = nullptr, *dW = nullptr;
+    void *ws = nullptr;
+    int fail = 0;
+    fail |= cudaMalloc(&dD, sizeof(double) * n) != cudaSuccess;
+    fail |= cudaMalloc(&dE, sizeof(double) * std::max(n - 1, 1)) != cudaSuccess;
+    fail |= cudaMalloc(&dW, sizeof(double) * n) != cudaSuccess;
+    fail |= cudaMalloc(&ws, ws_bytes) != cudaSuccess;
+    if (!fail) {
+        fail |= cudaMemcpyAsync(dD, d, sizeof(double) * n, cudaMemcpyHostToDevice,
+                                h->stream) != cudaSuccess;
+        fail |= cudaMemcpyAsync(dE, e, sizeof(double) * (n - 1),
+                                cudaMemcpyHostToDevice, h->stream) != cudaSuccess;
+    }
+    int dinfo = 0;
+    if (!fail) {
+        fail |= brdc_dstebr(h, n, dD, dE, dW, ws, ws_bytes) != BRDC_STATUS_SUCCESS;
+    }
+    if (!fail) {
+        const brdc_status st = brdc_get_info(h, ws, &dinfo);
+        fail |= !(st == BRDC_STATUS_SUCCESS || st == BRDC_STATUS_NOT_CONVERGED);
+    }
+    if (!fail) {
+        fail |= cudaMemcpyAsync(d, dW, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                                h->stream) != cudaSuccess;
+        fail |= cudaStreamSynchronize(h->stream) != cudaSuccess;
+    }
+    cudaFree(dD);
+    cudaFree(dE);
+    cudaFree(dW);
+    cudaFree(ws);
+    brdc_destroy(h);
+    if (fail) {
+        *info = n + 1;
+    } else if (dinfo > 0) {
+        *info = dinfo;
+    }
+    work[0] = (double)lwmin;
+    iwork[0] = liwmin;
+}

@@ -1,0 +1,454 @@
+// brdc_common.cuh -- data layout, merge-tree geometry and device helpers
+// shared by the kernels and the host driver.
+//
+// Merge tree.  A tridiagonal of order n is cut into 2^L leaves with
+// L = bitlen(n-1) - 4 for n > 16 (leaves of 8..16 rows), every node of size
+// s splitting into a left child of floor(s/2) and a right child of
+// ceil(s/2) rows: the tree of the reference prototype
+// (gpu/src/tridiag_solver_dc.cuh:213-225, tridiag_solver_extract.cuh:63-70).
+// Node starts are recomputed from the node index by walking down from the
+// root (O(depth) integer steps), so no tree table lives in memory.
+//
+// Forest.  The batched entry solves B independent tridiagonals packed back
+// to back; level k of the forest holds, for every instance b with L_b > k,
+// the 2^(L_b-1-k) merges at depth L_b-1-k of that instance.  A single
+// solve is a forest of one.
+//
+// Layout of one level's data in HBM (all arrays indexed by the global row
+// index of the forest, so every node owns the contiguous slice
+// [gstart, gstart+m) of each array; the pole arrays are padded so that each
+// node's slice starts 16-byte aligned for cp.async.bulk):
+//   cur_{d,f,l} / nxt_{d,f,l}  node eigenvalues (ascending) with the first
+//                              and last rows of the node eigenvector matrix
+//   m{d,z,f,l}, mflag         merged child lists (sorted) with z and rows
+//   a{d,z,f,l}                poles that survived the small-z test
+//   z{d,f,l}, g{d,f,l}        deflated by the small-z test / by rotation
+//   p{d,z,f,l}, pw            the K secular poles, their z and Loewner z
+//   r{org,do,tau,lam}         per root: origin pole, d at origin, shift,
+//                              eigenvalue
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include "../../include/brdc.h"
+
+namespace brdc {
+
+constexpr int kLeafMax = 16;
+constexpr int kSweepThreads = 256;  // threads per CTA of the sweep kernels
+constexpr int kTile = 1024;         // poles per shared-memory tile
+constexpr double kDeflTolScale = 8.0;  // tol = 8*eps*max(max|d|,max|z|)
+                                        // (merge_kernels.cuh:9-11,1090-1091)
+constexpr unsigned kWsMagic = 0x42524443u; // "BRDC"
+
+inline int tree_levels(long long n) {
+    if (n <= 16) {
+        return 0;
+    }
+    int bits = 0;
+    long long r = n - 1;
+    while (r > 0) {
+        ++bits;
+        r >>= 1;
+    }
+    return bits - 4;
+}
+
+// Per-level control block written by the kernels.
+struct LevelCtl {
+    int ticket;      // CTAs of the merge kernel that finished
+    int nodes;       // merges at this level (set by the host)
+    int tpr;         // lanes per root chosen for the sweeps
+    int items_sec;   // work items of the secular / Loewner kernels
+    int items_rows;  // work items of the row / placement kernel
+    int total_k;
+    int pad[2];
+};
+
+struct WsHeader {
+    unsigned magic;
+    int B;
+    long long total_n;
+    int max_levels;
+    int flags;
+    int status;      // device error code, 0 = ok
+    int nonconv;     // roots that hit the iteration cap
+    int leaf_sweeps_max;
+    int leaf_count;
+    int pad[2];
+    LevelCtl lvl[BRDC_MAX_LEVELS];
+    brdc_level_diagnostics diag[BRDC_MAX_LEVELS];
+};
+
+// Device error codes written to WsHeader::status.
+enum DeviceError : int {
+    kErrNone = 0,
+    kErrBarrierTimeout = 1,
+    kErrBadGeometry = 2,
+};
+
+// Forest description passed by value to every kernel.
+struct Forest {
+    int B;
+    int max_levels;
+    long long n0;               // B == 1: order
+    int L0;                     // B == 1: levels
+    const long long *off;       // [B+1] row offsets (B > 1)
+    const int *lev;             // [B] levels per instance (B > 1)
+    const int *node_prefix;     // [max_levels][B+1] node-count prefix (B > 1)
+    const int *leaf_prefix;     // [B+1] leaf-count prefix (B > 1)
+};
+
+// Every device array of one workspace.
+struct Ws {
+    WsHeader *hdr;
+    // node data, ping-pong
+    double *cd, *cf, *cl;
+    double *nd, *nf, *nl;
+    // merged lists
+    double *md, *mz, *mf, *ml;
+    int *mflag, *morig;
+    // small-z survivors, deflated lists
+    double *ad, *az, *af, *al;
+    int *amap, *gmark, *gbase;
+    double *gc, *gs;
+    double *zd, *zf, *zl;
+    double *gd, *gf, *gl;
+    // poles and roots (padded layout)
+    double *pd, *pz, *pf, *pl, *pw;
+    int *pmap;
+    int *rorg;
+    double *rdo, *rtau, *rlam;
+    // per node at one level
+    int *nK, *nKz;
+    double *nrho, *ntol, *nzn;
+    int *pref_sec, *pref_rows;
+    // forest tables (batched)
+    long long *f_off;
+    int *f_lev, *f_node_prefix, *f_leaf_prefix;
+};
+
+struct Layout {
+    size_t bytes;
+    long long nt;     // total rows
+    long long np;     // padded pole-array length
+    long long nn0;    // nodes of the widest level
+    size_t o_hdr;
+    size_t o_d[40];
+    size_t o_i[16];
+    size_t o_f_off, o_f_lev, o_f_node_prefix, o_f_leaf_prefix;
+};
+
+#if defined(__CUDACC__)
+
+__host__ __device__ inline void walk_node(long long n, int depth, long long idx,
+                                          long long *start, long long *size) {
+    long long s = n, st = 0;
+    for (int bit = depth - 1; bit >= 0; --bit) {
+        const long long h = s >> 1;
+        if ((idx >> bit) & 1) {
+            st += h;
+            s -= h;
+        } else {
+            s = h;
+        }
+    }
+    *start = st;
+    *size = s;
+}
+
+struct NodeGeom {
+    int inst;
+    int depth;        // depth of the merged node (0 = instance root)
+    long long gstart; // first row of the node in the forest
+    long long istart; // first row of the instance
+    long long iend;   // one past the last row of the instance
+    int m, m1;        // node rows, rows of the left child
+    long long poff;   // aligned start of the node's pole slice
+};
+
+__device__ inline int upper_bound_int(const int *a, int n, int x) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (a[mid] <= x) {
+            lo = mid + 1;
+        } else {
+            hi = mid;
+        }
+    }
+    return lo;
+}
+
+// Geometry of merge node g (global index at forest level k).
+__device__ inline NodeGeom node_geom(const Forest &F, int k, int g) {
+    NodeGeom G;
+    int b = 0;
+    long long idx = g;
+    long long n = F.n0;
+    int L = F.L0;
+    long long base = 0;
+    if (F.B > 1) {
+        const int *pre = F.node_prefix + (size_t)k * (F.B + 1);
+        b = upper_bound_int(pre, F.B + 1, g) - 1;
+        idx = g - pre[b];
+        L = F.lev[b];
+        base = F.off[b];
+        n = F.off[b + 1] - base;
+    }
+    G.inst = b;
+    G.depth = L - 1 - k;
+    long long st, s;
+    walk_node(n, G.depth, idx, &st, &s);
+    G.gstart = base + st;
+    G.istart = base;
+    G.iend = base + n;
+    G.m = (int)s;
+    G.m1 = (int)(s >> 1);
+    G.poff = (G.gstart + g + 1) & ~1LL;
+    return G;
+}
+
+struct LeafGeom {
+    long long gstart, istart, iend;
+    int s;
+    int top; // instance is a single leaf
+};
+
+__device__ inline LeafGeom leaf_geom(const Forest &F, long long g) {
+    LeafGeom G;
+    int b = 0;
+    long long idx = g;
+    long long n = F.n0;
+    int L = F.L0;
+    long long base = 0;
+    if (F.B > 1) {
+        b = upper_bound_int(F.leaf_prefix, F.B + 1, (int)g) - 1;
+        idx = g - F.leaf_prefix[b];
+        L = F.lev[b];
+        base = F.off[b];
+        n = F.off[b + 1] - base;
+    }
+    long long st, s;
+    walk_node(n, L, idx, &st, &s);
+    G.gstart = base + st;
+    G.istart = base;
+    G.iend = base + n;
+    G.s = (int)s;
+    G.top = (L == 0);
+    return G;
+}
+
+// ---------------------------------------------------------------- helpers
+
+__device__ inline double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+    }
+    return v;
+}
+
+__device__ inline double warp_max(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    }
+    return v;
+}
+
+// Block-wide reductions; scratch holds >= 32 doubles.  All threads return
+// the result.
+template <int T>
+__device__ inline double block_sum(double v, double *scratch) {
+    v = warp_sum(v);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) {
+        scratch[w] = v;
+    }
+    __syncthreads();
+    double r = 0.0;
+    if constexpr (T > 32) {
+        r = (l < (T >> 5)) ? scratch[l] : 0.0;
+        r = warp_sum(r);
+    } else {
+        r = scratch[0];
+    }
+    return r;
+}
+
+template <int T>
+__device__ inline double block_max(double v, double *scratch) {
+    v = warp_max(v);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) {
+        scratch[w] = v;
+    }
+    __syncthreads();
+    double r;
+    if constexpr (T > 32) {
+        r = (l < (T >> 5)) ? scratch[l] : 0.0;
+        r = warp_max(r);
+    } else {
+        r = scratch[0];
+    }
+    return r;
+}
+
+// Exclusive scan of one int per thread; *total receives the block sum.
+template <int T>
+__device__ inline int block_exscan(int v, int *scratch, int *total) {
+    const int l = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (l >= o) {
+            x += y;
+        }
+    }
+    __syncthreads();
+    if (l == 31) {
+        scratch[w] = x;
+    }
+    __syncthreads();
+    int wpre = 0, tot = 0;
+    if constexpr (T > 32) {
+        int s = (l < (T >> 5)) ? scratch[l] : 0;
+        int inc = s;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (l >= o) {
+                inc += y;
+            }
+        }
+        tot = __shfl_sync(0xffffffffu, inc, 31);
+        wpre = __shfl_sync(0xffffffffu, inc - s, w);
+    } else {
+        tot = scratch[0];
+    }
+    *total = tot;
+    return wpre + x - v;
+}
+
+// Plane rotation zeroing g against f: c*f + s*g = r >= 0, -s*f + c*g = 0
+// (same convention as the reference's device_lartg,
+// gpu/src/tridiag_solver_device.cuh:15-36).
+__device__ inline void lartg(double f, double g, double *c, double *s,
+                             double *r) {
+    if (g == 0.0) {
+        *c = 1.0;
+        *s = 0.0;
+        *r = f;
+        return;
+    }
+    if (f == 0.0) {
+        *c = 0.0;
+        *s = 1.0;
+        *r = g;
+        return;
+    }
+    const double scale = fabs(f) + fabs(g);
+    const double fs = f / scale, gs = g / scale;
+    const double nrm = scale * sqrt(fs * fs + gs * gs);
+    *c = f / nrm;
+    *s = g / nrm;
+    *r = nrm;
+}
+
+template <typename T>
+__device__ inline int lower_bound_d(const T *a, int n, T x) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (a[mid] < x) {
+            lo = mid + 1;
+        } else {
+            hi = mid;
+        }
+    }
+    return lo;
+}
+
+template <typename T>
+__device__ inline int upper_bound_d(const T *a, int n, T x) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (a[mid] <= x) {
+            lo = mid + 1;
+        } else {
+            hi = mid;
+        }
+    }
+    return lo;
+}
+
+// -------------------------------------------- TMA bulk copies + mbarriers
+// One-dimensional cp.async.bulk global -> shared with transaction-count
+// completion on an mbarrier.  Every wait is bounded: on timeout the kernel
+// records kErrBarrierTimeout and the caller abandons the work item.
+
+constexpr unsigned kMbarSpinLimit = 1u << 26;
+
+__device__ inline unsigned smem_u32(const void *p) {
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ inline void mbar_init(uint64_t *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(count)
+                 : "memory");
+}
+
+__device__ inline void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ inline void fence_proxy_async() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ inline void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+    asm volatile(
+        "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
+            smem_u32(bar)),
+        "r"(bytes)
+        : "memory");
+}
+
+__device__ inline void bulk_g2s(void *dst, const void *src, unsigned bytes,
+                                uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes "
+        "[%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// Returns true when the phase completed, false on timeout.
+__device__ inline bool mbar_wait(uint64_t *bar, unsigned phase) {
+    const unsigned a = smem_u32(bar);
+    for (unsigned it = 0; it < kMbarSpinLimit; ++it) {
+        unsigned done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(phase)
+            : "memory");
+        if (done) {
+            return true;
+        }
+    }
+    return false;
+}
+
+#endif // __CUDACC__
+
+} // namespace brdc

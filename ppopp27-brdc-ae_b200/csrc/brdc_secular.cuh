@@ -1,0 +1,388 @@
+// brdc_secular.cuh -- one secular root as a resumable state machine.
+//
+// Solves  f(lambda) = 1/rho + sum_j z_j^2 / (d_j - lambda) = 0  for root i of
+// a deflated rank-one update (poles d_0 < ... < d_{K-1}, rho > 0): root
+// i < K-1 lies in (d_i, d_{i+1}), root K-1 in (d_{K-1}, d_{K-1}+rho*|z|^2].
+//
+// The iteration is Ren-Cang Li's "middle way" / "fixed weight" rational
+// scheme with bisection safeguards (R.-C. Li, "Solving secular equations
+// stably and efficiently", LAPACK Working Note 89, 1994), the scheme LAPACK
+// DLAED4 implements and the reference calls for every root
+// (cpu/src/dlaed4_br.f:59; its GPU prototype restates it without the
+// three-pole step in gpu/src/tridiag_solver_secular.cuh:404-601,953-1085).
+// This file is written for a GPU that evaluates the O(K) sums of many roots
+// in one sweep over shared-memory tiles of poles:
+//   * the state is advanced between sweeps (sec_after_sweep), so a thread
+//     block can interleave the sweeps of all its roots;
+//   * every delta is recomputed from the compact pair (origin, tau),
+//     delta_j = (d_j - d_org) - tau, instead of being updated in place, so no
+//     O(K) delta column is stored per root (the compact ORG/TAU
+//     representation of cpu/src/dlaed4_br.f:15-26,95-103);
+//   * the sweep excludes the two bracketing poles p, p+1; the root adds
+//     their terms itself so they are never cancelled against the rest.
+// The error bound is LAPACK's running-sum bound for the summation order the
+// sweep actually uses.
+#pragma once
+
+#include <cmath>
+
+#ifndef __CUDACC__
+#ifndef __host__
+#define __host__
+#endif
+#ifndef __device__
+#define __device__
+#endif
+#endif
+
+namespace brdc {
+
+constexpr int kSecularMaxIter = 64;
+
+struct SecSums {
+    double psi;   // sum_{j < p} z_j^2 / delta_j
+    double dpsi;  // sum_{j < p} z_j^2 / delta_j^2
+    double phi;   // sum_{j > p+1} z_j^2 / delta_j
+    double dphi;  // sum_{j > p+1} z_j^2 / delta_j^2
+    double err;   // running-sum rounding bound of the two partial sums
+};
+
+__host__ __device__ inline void sec_zero(SecSums &s) {
+    s.psi = 0.0;
+    s.dpsi = 0.0;
+    s.phi = 0.0;
+    s.dphi = 0.0;
+    s.err = 0.0;
+}
+
+struct SecRoot {
+    // problem (fixed)
+    int i;         // root index
+    int p;         // left model pole (i, or K-2 for the last root)
+    int last;      // 1 for the root right of the last pole
+    double dp, dq; // d_p, d_{p+1}
+    double zp2, zq2;
+    double rhoinv;
+    double hi0;    // last root: rho * |z|^2 (upper bound of tau)
+    // iteration state
+    int stage;     // 0: midpoint sums pending, 1: iterating, 2: done
+    int org;       // origin pole index (p or p+1)
+    double dorg;   // d_org
+    double tau;    // lambda = d_org + tau
+    double lo, hi; // bracket of tau
+    double prevw;
+    int iter;
+    int swtch;     // 1: middle way, 0: fixed weight
+    int failed;
+    // evaluation point of the next sweep: delta_j = (d_j - eorg_d) - etau
+    double eorg_d;
+    double etau;
+};
+
+// Set up root i (0-based) of a problem with K >= 2 poles.  d and z are the
+// pole and weight arrays (only d_p, d_{p+1}, z_p, z_{p+1} are read).
+__host__ __device__ inline void sec_init(SecRoot &r, int i, int K,
+                                         const double *d, const double *z,
+                                         double rho, double znorm2) {
+    r.i = i;
+    r.last = (i == K - 1) ? 1 : 0;
+    r.p = r.last ? K - 2 : i;
+    r.dp = d[r.p];
+    r.dq = d[r.p + 1];
+    r.zp2 = z[r.p] * z[r.p];
+    r.zq2 = z[r.p + 1] * z[r.p + 1];
+    r.rhoinv = 1.0 / rho;
+    r.hi0 = rho * znorm2;
+    r.stage = 0;
+    r.iter = 0;
+    r.swtch = 0;
+    r.failed = 0;
+    r.prevw = 0.0;
+    if (r.last) {
+        r.org = r.p + 1;
+        r.dorg = r.dq;
+        r.lo = 0.0;
+        r.hi = r.hi0;
+        r.eorg_d = r.dq;
+        r.etau = 0.5 * r.hi0;
+    } else {
+        r.org = r.p;
+        r.dorg = r.dp;
+        const double mid = 0.5 * (r.dq - r.dp);
+        r.lo = 0.0;
+        r.hi = mid;
+        r.eorg_d = r.dp;
+        r.etau = mid;
+    }
+    r.tau = r.etau;
+}
+
+// One term of the sweep for pole j (d_j, z_j).  Poles p and p+1 are skipped.
+// Branch-free, because the lanes of a warp serve roots with different p.
+__host__ __device__ inline void sec_accum(SecSums &s, const SecRoot &r, int j,
+                                          double dj, double zj) {
+    const bool skip = (j == r.p) || (j == r.p + 1);
+    const bool left = j < r.p;
+    const double delta = (dj - r.eorg_d) - r.etau;
+    double t = zj / delta;
+    t = skip ? 0.0 : t;
+    const double term = zj * t;
+    const double t2 = t * t;
+    s.psi += left ? term : 0.0;
+    s.dpsi += left ? t2 : 0.0;
+    s.phi += left ? 0.0 : term;
+    s.dphi += left ? 0.0 : t2;
+    s.err += skip ? 0.0 : (left ? -s.psi : s.phi);
+}
+
+// Combine partial sums of two lanes (the tree adds its own rounding).  Every
+// operation is commutative in (a, b), so the lanes of a butterfly reduction
+// end with bit-identical sums and take identical branches afterwards.
+__host__ __device__ inline void sec_combine(SecSums &a, const SecSums &b) {
+    a.psi = a.psi + b.psi;
+    a.dpsi = a.dpsi + b.dpsi;
+    a.phi = a.phi + b.phi;
+    a.dphi = a.dphi + b.dphi;
+    a.err = (a.err + b.err) + (fabs(a.psi) + a.phi);
+}
+
+__host__ __device__ inline double sec_clamp_tau(double t, double lo, double hi) {
+    if (!(t > lo && t < hi)) {
+        t = 0.5 * (lo + hi);
+    }
+    return t;
+}
+
+// Advance the state after a sweep evaluated at (eorg_d, etau).  Returns the
+// new stage (2 once converged or failed).
+__host__ __device__ inline int sec_after_sweep(SecRoot &r, const SecSums &s,
+                                               double eps) {
+    if (r.stage == 2) {
+        return 2;
+    }
+    if (r.stage == 0) {
+        // Initial guess from the two bracketing poles with the rest of the
+        // sum frozen at the evaluation point.
+        const double c = r.rhoinv + s.psi + s.phi;
+        if (!r.last) {
+            const double del = r.dq - r.dp;
+            const double mid = r.etau;
+            const double w = c + r.zp2 / (-mid) + r.zq2 / ((r.dq - r.dp) - mid);
+            double tau;
+            if (w > 0.0) {
+                // root in (d_p, mid): origin p
+                r.org = r.p;
+                r.dorg = r.dp;
+                r.lo = 0.0;
+                r.hi = mid;
+                const double a = c * del + r.zp2 + r.zq2;
+                const double b = r.zp2 * del;
+                const double disc = sqrt(fabs(a * a - 4.0 * b * c));
+                tau = (a > 0.0) ? 2.0 * b / (a + disc) : (a - disc) / (2.0 * c);
+            } else {
+                // root in [mid, d_q): origin p+1
+                r.org = r.p + 1;
+                r.dorg = r.dq;
+                r.lo = -mid;
+                r.hi = 0.0;
+                const double a = c * del - r.zp2 - r.zq2;
+                const double b = r.zq2 * del;
+                const double disc = sqrt(fabs(a * a + 4.0 * b * c));
+                tau = (a < 0.0) ? 2.0 * b / (a - disc) : -(a + disc) / (2.0 * c);
+            }
+            r.tau = sec_clamp_tau(tau, r.lo, r.hi);
+        } else {
+            const double del = r.dq - r.dp;
+            const double mid = r.etau;
+            const double w = c + r.zp2 / ((r.dp - r.dq) - mid) + r.zq2 / (-mid);
+            if (w <= 0.0) {
+                r.lo = mid;
+                r.hi = r.hi0;
+            } else {
+                r.lo = 0.0;
+                r.hi = mid;
+            }
+            double tau = 0.5 * (r.lo + r.hi);
+            if (c > 0.0) {
+                const double a = c * del - r.zp2 - r.zq2;
+                const double b = r.zq2 * del;
+                const double disc = sqrt(fabs(a * a + 4.0 * b * c));
+                const double t2 = (a <= 0.0) ? (disc - a) / (2.0 * c)
+                                             : 2.0 * b / (a + disc);
+                if (t2 > r.lo && t2 <= r.hi) {
+                    tau = t2;
+                } else if (!(t2 > r.lo)) {
+                    tau = 0.5 * (r.lo + r.hi);
+                } else {
+                    tau = r.hi;
+                }
+            }
+            r.tau = tau;
+        }
+        r.stage = 1;
+        r.iter = 0;
+        r.eorg_d = r.dorg;
+        r.etau = r.tau;
+        return 1;
+    }
+
+    // stage 1: sums at (dorg, tau)
+    r.iter += 1;
+    const double tau = r.tau;
+    const double dlp = (r.dp - r.dorg) - tau; // delta_p
+    const double dlq = (r.dq - r.dorg) - tau; // delta_{p+1}
+    const double tp = r.zp2 / dlp;
+    const double tq = r.zq2 / dlq;
+    const double dtp = tp / dlp;
+    const double dtq = tq / dlq;
+    const double psi_f = s.psi + tp;
+    const double phi_f = s.phi + tq;
+    const double dpsi_f = s.dpsi + dtp;
+    const double dphi_f = s.dphi + dtq;
+    const double w = r.rhoinv + psi_f + phi_f;
+    const double dw = dpsi_f + dphi_f;
+
+    double erretm;
+    if (!r.last) {
+        double psil = s.psi, phil = s.phi, err = s.err, torg;
+        if (r.org == r.p) {
+            phil += tq;
+            err += phil;
+            torg = tp;
+        } else {
+            psil += tp;
+            err += fabs(psil);
+            torg = tq;
+        }
+        erretm = 8.0 * (phil - psil) + err + 2.0 * r.rhoinv +
+                 3.0 * fabs(torg) + fabs(tau) * dw;
+    } else {
+        const double psil = s.psi + tp;
+        const double err = s.err + fabs(psil);
+        erretm = 8.0 * (-tq - psil) + err - tq + r.rhoinv + fabs(tau) * dw;
+    }
+
+    if (fabs(w) <= eps * erretm || !(w == w)) {
+        r.stage = 2;
+        return 2;
+    }
+    if (w <= 0.0) {
+        r.lo = (tau > r.lo) ? tau : r.lo;
+    } else {
+        r.hi = (tau < r.hi) ? tau : r.hi;
+    }
+    if (r.hi - r.lo <= 2.0 * eps * fabs(tau) || r.iter >= kSecularMaxIter) {
+        // bracket collapsed to rounding level: accept; iteration cap: flag
+        if (r.iter >= kSecularMaxIter && !(r.hi - r.lo <= 2.0 * eps * fabs(tau))) {
+            r.failed = 1;
+        }
+        r.stage = 2;
+        return 2;
+    }
+
+    // switching rule between fixed-weight and middle-way models
+    if (!r.last) {
+        if (r.iter == 2) {
+            r.swtch = (r.org == r.p) ? (-w > fabs(r.prevw) / 10.0)
+                                     : (w > fabs(r.prevw) / 10.0);
+        } else if (r.iter > 2) {
+            if (w * r.prevw > 0.0 && fabs(w) > fabs(r.prevw) / 10.0) {
+                r.swtch = !r.swtch;
+            }
+        }
+    }
+    r.prevw = w;
+
+    double eta;
+    if (!r.last) {
+        double c;
+        if (r.swtch && r.iter > 1) {
+            c = w - dlp * dpsi_f - dlq * dphi_f;
+        } else if (r.org == r.p) {
+            // fixed weight: (d_p - d_q) * (z_p / delta_p)^2
+            c = w - dlq * dw - (r.dp - r.dq) * (r.zp2 / (dlp * dlp));
+        } else {
+            c = w - dlp * dw - (r.dq - r.dp) * (r.zq2 / (dlq * dlq));
+        }
+        const double a = (dlp + dlq) * w - dlp * dlq * dw;
+        const double b = dlp * dlq * w;
+        if (c == 0.0) {
+            double aa = a;
+            if (aa == 0.0) {
+                if (r.swtch && r.iter > 1) {
+                    aa = dlp * dlp * dpsi_f + dlq * dlq * dphi_f;
+                } else if (r.org == r.p) {
+                    aa = r.zp2 + dlq * dlq * dw;
+                } else {
+                    aa = r.zq2 + dlp * dlp * dw;
+                }
+            }
+            eta = b / aa;
+        } else if (a <= 0.0) {
+            eta = (a - sqrt(fabs(a * a - 4.0 * b * c))) / (2.0 * c);
+        } else {
+            eta = 2.0 * b / (a + sqrt(fabs(a * a - 4.0 * b * c)));
+        }
+        if (w * eta >= 0.0) {
+            eta = -w / dw;
+        }
+    } else {
+        const double c0 = w - dlp * dpsi_f - dlq * dphi_f;
+        const double c = (r.iter == 1) ? fabs(c0) : c0;
+        const double a = (dlp + dlq) * w - dlp * dlq * dw;
+        const double b = dlp * dlq * w;
+        if (c == 0.0) {
+            eta = r.hi - tau;
+        } else if (a >= 0.0) {
+            eta = (a + sqrt(fabs(a * a - 4.0 * b * c))) / (2.0 * c);
+        } else {
+            eta = 2.0 * b / (a - sqrt(fabs(a * a - 4.0 * b * c)));
+        }
+        if (w * eta > 0.0) {
+            eta = -w / dw;
+        }
+    }
+    double tnew = tau + eta;
+    if (!(tnew > r.lo && tnew < r.hi)) {
+        eta = (w < 0.0) ? 0.5 * (r.hi - tau) : 0.5 * (r.lo - tau);
+        tnew = tau + eta;
+    }
+    r.tau = tnew;
+    r.etau = tnew;
+    r.eorg_d = r.dorg;
+    return 1;
+}
+
+// Host/serial driver: solve root i of (d, z, rho) with K >= 1 poles by
+// repeated full sweeps.  Returns the number of sweeps; *org/*tau describe
+// the root (lambda = d[*org] + *tau).  Used by the CPU unit tests only.
+__host__ __device__ inline int sec_solve_serial(int K, const double *d,
+                                                const double *z, double rho,
+                                                double znorm2, int i, int *org,
+                                                double *tau, int *failed,
+                                                double eps) {
+    if (K == 1) {
+        *org = 0;
+        *tau = rho * z[0] * z[0];
+        *failed = 0;
+        return 0;
+    }
+    SecRoot r;
+    sec_init(r, i, K, d, z, rho, znorm2);
+    int sweeps = 0;
+    while (r.stage != 2) {
+        SecSums s;
+        sec_zero(s);
+        for (int j = 0; j < K; ++j) {
+            sec_accum(s, r, j, d[j], z[j]);
+        }
+        ++sweeps;
+        sec_after_sweep(r, s, eps);
+    }
+    *org = r.org;
+    *tau = r.tau;
+    *failed = r.failed;
+    return sweeps;
+}
+
+} // namespace brdc

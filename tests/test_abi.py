@@ -1,0 +1,69 @@
+"""C-ABI library: loads, exports every entry point of include/brdc.h, and
+answers the argument checks that need no GPU."""
+import ctypes
+import os
+import re
+
+import pytest
+
+import brdc
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    text = open(os.path.join(ROOT, "include", "brdc.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    names = set(re.findall(r"\b(brdc_[a-z0-9_]+)\s*\(", text))
+    return sorted(names)
+
+
+def test_header_matches_binding_list():
+    assert sorted(brdc.EXPORTS) == declared_symbols()
+
+
+def test_library_exports_every_declared_symbol(built_lib):
+    lib = ctypes.CDLL(built_lib)
+    for name in declared_symbols():
+        assert hasattr(lib, name), name
+
+
+def test_workspace_query(built_lib):
+    assert brdc.workspace_size(1) > 0
+    small, big = brdc.workspace_size(4096), brdc.workspace_size(65536)
+    assert big > small
+    # O(n): far below the reference's n*min(n,4096) delta slab
+    assert big < 400 * 65536
+    assert big % 256 == 0
+    with pytest.raises(brdc.BrdcError) as ei:
+        brdc.workspace_size(0)
+    assert ei.value.status == brdc.INVALID_VALUE
+    with pytest.raises(brdc.BrdcError):
+        brdc.workspace_size(-5)
+
+
+def test_argument_checks_without_device(built_lib):
+    lib = brdc.load()
+    # NULL handle first, as tridiag_solver.cu:2545-2547
+    assert lib.brdc_dstebr(None, 10, None, None, None, None, 0) == brdc.INVALID_HANDLE
+    assert lib.brdc_get_info(None, None, None) == brdc.INVALID_HANDLE
+    assert lib.brdc_destroy(None) == brdc.INVALID_HANDLE
+    assert lib.brdc_create(None) == brdc.INVALID_POINTER
+    assert brdc.load().brdc_status_to_string(9) == b"not_converged"
+    assert brdc.load().brdc_status_to_string(4) == b"invalid_workspace"
+
+
+def test_lapack_style_query(built_lib):
+    # cpu/src/dstedc_dc_br.f:44-75 query and argument errors
+    info, lw, liw = brdc.dstedc_dc_br_query(4096)
+    assert info == 0 and liw == 7 * 4096 and lw % 4096 == 0 and lw >= 18 * 4096
+    assert brdc.dstedc_dc_br_query(20)[1:] == (1, 1)
+    assert brdc.dstedc_dc_br_query(-1)[0] == -1
+    assert brdc.dstedc_dc_br_query(4096, lwork=10, liwork=7 * 4096)[0] == -5
+    assert brdc.dstedc_dc_br_query(4096, lwork=10**6, liwork=5)[0] == -7
+
+
+def test_batched_workspace_query(built_lib):
+    assert brdc.batched_workspace_size([0, 10, 50, 4146]) > brdc.workspace_size(4096)
+    with pytest.raises(brdc.BrdcError):
+        brdc.batched_workspace_size([0, 10, 10])

@@ -1,0 +1,121 @@
+"""Parity of the sm_100a solve with the oracle (C restatement of the
+reference's DSTEDC_DC_BR), LAPACK DSTERF and closed forms."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from brdc import families
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+TOL = 1e-12  # max |lambda - lambda_ref| / ||T||_2
+
+
+def gpu_solve(solver, d, e):
+    import torch
+
+    D = torch.tensor(d, dtype=torch.float64, device="cuda")
+    E = torch.tensor(e if len(e) else np.zeros(1), dtype=torch.float64, device="cuda")
+    W = solver.dstebr(D, E)
+    info = solver.info(len(d))
+    assert info == 0, f"info={info}"
+    return W.cpu().numpy()
+
+
+def rel_err(w, ref):
+    return float(np.max(np.abs(w - ref)) / max(np.max(np.abs(ref)), 1e-300))
+
+
+@pytest.mark.parametrize("n", list(range(1, 70)))
+def test_small_orders_every_tree_shape(solver, n):
+    rng = np.random.default_rng(1000 + n)
+    d, e = rng.standard_normal(n), rng.standard_normal(max(n - 1, 0))
+    w = gpu_solve(solver, d, e)
+    assert np.all(np.diff(w) >= 0)
+    assert rel_err(w, np.sort(oracle.dsterf(d, e))) < TOL
+
+
+@pytest.mark.parametrize("family", ["uniform", "normal", "clustered"])
+@pytest.mark.parametrize("n", [100, 1000, 4096, 8192])
+def test_families_vs_oracle(solver, family, n):
+    d, e = families.generate(family, n)
+    w = gpu_solve(solver, d, e)
+    ref = oracle.dstedc_dc_br(d, e)
+    assert rel_err(w, ref) < TOL
+    assert rel_err(w, np.sort(oracle.dsterf(d, e))) < TOL
+
+
+@pytest.mark.parametrize("n", [17, 33, 100, 4096, 65536])
+def test_toeplitz_closed_form(solver, n):
+    d, e = families.generate("toeplitz", n)
+    assert rel_err(gpu_solve(solver, d, e), families.toeplitz_eigenvalues(n)) < TOL
+
+
+@pytest.mark.parametrize("family", ["uniform", "normal", "clustered"])
+def test_full_size_vs_oracle(solver, family):
+    d, e = families.generate(family, 65536)
+    assert rel_err(gpu_solve(solver, d, e), oracle.dstedc_dc_br(d, e)) < TOL
+
+
+def test_reference_fixture_slice(solver):
+    z = np.load(os.path.join(GOLDEN, "reduced_dense_lead4096.npz"))
+    assert rel_err(gpu_solve(solver, z["d"], z["e"]), z["dsterf"]) < TOL
+
+
+def test_sign_of_offdiagonal_ignored(solver):
+    d, e = families.generate("normal", 3000)
+    w1 = gpu_solve(solver, d, e)
+    w2 = gpu_solve(solver, d, -e)
+    w3 = gpu_solve(solver, d, np.abs(e))
+    assert np.array_equal(w1, w2) and np.array_equal(w1, w3)
+
+
+def test_zero_couplings_block_diagonal(solver):
+    rng = np.random.default_rng(5)
+    d, e = rng.standard_normal(2048), rng.standard_normal(2047)
+    e[::37] = 0.0
+    e[1023] = 0.0  # the root cut
+    assert rel_err(gpu_solve(solver, d, e), np.sort(oracle.dsterf(d, e))) < TOL
+
+
+def test_diagonal_matrix(solver):
+    rng = np.random.default_rng(6)
+    d = rng.standard_normal(1000)
+    assert np.array_equal(gpu_solve(solver, d, np.zeros(999)), np.sort(d))
+
+
+def test_repeated_solves_bitwise_stable(solver):
+    d, e = families.generate("uniform", 20000)
+    w1 = gpu_solve(solver, d, e)
+    w2 = gpu_solve(solver, d, e)
+    assert np.array_equal(w1, w2)
+
+
+def test_trace_and_frobenius(solver):
+    d, e = families.generate("normal", 65536)
+    w = gpu_solve(solver, d, e)
+    assert abs(w.sum() - d.sum()) < 1e-10 * np.abs(w).sum()
+    assert abs((w * w).sum() - (d * d).sum() - 2 * (e * e).sum()) < 1e-10 * (w * w).sum()
+
+
+def test_diagnostics_counts(solver):
+    d, e = families.generate("uniform", 4096)
+    gpu_solve(solver, d, e)
+    dg = solver.diagnostics(4096)
+    assert dg["levels"] == 8 and dg["leaf_count"] == 256
+    for k, lv in enumerate(dg["level"]):
+        assert lv["merge_count"] == 2 ** (7 - k)
+        assert lv["size_sum"] == 4096
+        assert 0 <= lv["dd_after_sum"] <= lv["dd_before_sum"] <= 4096
+        assert lv["secular_iter_failed"] == 0
+
+
+def test_lapack_style_host_entry(built_lib):
+    import brdc
+
+    d, e = families.generate("normal", 5000)
+    w = brdc.dstedc_dc_br(d, e)
+    assert rel_err(w, np.sort(oracle.dsterf(d, e))) < TOL

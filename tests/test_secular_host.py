@@ -1,0 +1,78 @@
+"""The product's per-root secular state machine, compiled for the host,
+against LAPACK DLAED4 (the routine the reference calls per root,
+cpu/src/dlaed4_br.f:59)."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import oracle
+
+
+@pytest.fixture(scope="module")
+def hostlib(built_lib):
+    import build as b
+
+    lib = ctypes.CDLL(b.HOSTLIB)
+    dp = ctypes.POINTER(ctypes.c_double)
+    lib.brdc_host_secular_root.argtypes = [
+        ctypes.c_int, dp, dp, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+        ctypes.POINTER(ctypes.c_int), dp, ctypes.POINTER(ctypes.c_int),
+    ]
+    return lib
+
+
+def _root(lib, d, z, rho, i):
+    dp = ctypes.POINTER(ctypes.c_double)
+    org, tau, f = ctypes.c_int(), ctypes.c_double(), ctypes.c_int()
+    sweeps = lib.brdc_host_secular_root(len(d), d.ctypes.data_as(dp), z.ctypes.data_as(dp),
+                                        rho, float(z @ z), i, ctypes.byref(org),
+                                        ctypes.byref(tau), ctypes.byref(f))
+    return d[org.value] + tau.value, sweeps, f.value
+
+
+@pytest.mark.parametrize("kind", ["normal", "uniform", "clustered", "tiny_z"])
+def test_roots_match_dlaed4(hostlib, kind):
+    rng = np.random.default_rng(hash(kind) % 2**32)
+    worst, sw_max = 0.0, 0
+    for _ in range(40):
+        K = int(rng.integers(2, 200))
+        if kind == "normal":
+            d = np.sort(rng.standard_normal(K))
+        elif kind == "uniform":
+            d = np.sort(rng.uniform(0, 1, K))
+        elif kind == "clustered":
+            d = np.unique(np.concatenate([rng.uniform(-1, 1, K // 2), 0.3 + 1e-8 * rng.uniform(-1, 1, K - K // 2)]))
+            K = d.shape[0]
+        else:
+            d = np.sort(rng.standard_normal(K))
+        z = rng.standard_normal(K)
+        if kind == "tiny_z":
+            z[::2] *= 1e-7
+        z /= np.linalg.norm(z)
+        rho = float(rng.uniform(0.05, 4.0))
+        for i in range(K):
+            lam_ref, _ = oracle.dlaed4(d, z, rho, i)
+            lam, sweeps, failed = _root(hostlib, d, z, rho, i)
+            assert not failed
+            gap = float(np.min(np.abs(d - lam_ref)))
+            err = abs(lam - lam_ref) / max(min(gap, abs(lam_ref)) if lam_ref != 0 else gap, 1e-300)
+            worst = max(worst, min(err, abs(lam - lam_ref) / max(abs(lam_ref), 1e-300)))
+            sw_max = max(sw_max, sweeps)
+            if i < K - 1:
+                assert d[i] <= lam <= d[i + 1]
+            else:
+                assert lam >= d[K - 1]
+    assert worst < 1e-12
+    assert sw_max <= 20
+
+
+def test_two_poles_closed_form(hostlib):
+    d = np.array([0.0, 1.0])
+    z = np.array([0.6, 0.8])
+    rho = 1.5
+    M = np.diag(d) + rho * np.outer(z, z)
+    ev = np.linalg.eigvalsh(M)
+    for i in range(2):
+        lam, _, _ = _root(hostlib, d, z, rho, i)
+        assert abs(lam - ev[i]) < 1e-15 * 4
