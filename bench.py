@@ -64,7 +64,7 @@ def start_clock_sampler(path):
              "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-             "--format=csv,noheader,nounits", "-lms", "200"],
+             "--format=csv,noheader,nounits", "-lms", "50"],
             stdout=open(path, "w"), stderr=subprocess.DEVNULL)
     except Exception:
         return None
@@ -177,7 +177,7 @@ def run_reference_arm(args, rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true")
@@ -291,17 +291,24 @@ def collect_extras(torch, brdc, families, solver, D, E, W, ws, d, e, flush, args
 
     # per-phase timings and roofline of the dominant kernel
     solver.set_timing(True)
-    acc = None
+    keys = ("leaf_ms", "merge_ms", "secular_ms", "lowner_ms", "rows_ms", "total_ms")
+    acc = {k: 0.0 for k in keys}
+    level_acc = None
     reps = 5
+    launches = 0
     for _ in range(reps):
         flush.zero_()
         solver.dstebr(D, E, W=W, workspace=ws)
         t = solver.last_timings()
-        if acc is None:
-            acc = {k: 0.0 for k in ("leaf_ms", "merge_ms", "secular_ms", "lowner_ms", "rows_ms", "total_ms")}
-        for k in acc:
+        for k in keys:
             acc[k] += t[k] / reps
         launches = t["launches"]
+        if level_acc is None:
+            level_acc = [[0.0] * 4 for _ in t["level_ms"]]
+        for k2, row in enumerate(t["level_ms"]):
+            for j in range(4):
+                level_acc[k2][j] += row[j] / reps
+    acc["level_ms"] = level_acc
     solver.set_timing(False)
     out["launches"] = launches
     out["phase_ms"] = acc

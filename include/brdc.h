@@ -60,8 +60,9 @@ typedef struct brdc_handle_struct *brdc_handle;
 brdc_status brdc_create(brdc_handle *handle);
 brdc_status brdc_destroy(brdc_handle handle);
 
-/* Run on a caller-owned stream instead (NULL restores the handle's own
- * stream).  No reference counterpart: the reference always uses its own. */
+/* Run on a caller-owned stream instead of the handle's own one.  As in the
+ * CUDA runtime, NULL names the legacy default stream.  No reference
+ * counterpart: the reference always uses its own stream. */
 brdc_status brdc_set_stream(brdc_handle handle, brdc_stream_t stream);
 brdc_status brdc_get_stream(brdc_handle handle, brdc_stream_t *stream);
 

@@ -384,8 +384,7 @@ extern "C" brdc_status brdc_set_stream(brdc_handle h, brdc_stream_t stream) {
     if (h == nullptr) {
         return BRDC_STATUS_INVALID_HANDLE;
     }
-    h->stream = stream != nullptr ? reinterpret_cast<cudaStream_t>(stream)
-                                  : h->own_stream;
+    h->stream = reinterpret_cast<cudaStream_t>(stream);
     return BRDC_STATUS_SUCCESS;
 }
 
