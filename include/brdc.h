@@ -99,6 +99,30 @@ brdc_status brdc_dstebr(brdc_handle handle, int64_t n, const double *d_D,
                         const double *d_E, double *d_W, void *workspace,
                         size_t workspace_size);
 
+/* Allocation-free variant of brdc_dstebr, for callers that cannot allocate
+ * device memory when they solve (work inside host callbacks or
+ * stream-ordered sections where cudaMalloc would synchronise or is not
+ * allowed, plug-ins whose host owns every device allocation, paths that
+ * must not meet an allocation failure).  No reference counterpart: the
+ * reference solve always takes a caller-allocated workspace.
+ *  - Scratch is one static device array of 4.5 MiB inside the library,
+ *    present on every GPU that loads it until the process exits; it bounds
+ *    n to 16384.  Larger n returns BRDC_STATUS_INVALID_VALUE and records
+ *    the reason as the last error.
+ *  - The first call on a device looks up the array's device address
+ *    (cudaGetSymbolAddress) with that device current; make that first call
+ *    before any stream capture.  The handle must belong to the current
+ *    device.  No cudaMalloc or cudaFree is ever called.
+ *  - All calls share the one array: calls whose solves overlap on the GPU
+ *    (other streams, other host threads) race and corrupt each other.
+ *    Serialise them on one stream.  The array keeps the last call's data;
+ *    every solve writes what it reads, so nothing needs clearing.
+ *  - Status of the device side (brdc_get_info) is not available for this
+ *    entry; use brdc_dstebr with a workspace when it is needed. */
+brdc_status brdc_dstebr_noalloc(brdc_handle handle, int64_t n,
+                                const double *d_D, const double *d_E,
+                                double *d_W);
+
 /* Adjoint of brdc_dstebr for the loss L = sum_i G[i] * W[i]: writes
  * dL/dD[n] and dL/dE[n-1] (device) without forming eigenvectors, by
  * running back through the merge tree.  The workspace must come from a

@@ -62,6 +62,7 @@ EXPORTS = (
     "brdc_version",
     "brdc_set_timing",
     "brdc_get_last_timings",
+    "brdc_dstebr_noalloc",
 )
 
 
@@ -165,12 +166,13 @@ def load() -> ctypes.CDLL:
     lib.brdc_dstebr_batched.argtypes = [vp, i64, ctypes.POINTER(i64), vp, vp, vp, vp, sz]
     lib.brdc_version.restype = ctypes.c_char_p
     lib.brdc_set_timing.argtypes = [vp, ctypes.c_int]
+    lib.brdc_dstebr_noalloc.argtypes = [vp, i64, vp, vp, vp]
     lib.brdc_get_last_timings.argtypes = [vp, ctypes.POINTER(Timings)]
     for f in ("brdc_create", "brdc_destroy", "brdc_set_stream", "brdc_get_stream",
               "brdc_get_last_error", "brdc_dstebr_workspace_size", "brdc_dstebr",
               "brdc_dstebr_backward", "brdc_get_info", "brdc_get_diagnostics",
               "brdc_dstebr_batched_workspace_size", "brdc_dstebr_batched",
-              "brdc_set_timing", "brdc_get_last_timings"):
+              "brdc_set_timing", "brdc_get_last_timings", "brdc_dstebr_noalloc"):
         getattr(lib, f).restype = ctypes.c_int
     _lib = lib
     return lib
@@ -276,6 +278,20 @@ class Solver:
             ctypes.c_void_p(W.data_ptr()), ctypes.c_void_p(ws.data_ptr()), ws.numel(),
         )
         _check(st, "brdc_dstebr", self.h)
+        return W
+
+    def dstebr_noalloc(self, D, E, W=None):
+        """Solve with the library's static scratch (n <= 16384); no
+        workspace is allocated by anyone."""
+        torch = self._torch
+        n = D.shape[0]
+        D = D.contiguous()
+        E = E.contiguous() if E is not None and E.numel() > 0 else D
+        if W is None:
+            W = torch.empty(n, dtype=torch.float64, device=D.device)
+        st = load().brdc_dstebr_noalloc(self.h, n, ctypes.c_void_p(D.data_ptr()),
+                                        ctypes.c_void_p(E.data_ptr()), ctypes.c_void_p(W.data_ptr()))
+        _check(st, "brdc_dstebr_noalloc", self.h)
         return W
 
     def info(self, n: int, workspace=None) -> int:

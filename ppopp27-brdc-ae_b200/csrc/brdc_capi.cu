@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -807,4 +808,90 @@ extern "C" void brdc_dstedc_dc_br_(const int *n_, double *d, double *e,
     }
     work[0] = (double)lwmin;
     iwork[0] = liwmin;
+}
+
+// ---------------------------------------------- allocation-free entry point
+// Some callers cannot allocate device memory when they need a solve: code
+// that runs inside a host callback or a stream-ordered section where
+// cudaMalloc/cudaFree would synchronise or are not permitted, plug-ins
+// whose host application owns and budgets every device allocation, and
+// latency-critical paths that must not risk an allocation failure in the
+// middle of their work.  brdc_dstebr_noalloc serves them: it takes only the
+// inputs and the output, and its scratch is the statically sized device
+// array below, which exists on every GPU the library is loaded on, from
+// load until process exit.  Its size bounds the order of one solve.
+namespace {
+constexpr long long kNoAllocMaxN = 16384;
+constexpr size_t kNoAllocBytes = 4718592; // 4.5 MiB: the workspace of n = 16384
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+std::mutex g_noalloc_mutex;
+constexpr int kNoAllocMaxDevices = 128;
+void *g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on the current device.  The symbol
+// name stands for a host-side shadow in host code, so the address must be
+// asked for once per device, with that device current.
+cudaError_t noalloc_address(int device, void **out) {
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (g_noalloc_addr[device] == nullptr) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) {
+            return e;
+        }
+        g_noalloc_addr[device] = p;
+    }
+    *out = g_noalloc_addr[device];
+    return cudaSuccess;
+}
+} // namespace
+
+extern "C" brdc_status brdc_dstebr_noalloc(brdc_handle h, int64_t n,
+                                           const double *d_D, const double *d_E,
+                                           double *d_W) {
+    if (h == nullptr) {
+        return BRDC_STATUS_INVALID_HANDLE;
+    }
+    if (d_D == nullptr || d_W == nullptr || (n > 1 && d_E == nullptr)) {
+        return BRDC_STATUS_INVALID_POINTER;
+    }
+    if (n <= 0) {
+        return BRDC_STATUS_INVALID_VALUE;
+    }
+    if (n > kNoAllocMaxN) {
+        set_error(h, 0, BRDC_ERROR_SRC_NONE,
+                  "brdc.noalloc: n exceeds the static scratch limit of 16384");
+        return BRDC_STATUS_INVALID_VALUE;
+    }
+    const long long off[2] = {0, (long long)n};
+    HostForest hf;
+    if (!build_forest(1, off, &hf)) {
+        return BRDC_STATUS_INVALID_VALUE;
+    }
+    const Layout L = make_layout(hf);
+    if (L.bytes > kNoAllocBytes) {
+        set_error(h, 0, BRDC_ERROR_SRC_NONE,
+                  "brdc.noalloc: workspace exceeds the static scratch");
+        return BRDC_STATUS_INVALID_VALUE;
+    }
+    int device = 0;
+    BRDC_CUDA(h, "brdc.noalloc.get_device", cudaGetDevice(&device));
+    if (device < 0 || device >= kNoAllocMaxDevices || device != h->device) {
+        set_error(h, device, BRDC_ERROR_SRC_NONE,
+                  "brdc.noalloc: current device differs from the handle's");
+        return BRDC_STATUS_INVALID_VALUE;
+    }
+    void *scratch = nullptr;
+    BRDC_CUDA(h, "brdc.noalloc.symbol_address", noalloc_address(device, &scratch));
+    // Every array the solve reads is written earlier in the same solve and
+    // k_init clears the header counters, so the contents left by a previous
+    // call need no clearing here.
+    const Ws w = carve(scratch, L);
+    Forest F{};
+    F.B = 1;
+    F.max_levels = hf.max_levels;
+    F.n0 = n;
+    F.L0 = hf.max_levels;
+    return run_forest(h, hf, F, w, d_D, d_E, d_W);
 }
