@@ -269,6 +269,9 @@ def main():
             "ms_median": float(np.median(times)),
             "workspace_bytes": ws.numel(),
             "deflation_K_per_level": [lv["dd_after_sum"] for lv in diag["level"]],
+            "secular_iters_per_level": [
+                [round(lv["secular_iter_sum"] / max(lv["dd_after_sum"], 1), 2), lv["secular_iter_max"],
+                 lv["secular_iter_failed"], lv["threads_per_root"]] for lv in diag["level"]],
             "clocks": clocks,
         }
         line.update({k: v for k, v in extras.items() if k != "launches"})

@@ -105,7 +105,7 @@ brdc_status brdc_dstebr(brdc_handle handle, int64_t n, const double *d_D,
  * allowed, plug-ins whose host owns every device allocation, paths that
  * must not meet an allocation failure).  No reference counterpart: the
  * reference solve always takes a caller-allocated workspace.
- *  - Scratch is one static device array of 4.5 MiB inside the library,
+ *  - Scratch is one static device array of 6 MiB inside the library,
  *    present on every GPU that loads it until the process exits; it bounds
  *    n to 16384.  Larger n returns BRDC_STATUS_INVALID_VALUE and records
  *    the reason as the last error.

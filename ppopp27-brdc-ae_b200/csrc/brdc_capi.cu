@@ -1,8 +1,9 @@
 // brdc_capi.cu -- host driver and C ABI (include/brdc.h).
 //
 // The driver plans a forest (one or many tridiagonals), carves the caller's
-// workspace, and enqueues per level: k_merge_deflate, k_secular, k_lowner,
-// k_rows_place.  All launch shapes depend only on the orders, never on data,
+// workspace, and enqueues per level: k_merge, k_merge_deflate, k_secular,
+// k_lowner, k_rows, k_place.  All launch shapes depend only on the orders,
+// never on data,
 // and no call synchronises the stream, so a solve can be captured in a CUDA
 // graph.  Data-dependent sizes (deflation counts K) travel from kernel to
 // kernel through the workspace header; that replaces the per-level device
@@ -121,7 +122,7 @@ enum DArr {
     A_cd, A_cf, A_cl, A_nd, A_nf, A_nl, A_md, A_mz, A_mf, A_ml, A_ad, A_az,
     A_af, A_al, A_gc, A_gs, A_zd, A_zf, A_zl, A_gd, A_gf, A_gl, A_NDN
 };
-enum PArr { P_pd, P_pz, P_pf, P_pl, P_pw, P_rdo, P_rtau, P_rlam, P_NDP };
+enum PArr { P_pd, P_pz, P_pf, P_pl, P_pw, P_rdo, P_rtau, P_rlam, P_rf, P_rl, P_NDP };
 enum IArr { I_mflag, I_morig, I_amap, I_gmark, I_gbase, I_NIN };
 enum QArr { Q_pmap, Q_rorg, Q_NIP };
 
@@ -158,6 +159,10 @@ Layout make_layout(const HostForest &f) {
     cur = align_up(cur + sizeof(int) * (size_t)(L.nn0 + 1));
     L.o_i[I_NIN + Q_NIP + 3] = cur;
     cur = align_up(cur + sizeof(int) * (size_t)(L.nn0 + 1));
+    L.o_i[I_NIN + Q_NIP + 4] = cur;
+    cur = align_up(cur + sizeof(int) * (size_t)(L.nt + L.nn0 + 2));
+    L.o_i[I_NIN + Q_NIP + 5] = cur;
+    cur = align_up(cur + sizeof(int) * (size_t)(L.nt / 8 + L.nn0 + 2));
     L.o_d[A_NDN + P_NDP + 0] = cur;
     cur = align_up(cur + sizeof(double) * (size_t)L.nn0);
     L.o_d[A_NDN + P_NDP + 1] = cur;
@@ -190,7 +195,7 @@ Ws carve(void *base, const Layout &L) {
     for (int i = 0; i < A_NDN; ++i) {
         *dp[i] = reinterpret_cast<double *>(b + L.o_d[i]);
     }
-    double **pp[P_NDP] = {&w.pd, &w.pz, &w.pf, &w.pl, &w.pw, &w.rdo, &w.rtau, &w.rlam};
+    double **pp[P_NDP] = {&w.pd, &w.pz, &w.pf, &w.pl, &w.pw, &w.rdo, &w.rtau, &w.rlam, &w.rf, &w.rl};
     for (int i = 0; i < P_NDP; ++i) {
         *pp[i] = reinterpret_cast<double *>(b + L.o_d[A_NDN + i]);
     }
@@ -202,8 +207,10 @@ Ws carve(void *base, const Layout &L) {
     w.rorg = reinterpret_cast<int *>(b + L.o_i[I_NIN + Q_rorg]);
     w.nK = reinterpret_cast<int *>(b + L.o_i[I_NIN + Q_NIP + 0]);
     w.nKz = reinterpret_cast<int *>(b + L.o_i[I_NIN + Q_NIP + 1]);
-    w.pref_sec = reinterpret_cast<int *>(b + L.o_i[I_NIN + Q_NIP + 2]);
-    w.pref_rows = reinterpret_cast<int *>(b + L.o_i[I_NIN + Q_NIP + 3]);
+    w.pref_w = reinterpret_cast<int *>(b + L.o_i[I_NIN + Q_NIP + 2]);
+    w.pref_c = reinterpret_cast<int *>(b + L.o_i[I_NIN + Q_NIP + 3]);
+    w.items_w = reinterpret_cast<int *>(b + L.o_i[I_NIN + Q_NIP + 4]);
+    w.items_c = reinterpret_cast<int *>(b + L.o_i[I_NIN + Q_NIP + 5]);
     w.nrho = reinterpret_cast<double *>(b + L.o_d[A_NDN + P_NDP + 0]);
     w.ntol = reinterpret_cast<double *>(b + L.o_d[A_NDN + P_NDP + 1]);
     w.nzn = reinterpret_cast<double *>(b + L.o_d[A_NDN + P_NDP + 2]);
@@ -252,7 +259,7 @@ cudaError_t set_attrs() {
                                  (int)smem_tiles(3));
     }
     if (e == cudaSuccess) {
-        e = cudaFuncSetAttribute(k_rows_place,
+        e = cudaFuncSetAttribute(k_rows,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem_tiles(4));
     }
@@ -290,7 +297,7 @@ brdc_status run_forest(brdc_handle h, const HostForest &hf, const Forest &F,
     a.E = E;
     a.W = W;
     {
-        const long long per = (long long)kLeafWarps;
+        const long long per = 2LL * kLeafWarps; // leaves per block
         long long grid = (hf.leaves + per - 1) / per;
         grid = std::min<long long>(grid, (long long)h->sm_count * 16);
         grid = std::max<long long>(grid, 1);
@@ -299,18 +306,26 @@ brdc_status run_forest(brdc_handle h, const HostForest &hf, const Forest &F,
         ++h->launches;
         mark(h, 2);
     }
-    const int sweep_grid = h->sm_count * 3;
+    const int warp_blocks = h->sm_count * 2;
+    long long elem_grid = (hf.total_n + 255) / 256;
+    elem_grid = std::max<long long>(1, std::min<long long>(elem_grid, (long long)h->sm_count * 8));
     for (int k = 0; k < hf.max_levels; ++k) {
         a.k = k;
         a.nodes = hf.level_nodes[k];
+        // CTA-role blocks exist only where a merge can exceed kWarpMaxK poles
+        const int cta_blocks = hf.level_mmax[k] > kWarpMaxK ? h->sm_count * 2 : 0;
+        const int grid = cta_blocks + warp_blocks;
+        k_merge<<<(unsigned)elem_grid, 256, 0, s>>>(a, hf.total_n);
+        BRDC_CUDA(h, "brdc.merge", cudaGetLastError());
         launch_merge_deflate(a, hf.level_mmax[k], s);
         BRDC_CUDA(h, "brdc.merge_deflate", cudaGetLastError());
-        mark(h, 3 + 4 * k);
-        k_secular<<<sweep_grid, kSweepThreads, smem_tiles(2), s>>>(a);
-        BRDC_CUDA(h, "brdc.secular", cudaGetLastError());
-        mark(h, 4 + 4 * k);
         h->launches += 2;
-        // Loewner z is needed unless every merge of this level is a root
+        mark(h, 3 + 4 * k);
+        k_secular<<<grid, kSweepThreads, cta_blocks ? smem_tiles(2) : 0, s>>>(a, cta_blocks);
+        BRDC_CUDA(h, "brdc.secular", cudaGetLastError());
+        ++h->launches;
+        mark(h, 4 + 4 * k);
+        // rows are needed unless every merge of this level is an instance root
         bool any_inner = false;
         for (int b = 0; b < hf.B; ++b) {
             if (hf.lev[b] - 1 > k) {
@@ -320,13 +335,18 @@ brdc_status run_forest(brdc_handle h, const HostForest &hf, const Forest &F,
         }
         h->has_lowner[k] = any_inner ? 1 : 0;
         if (any_inner) {
-            k_lowner<<<sweep_grid, kSweepThreads, smem_tiles(3), s>>>(a);
+            k_lowner<<<grid, kSweepThreads, cta_blocks ? smem_tiles(3) : 0, s>>>(a, cta_blocks);
             BRDC_CUDA(h, "brdc.lowner", cudaGetLastError());
             ++h->launches;
         }
         mark(h, 5 + 4 * k);
-        k_rows_place<<<sweep_grid, kSweepThreads, smem_tiles(4), s>>>(a);
-        BRDC_CUDA(h, "brdc.rows_place", cudaGetLastError());
+        if (any_inner) {
+            k_rows<<<grid, kSweepThreads, cta_blocks ? smem_tiles(4) : 0, s>>>(a, cta_blocks);
+            BRDC_CUDA(h, "brdc.rows", cudaGetLastError());
+            ++h->launches;
+        }
+        k_place<<<(unsigned)elem_grid, 256, 0, s>>>(a, hf.total_n);
+        BRDC_CUDA(h, "brdc.place", cudaGetLastError());
         ++h->launches;
         mark(h, 6 + 4 * k);
         std::swap(a.w.cd, a.w.nd);
@@ -822,7 +842,7 @@ extern "C" void brdc_dstedc_dc_br_(const int *n_, double *d, double *e,
 // load until process exit.  Its size bounds the order of one solve.
 namespace {
 constexpr long long kNoAllocMaxN = 16384;
-constexpr size_t kNoAllocBytes = 4718592; // 4.5 MiB: the workspace of n = 16384
+constexpr size_t kNoAllocBytes = 6291456; // 6 MiB: the workspace of n = 16384 plus headroom
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
 std::mutex g_noalloc_mutex;

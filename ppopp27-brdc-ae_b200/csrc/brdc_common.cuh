@@ -38,6 +38,7 @@ namespace brdc {
 constexpr int kLeafMax = 16;
 constexpr int kSweepThreads = 256;  // threads per CTA of the sweep kernels
 constexpr int kTile = 1024;         // poles per shared-memory tile
+constexpr int kWarpMaxK = 2048;     // merges up to this K run one warp per item
 constexpr double kDeflTolScale = 8.0;  // tol = 8*eps*max(max|d|,max|z|)
                                         // (merge_kernels.cuh:9-11,1090-1091)
 constexpr unsigned kWsMagic = 0x42524443u; // "BRDC"
@@ -58,12 +59,13 @@ inline int tree_levels(long long n) {
 // Per-level control block written by the kernels.
 struct LevelCtl {
     int ticket;      // CTAs of the merge kernel that finished
-    int nodes;       // merges at this level (set by the host)
-    int tpr;         // lanes per root chosen for the sweeps
-    int items_sec;   // work items of the secular / Loewner kernels
-    int items_rows;  // work items of the row / placement kernel
+    int nodes;       // merges at this level
+    int tpr_w;       // lanes per root, warp-role merges (K <= kWarpMaxK)
+    int tpr_c;       // lanes per root, CTA-role merges (K > kWarpMaxK)
+    int items_w;     // warp work items of the level
+    int items_c;     // CTA work items of the level
     int total_k;
-    int pad[2];
+    int pad;
 };
 
 struct WsHeader {
@@ -123,7 +125,9 @@ struct Ws {
     // per node at one level
     int *nK, *nKz;
     double *nrho, *ntol, *nzn;
-    int *pref_sec, *pref_rows;
+    int *pref_w, *pref_c;        // first work item of each merge (per role)
+    int *items_w, *items_c;      // work item -> merge node (per role)
+    double *rf, *rl;             // new boundary rows of each root (padded)
     // forest tables (batched)
     long long *f_off;
     int *f_lev, *f_node_prefix, *f_leaf_prefix;
@@ -208,6 +212,51 @@ __device__ inline NodeGeom node_geom(const Forest &F, int k, int g) {
     G.m1 = (int)(s >> 1);
     G.poff = (G.gstart + g + 1) & ~1LL;
     return G;
+}
+
+// Merge node at forest level k that contains global row x.  Returns false
+// when the row's instance has no merge at this level.
+__device__ inline bool elem_node(const Forest &F, int k, long long x, int *g,
+                                 long long *gstart, int *m, int *depth_out) {
+    long long base = 0, n = F.n0;
+    int L = F.L0, pre = 0;
+    if (F.B > 1) {
+        int lo = 0, hi = F.B; // last b with off[b] <= x
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (F.off[mid] <= x) {
+                lo = mid;
+            } else {
+                hi = mid;
+            }
+        }
+        base = F.off[lo];
+        n = F.off[lo + 1] - base;
+        L = F.lev[lo];
+        pre = F.node_prefix[(size_t)k * (F.B + 1) + lo];
+    }
+    if (L <= k) {
+        return false;
+    }
+    const int depth = L - 1 - k;
+    long long st = 0, s = n, idx = 0;
+    const long long r = x - base;
+    for (int t = 0; t < depth; ++t) {
+        const long long h = s >> 1;
+        if (r - st >= h) {
+            st += h;
+            s -= h;
+            idx = 2 * idx + 1;
+        } else {
+            s = h;
+            idx = 2 * idx;
+        }
+    }
+    *g = pre + (int)idx;
+    *gstart = base + st;
+    *m = (int)s;
+    *depth_out = depth;
+    return true;
 }
 
 struct LeafGeom {

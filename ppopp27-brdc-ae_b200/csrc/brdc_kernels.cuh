@@ -1,16 +1,20 @@
 // brdc_kernels.cuh -- sm_100a kernels of the forward BR solve.
 //
-// One forest level runs four kernels:
-//   k_merge_deflate  one CTA per merge: z from the children's boundary rows,
-//                    merge of the two sorted child spectra, small-z and
-//                    close-pole deflation with Givens rotations of z and of
-//                    both boundary rows, compaction, work plan of the level
-//   k_secular        secular roots, TPR lanes per root, pole tiles staged in
+// One forest level runs six kernels:
+//   k_merge          one thread per row: rank merge of the two sorted child
+//                    spectra, z from the children's boundary rows
+//   k_merge_deflate  one CTA per merge: small-z and close-pole deflation
+//                    with Givens rotations of z and of both boundary rows,
+//                    compaction, work plan of the level
+//   k_secular        secular roots, TPR lanes per root; merges with K <=
+//                    kWarpMaxK one warp per work item (poles through L1),
+//                    larger ones one CTA per item with pole tiles staged in
 //                    shared memory by cp.async.bulk
-//   k_lowner         Loewner / Gu-Eisenstat recomputation of z
-//   k_rows_place     first/last rows of the merged eigenvector matrix for
-//                    every root, and the final sorted placement of all
-//                    eigenvalues of the node
+//   k_lowner         Loewner / Gu-Eisenstat recomputation of z (same roles)
+//   k_rows           first/last rows of the merged eigenvector matrix for
+//                    every root (same roles)
+//   k_place          one thread per row: every eigenvalue of a node to its
+//                    place in the node's ascending spectrum
 // The leaves are solved first by k_leaf (one warp per leaf, parallel
 // cyclic Jacobi).
 #pragma once
@@ -34,180 +38,213 @@ struct KArgs {
 };
 
 // ------------------------------------------------------------------ leaves
-// One warp per leaf of <= 16 rows.  The leaf matrix (with the rank-one cut
-// corrections D -= |E_cut| at both ends, gpu/src/tridiag_solver_extract.cuh:
-// 104-117) is diagonalised by cyclic Jacobi with the round-robin ordering:
-// 8 disjoint rotations per round, 15 rounds per sweep, applied by all 32
-// lanes at once.  The reference runs a serial Jacobi on one thread per leaf
-// (gpu/src/tridiag_solver_leaf.cuh:56-123).  Output: ascending eigenvalues,
-// and the first and last rows of the eigenvector matrix in that order.
+// Leaves of <= 16 rows, two per warp (one per half-warp), by parallel
+// cyclic Jacobi, as the reference solves its leaves by Jacobi
+// (gpu/src/tridiag_solver_leaf.cuh:56-123, one thread per leaf there).
+//
+// Lane x of a half-warp owns column x of the 16x16 leaf matrix in
+// registers, stored XOR-skewed: reg[j] = A[x^j][x].  Sweep m = 1..15 of the
+// XOR tournament pairs index x with x^m (every pair exactly once per sweep),
+// so in round m: the diagonal is reg[0], the entry to annihilate is reg[m],
+// the two rows a rotation mixes in my column are reg[j] and reg[j^m], and
+// the partner column's entry of the same row is the partner lane's
+// reg[j^m] -- all compile-time register indices, exchanged by
+// __shfl_xor_sync.  Only the first and last rows of the eigenvector matrix
+// are accumulated (two values per lane).  The rank-one cut corrections
+// D -= |E_cut| at both ends (gpu/src/tridiag_solver_extract.cuh:104-117) are
+// applied on load.  Output: ascending eigenvalues with the first and last
+// rows in that order.
 constexpr int kLeafWarps = 4;
-constexpr int kLeafLd = 17;
+constexpr unsigned kFull = 0xffffffffu;
+
+template <int M>
+__device__ __forceinline__ void leaf_round(double (&a)[16], double &v0,
+                                           double &v1, int x, double th) {
+    const bool isp = x < (x ^ M);
+    const double mydiag = a[0];
+    const double odiag = __shfl_xor_sync(kFull, mydiag, M);
+    const double apq_mine = a[M];
+    const double app = isp ? mydiag : odiag;
+    const double aqq = isp ? odiag : mydiag;
+    double c = 1.0, sn = 0.0, t = 0.0;
+    int rot = 0;
+    if (fabs(apq_mine) > th) {
+        const double theta = (aqq - app) / (2.0 * apq_mine);
+        if (fabs(theta) > 1.0e150) {
+            t = 0.5 / theta;
+        } else {
+            t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+        }
+        c = 1.0 / sqrt(t * t + 1.0);
+        sn = t * c;
+        rot = 1;
+    }
+    // the lane holding the larger index adopts its partner's rotation, so
+    // both columns of a pair turn by exactly the same plane rotation
+    {
+        const double co = __shfl_xor_sync(kFull, c, M);
+        const double so = __shfl_xor_sync(kFull, sn, M);
+        const double to = __shfl_xor_sync(kFull, t, M);
+        const int ro = __shfl_xor_sync(kFull, rot, M);
+        if (!isp) {
+            c = co;
+            sn = so;
+            t = to;
+            rot = ro;
+        }
+    }
+    const double apq_o = __shfl_xor_sync(kFull, apq_mine, M);
+    const double apq = isp ? apq_mine : apq_o;
+    // columns: B = A J  (col p: c*col_p - s*col_q, col q: s*col_p + c*col_q)
+    const double sgx = isp ? -1.0 : 1.0;
+    double b[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        const double other = __shfl_xor_sync(kFull, a[j ^ M], M);
+        b[j] = c * a[j] + sgx * sn * other;
+    }
+    {
+        const double o0 = __shfl_xor_sync(kFull, v0, M);
+        const double o1 = __shfl_xor_sync(kFull, v1, M);
+        v0 = c * v0 + sgx * sn * o0;
+        v1 = c * v1 + sgx * sn * o1;
+    }
+    // rows: A' = J^T B; rows x^j and x^j^M use the rotation of lane x^j
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        if (j < (j ^ M)) {
+            const int jj = j ^ M;
+            const double cr = __shfl_xor_sync(kFull, c, j);
+            const double sr = __shfl_xor_sync(kFull, sn, j);
+            const int r = x ^ j;
+            const double sgr = (r < (r ^ M)) ? -1.0 : 1.0;
+            const double bj = b[j], bjj = b[jj];
+            a[j] = cr * bj + sgr * sr * bjj;
+            a[jj] = cr * bjj - sgr * sr * bj;
+        }
+    }
+    if (rot) {
+        a[0] = isp ? app - t * apq : aqq + t * apq;
+        a[M] = 0.0;
+    }
+}
+
+__device__ __forceinline__ double half_max(double v) {
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) {
+        v = fmax(v, __shfl_xor_sync(kFull, v, o));
+    }
+    return v;
+}
 
 __global__ void __launch_bounds__(kLeafWarps * 32)
     k_leaf(KArgs a, long long total_leaves) {
-    __shared__ double sA[kLeafWarps][16 * kLeafLd];
-    __shared__ double sV[kLeafWarps][16 * kLeafLd];
-    __shared__ int sPart[kLeafWarps][16];
-    __shared__ double sC[kLeafWarps][16];
-    __shared__ double sS[kLeafWarps][16];
-    __shared__ double sDiag[kLeafWarps][16];
-    __shared__ int sRot[kLeafWarps][16];
-
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    double *A = sA[warp];
-    double *V = sV[warp];
+    const int lane = threadIdx.x & 31;
+    const int x = lane & 15;
+    const int half = lane >> 4;
     const double eps = DBL_EPSILON;
     int sweeps_max = 0;
-
-    for (long long leaf = (long long)blockIdx.x * kLeafWarps + warp;
-         leaf < total_leaves; leaf += (long long)gridDim.x * kLeafWarps) {
-        const LeafGeom G = leaf_geom(a.F, leaf);
-        const int s = G.s;
-        for (int e = lane; e < 256; e += 32) {
-            const int r = e >> 4, c = e & 15;
-            A[r * kLeafLd + c] = 0.0;
-            V[r * kLeafLd + c] = (r == c) ? 1.0 : 0.0;
+    const long long pairs = (total_leaves + 1) / 2;
+    for (long long pr = (long long)blockIdx.x * kLeafWarps + (threadIdx.x >> 5); pr < pairs;
+         pr += (long long)gridDim.x * kLeafWarps) {
+        const long long leaf = 2 * pr + half;
+        const bool has = leaf < total_leaves;
+        LeafGeom G{};
+        int s = 0;
+        if (has) {
+            G = leaf_geom(a.F, leaf);
+            s = G.s;
         }
-        __syncwarp();
-        double amax = 0.0;
-        if (lane < s) {
-            double dv = a.D[G.gstart + lane];
-            if (lane == 0 && G.gstart > G.istart) {
-                dv -= fabs(a.E[G.gstart - 1]);
+        double dx = 0.0, ex = 0.0, exm1 = 0.0;
+        if (x < s) {
+            dx = a.D[G.gstart + x];
+            if (x == 0 && G.gstart > G.istart) {
+                dx -= fabs(a.E[G.gstart - 1]);
             }
-            if (lane == s - 1 && G.gstart + s < G.iend) {
-                dv -= fabs(a.E[G.gstart + s - 1]);
+            if (x == s - 1 && G.gstart + s < G.iend) {
+                dx -= fabs(a.E[G.gstart + s - 1]);
             }
-            A[lane * kLeafLd + lane] = dv;
-            amax = fabs(dv);
-            if (lane + 1 < s) {
-                const double ev = fabs(a.E[G.gstart + lane]);
-                A[lane * kLeafLd + lane + 1] = ev;
-                A[(lane + 1) * kLeafLd + lane] = ev;
-                amax = fmax(amax, ev);
+            if (x + 1 < s) {
+                ex = fabs(a.E[G.gstart + x]);
+            }
+            if (x >= 1) {
+                exm1 = fabs(a.E[G.gstart + x - 1]);
             }
         }
-        amax = warp_max(amax);
-        __syncwarp();
-        const double thresh = 1.0e-3 * eps * amax;
-
+        double reg[16];
+        const int jup = x ^ (x + 1);
+        const int jdn = x ^ (x - 1);
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            reg[j] = (j == 0) ? dx : ((j == jup) ? ex : ((j == jdn) ? exm1 : 0.0));
+        }
+        double v0 = (x == 0 && s > 0) ? 1.0 : 0.0;
+        double v1 = (x == s - 1) ? 1.0 : 0.0;
+        const double amax = half_max(fmax(fabs(dx), fmax(ex, exm1)));
+        const double th = 1.0e-3 * eps * amax;
         int sweep = 0;
         for (; sweep < 40; ++sweep) {
             double off = 0.0;
-            for (int e = lane; e < 256; e += 32) {
-                const int r = e >> 4, c = e & 15;
-                if (r != c) {
-                    off = fmax(off, fabs(A[r * kLeafLd + c]));
-                }
+#pragma unroll
+            for (int j = 1; j < 16; ++j) {
+                off = fmax(off, fabs(reg[j]));
             }
-            off = warp_max(off);
-            if (!(off > thresh)) {
+            off = half_max(off);
+            if (!__any_sync(kFull, off > th)) {
                 break;
             }
-            for (int round = 0; round < 15; ++round) {
-                if (lane < 8) {
-                    int pa, pb;
-                    if (lane == 0) {
-                        pa = round;
-                        pb = 15;
-                    } else {
-                        pa = (round + lane) % 15;
-                        pb = (round + 15 - lane) % 15;
-                    }
-                    const int p = pa < pb ? pa : pb;
-                    const int q = pa < pb ? pb : pa;
-                    const double apq = A[p * kLeafLd + q];
-                    const double app = A[p * kLeafLd + p];
-                    const double aqq = A[q * kLeafLd + q];
-                    double c = 1.0, sn = 0.0, t = 0.0;
-                    int rot = 0;
-                    if (fabs(apq) > thresh) {
-                        const double theta = (aqq - app) / (2.0 * apq);
-                        if (fabs(theta) > 1.0e150) {
-                            t = 0.5 / theta;
-                        } else {
-                            t = (theta >= 0.0 ? 1.0 : -1.0) /
-                                (fabs(theta) + sqrt(theta * theta + 1.0));
-                        }
-                        c = 1.0 / sqrt(t * t + 1.0);
-                        sn = t * c;
-                        rot = 1;
-                    }
-                    sPart[warp][p] = q;
-                    sPart[warp][q] = p;
-                    sC[warp][p] = c;
-                    sC[warp][q] = c;
-                    sS[warp][p] = -sn; // J(q,p)
-                    sS[warp][q] = sn;  // J(p,q)
-                    sRot[warp][p] = rot;
-                    sRot[warp][q] = rot;
-                    sDiag[warp][p] = app - t * apq;
-                    sDiag[warp][q] = aqq + t * apq;
-                }
-                __syncwarp();
-                double na[8], nv[8];
-#pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    const int e = lane + 32 * u;
-                    const int r = e >> 4, c = e & 15;
-                    const int rb = sPart[warp][r], cb = sPart[warp][c];
-                    const double cr = sC[warp][r], sr = sS[warp][r];
-                    const double cc = sC[warp][c], sc = sS[warp][c];
-                    double v;
-                    if (r == c) {
-                        v = sRot[warp][r] ? sDiag[warp][r] : A[r * kLeafLd + r];
-                    } else if (c == rb) {
-                        v = sRot[warp][r] ? 0.0 : A[r * kLeafLd + c];
-                    } else {
-                        v = cr * (A[r * kLeafLd + c] * cc + A[r * kLeafLd + cb] * sc) +
-                            sr * (A[rb * kLeafLd + c] * cc + A[rb * kLeafLd + cb] * sc);
-                    }
-                    na[u] = v;
-                    nv[u] = V[r * kLeafLd + c] * cc + V[r * kLeafLd + cb] * sc;
-                }
-                __syncwarp();
-#pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    const int e = lane + 32 * u;
-                    const int r = e >> 4, c = e & 15;
-                    A[r * kLeafLd + c] = na[u];
-                    V[r * kLeafLd + c] = nv[u];
-                }
-                __syncwarp();
-            }
+            leaf_round<1>(reg, v0, v1, x, th);
+            leaf_round<2>(reg, v0, v1, x, th);
+            leaf_round<3>(reg, v0, v1, x, th);
+            leaf_round<4>(reg, v0, v1, x, th);
+            leaf_round<5>(reg, v0, v1, x, th);
+            leaf_round<6>(reg, v0, v1, x, th);
+            leaf_round<7>(reg, v0, v1, x, th);
+            leaf_round<8>(reg, v0, v1, x, th);
+            leaf_round<9>(reg, v0, v1, x, th);
+            leaf_round<10>(reg, v0, v1, x, th);
+            leaf_round<11>(reg, v0, v1, x, th);
+            leaf_round<12>(reg, v0, v1, x, th);
+            leaf_round<13>(reg, v0, v1, x, th);
+            leaf_round<14>(reg, v0, v1, x, th);
+            leaf_round<15>(reg, v0, v1, x, th);
         }
         sweeps_max = sweeps_max > sweep ? sweeps_max : sweep;
 
-        // bitonic sort of (eigenvalue, column) over the 32 lanes
-        double key = (lane < s) ? A[lane * kLeafLd + lane] : INFINITY;
-        int col = lane;
-        for (int size = 2; size <= 32; size <<= 1) {
+        // bitonic sort of (eigenvalue, column) within the half-warp
+        double key = (x < s) ? reg[0] : INFINITY;
+        int col = x;
+#pragma unroll
+        for (int size = 2; size <= 16; size <<= 1) {
+#pragma unroll
             for (int stride = size >> 1; stride > 0; stride >>= 1) {
-                const double ok = __shfl_xor_sync(0xffffffffu, key, stride);
-                const int oc = __shfl_xor_sync(0xffffffffu, col, stride);
-                const bool up = ((lane & size) == 0);
-                const bool lower = ((lane & stride) == 0);
+                const double ok = __shfl_xor_sync(kFull, key, stride);
+                const int oc = __shfl_xor_sync(kFull, col, stride);
+                const double o0 = __shfl_xor_sync(kFull, v0, stride);
+                const double o1 = __shfl_xor_sync(kFull, v1, stride);
+                const bool up = (size == 16) || ((x & size) == 0);
+                const bool lower = ((x & stride) == 0);
                 const bool take_min = (up == lower);
                 const bool swap = take_min ? (ok < key || (ok == key && oc < col))
                                            : (ok > key || (ok == key && oc > col));
                 if (swap) {
                     key = ok;
                     col = oc;
+                    v0 = o0;
+                    v1 = o1;
                 }
             }
         }
-        if (lane < s) {
-            const long long o = G.gstart + lane;
+        if (x < s) {
+            const long long o = G.gstart + x;
             if (G.top) {
                 a.W[o] = key;
             } else {
                 a.w.cd[o] = key;
-                a.w.cf[o] = V[0 * kLeafLd + col];
-                a.w.cl[o] = V[(s - 1) * kLeafLd + col];
+                a.w.cf[o] = v0;
+                a.w.cl[o] = v1;
             }
         }
-        __syncwarp();
     }
     if (lane == 0 && sweeps_max > 0) {
         atomicMax(&a.w.hdr->leaf_sweeps_max, sweeps_max);
@@ -226,6 +263,52 @@ __global__ void __launch_bounds__(kLeafWarps * 32)
 // The rotation is applied to both boundary rows with the same orientation
 // as to z (new_b = c*b + s*t, new_t = -s*b + c*t), so the parent rows stay
 // consistent with the rotated z.
+// Rank merge of the two sorted child spectra of every merge of the level,
+// one thread per row: a row of the left child lands at its own index plus
+// the number of right-child poles below it, a right-child row at its index
+// plus the left-child poles at or below it (left wins ties).  Writes the
+// merged d, z = (last row of the left child | first row of the right
+// child)/sqrt2, and the block-diagonal projections of the parent's first
+// and last rows.
+__global__ void __launch_bounds__(256) k_merge(KArgs a, long long total_n) {
+    const Ws &w = a.w;
+    const double isq2 = 0.70710678118654752440;
+    for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x; x < total_n;
+         x += (long long)gridDim.x * blockDim.x) {
+        int g, m, depth;
+        long long gs;
+        if (!elem_node(a.F, a.k, x, &g, &gs, &m, &depth)) {
+            continue;
+        }
+        const int m1 = m >> 1, m2 = m - m1;
+        const int e = (int)(x - gs);
+        const double *Ad = w.cd + gs;
+        const double *Bd = w.cd + gs + m1;
+        double xv, z, f, l;
+        int pos;
+        if (e < m1) {
+            xv = Ad[e];
+            pos = e + lower_bound_d(Bd, m2, xv);
+            z = w.cl[x] * isq2;
+            f = w.cf[x];
+            l = 0.0;
+        } else {
+            const int j = e - m1;
+            xv = Bd[j];
+            pos = j + upper_bound_d(Ad, m1, xv);
+            z = w.cf[x] * isq2;
+            f = 0.0;
+            l = w.cl[x];
+        }
+        const long long o = gs + pos;
+        w.md[o] = xv;
+        w.mz[o] = z;
+        w.mf[o] = f;
+        w.ml[o] = l;
+        w.morig[o] = e;
+    }
+}
+
 template <int T>
 __global__ void __launch_bounds__(T) k_merge_deflate(KArgs a) {
     __shared__ double red[32];
@@ -237,7 +320,6 @@ __global__ void __launch_bounds__(T) k_merge_deflate(KArgs a) {
     const long long gs = G.gstart;
     const int m = G.m, m1 = G.m1, m2 = G.m - G.m1;
     const double eps = DBL_EPSILON;
-    const double isq2 = 0.70710678118654752440;
 
     const double *Ad = w.cd + gs;
     const double *Bd = w.cd + gs + m1;
@@ -246,39 +328,10 @@ __global__ void __launch_bounds__(T) k_merge_deflate(KArgs a) {
                        fmax(fabs(Bd[0]), fabs(Bd[m2 - 1])));
     double lz = 0.0;
     for (int e = threadIdx.x; e < m; e += T) {
-        const double z = (e < m1) ? w.cl[gs + e] * isq2 : w.cf[gs + e] * isq2;
-        lz = fmax(lz, fabs(z));
+        lz = fmax(lz, fabs(w.mz[gs + e]));
     }
     const double maxz = block_max<T>(lz, red);
     const double tol = kDeflTolScale * eps * fmax(maxd, maxz);
-
-    // merge of the two sorted child lists by rank in the sibling
-    for (int e = threadIdx.x; e < m; e += T) {
-        double x, z, f, l;
-        int pos;
-        if (e < m1) {
-            x = Ad[e];
-            pos = e + lower_bound_d(Bd, m2, x);
-            z = w.cl[gs + e] * isq2;
-            f = w.cf[gs + e];
-            l = 0.0;
-        } else {
-            const int j = e - m1;
-            x = Bd[j];
-            pos = j + upper_bound_d(Ad, m1, x);
-            z = w.cf[gs + e] * isq2;
-            f = 0.0;
-            l = w.cl[gs + e];
-        }
-        const long long o = gs + pos;
-        w.md[o] = x;
-        w.mz[o] = z;
-        w.mf[o] = f;
-        w.ml[o] = l;
-        w.mflag[o] = fabs(rho * z) > tol ? 1 : 0;
-        w.morig[o] = e;
-    }
-    __syncthreads();
 
     // compaction 1: small-z survivors (sorted) and small-z deflated (sorted)
     int carry_a = 0, carry_z = 0;
@@ -288,7 +341,7 @@ __global__ void __launch_bounds__(T) k_merge_deflate(KArgs a) {
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int idx = base + 4 * threadIdx.x + q;
-            fl[q] = (idx < m) ? w.mflag[gs + idx] : 0;
+            fl[q] = (idx < m) ? (fabs(rho * w.mz[gs + idx]) > tol) : 0;
             cnt += fl[q];
         }
         int tot;
@@ -447,48 +500,91 @@ __global__ void __launch_bounds__(T) k_merge_deflate(KArgs a) {
     if (!s_last) {
         return;
     }
-    // Last CTA of the level: work plan of the sweep kernels.
+    // Last CTA of the level: work plan of the sweep kernels.  Merges with
+    // K <= kWarpMaxK are served one warp per work item; larger ones by whole
+    // CTAs that stage pole tiles in shared memory.
     __threadfence();
-    long long tk = 0;
+    double tkw = 0.0, tkc = 0.0, cw = 0.0, cc = 0.0;
     for (int i = threadIdx.x; i < a.nodes; i += T) {
-        tk += ((volatile int *)w.nK)[i];
+        const int kk = ((volatile int *)w.nK)[i];
+        if (kk > kWarpMaxK) {
+            tkc += kk;
+            cc += 1.0;
+        } else if (kk > 0) {
+            tkw += kk;
+            cw += 1.0;
+        }
     }
-    const double totk = block_sum<T>((double)tk, red);
-    const double target = 148.0 * 2048.0;
-    int tpr = 1;
-    while (tpr < 32 && (double)tpr * totk < target) {
-        tpr <<= 1;
+    tkw = block_sum<T>(tkw, red);
+    tkc = block_sum<T>(tkc, red);
+    cw = block_sum<T>(cw, red);
+    cc = block_sum<T>(cc, red);
+    // warp role: each root's sweeps form a serial latency chain, so spread
+    // the roots over enough lanes to keep every scheduler busy (~75k
+    // threads); with one root per warp the warp also never diverges.
+    int tpr_w = 1;
+    while (tpr_w < 32 && (double)tpr_w * tkw < 75776.0) {
+        tpr_w <<= 1;
     }
-    const int R = kSweepThreads / tpr;
-    int carry_s = 0, carry_r = 0;
+    // CTA role: enough lanes to fill the GPU (~75k threads), at least ~16
+    // poles per lane and sweep
+    const double kavg_c = tkc / fmax(cc, 1.0);
+    int tpr_c = 1;
+    while (tpr_c < 32 && (double)tpr_c * tkc < 75776.0) {
+        tpr_c <<= 1;
+    }
+    int cap = 1;
+    while (cap < 32 && (double)(cap * 2) * 16.0 <= kavg_c) {
+        cap <<= 1;
+    }
+    tpr_c = tpr_c < cap ? tpr_c : cap;
+    const int Rw = 32 / tpr_w;
+    const int Rc = kSweepThreads / tpr_c;
+    int carry_w = 0, carry_c = 0;
     for (int base = 0; base < a.nodes; base += T) {
         const int i = base + threadIdx.x;
-        int is = 0, ir = 0;
+        int iw = 0, ic = 0;
         if (i < a.nodes) {
             const int kk = ((volatile int *)w.nK)[i];
-            const NodeGeom Gi = node_geom(a.F, a.k, i);
-            is = (kk + R - 1) / R;
-            ir = (Gi.m + R - 1) / R;
+            if (kk > kWarpMaxK) {
+                ic = (kk + Rc - 1) / Rc;
+            } else {
+                iw = (kk + Rw - 1) / Rw;
+            }
         }
-        int ts, tr;
-        const int es = block_exscan<T>(is, iscan, &ts);
-        const int er = block_exscan<T>(ir, iscan, &tr);
+        int tw, tc;
+        const int ew = block_exscan<T>(iw, iscan, &tw);
+        const int ec = block_exscan<T>(ic, iscan, &tc);
         if (i < a.nodes) {
-            w.pref_sec[i] = carry_s + es;
-            w.pref_rows[i] = carry_r + er;
+            w.pref_w[i] = carry_w + ew;
+            w.pref_c[i] = carry_c + ec;
         }
-        carry_s += ts;
-        carry_r += tr;
+        carry_w += tw;
+        carry_c += tc;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < a.nodes; i += T) {
+        const int s0 = w.pref_w[i];
+        const int s1 = (i + 1 < a.nodes) ? w.pref_w[i + 1] : carry_w;
+        for (int q = s0; q < s1; ++q) {
+            w.items_w[q] = i;
+        }
+        const int c0 = w.pref_c[i];
+        const int c1 = (i + 1 < a.nodes) ? w.pref_c[i + 1] : carry_c;
+        for (int q = c0; q < c1; ++q) {
+            w.items_c[q] = i;
+        }
     }
     if (threadIdx.x == 0) {
-        w.pref_sec[a.nodes] = carry_s;
-        w.pref_rows[a.nodes] = carry_r;
+        w.pref_w[a.nodes] = carry_w;
+        w.pref_c[a.nodes] = carry_c;
         LevelCtl *c = &w.hdr->lvl[a.k];
-        c->tpr = tpr;
-        c->items_sec = carry_s;
-        c->items_rows = carry_r;
-        c->total_k = (int)totk;
-        w.hdr->diag[a.k].threads_per_root = tpr;
+        c->tpr_w = tpr_w;
+        c->tpr_c = tpr_c;
+        c->items_w = carry_w;
+        c->items_c = carry_c;
+        c->total_k = (int)(tkw + tkc);
+        w.hdr->diag[a.k].threads_per_root = carry_c > 0 ? tpr_c : tpr_w;
     }
 }
 
@@ -601,68 +697,225 @@ __device__ inline void record_error(WsHeader *h, int code) {
     atomicCAS(&h->status, 0, code);
 }
 
-// Item -> node lookup shared through shared memory.
-__device__ inline int item_node(const int *pref, int nodes, int item, int *s_node) {
+// Item -> node lookup (table written by the level plan).
+__device__ inline int item_node(const int *table, int item) {
     __syncthreads();
-    if (threadIdx.x == 0) {
-        *s_node = upper_bound_int(pref, nodes + 1, item) - 1;
-    }
-    __syncthreads();
-    return *s_node;
+    return table[item];
 }
 
-// ---------------------------------------------------------------- roots
-__global__ void __launch_bounds__(kSweepThreads)
-    k_secular(KArgs a) {
-    extern __shared__ __align__(16) double smem[];
-    __shared__ __align__(8) uint64_t bars[2];
-    __shared__ int s_node;
-    const Ws &w = a.w;
-    const LevelCtl *ctl = &w.hdr->lvl[a.k];
-    const int tpr = ctl->tpr;
-    const int R = kSweepThreads / tpr;
-    const int items = ctl->items_sec;
-    const int grp = threadIdx.x / tpr, lane = threadIdx.x % tpr;
-    const double eps = DBL_EPSILON;
+// Per-root / per-pole work of the three sweep phases, shared by the two
+// roles.  The warp role reads poles through L1 (__ldg); the CTA role reads
+// them from shared-memory tiles.
 
+struct RootIO {
+    const Ws *w;
+    long long po;
+    int K;
+};
+
+__device__ inline void secular_store(const Ws &w, const KArgs &a, long long po,
+                                     int r, const SecRoot &st) {
+    const long long o = po + r;
+    w.rorg[o] = st.org;
+    w.rdo[o] = st.dorg;
+    w.rtau[o] = st.tau;
+    w.rlam[o] = st.dorg + st.tau;
+    brdc_level_diagnostics *dg = &w.hdr->diag[a.k];
+    atomicAdd(&dg->secular_iter_sum, st.iter);
+    atomicMax(&dg->secular_iter_max, st.iter);
+    if (st.failed) {
+        atomicAdd(&dg->secular_iter_failed, 1);
+        atomicAdd(&w.hdr->nonconv, 1);
+    }
+}
+
+__device__ inline void secular_single(const Ws &w, long long po, double rho) {
+    const double z0 = w.pz[po];
+    const double t = rho * z0 * z0;
+    w.rorg[po] = 0;
+    w.rdo[po] = w.pd[po];
+    w.rtau[po] = t;
+    w.rlam[po] = w.pd[po] + t;
+}
+
+// Sums of one root over poles [j0, j0+cnt) taken with stride tpr from lane
+// l, for a block of roots whose bracket poles p all lie in [pmin, r1-1].  The
+// span is cut into three contiguous segments -- poles left of every root's
+// bracket, the few around the brackets, poles right of every bracket -- so
+// the outer two run as branch-free unrolled loops.  Each accumulator still
+// receives its poles in increasing order, as in a single pass.
+__device__ inline int seg_first(int x, int l, int tpr) {
+    // smallest jj >= x with jj % tpr == l (x >= 0, tpr a power of two)
+    return x + ((l - x) & (tpr - 1));
+}
+
+template <typename LD>
+__device__ inline void secular_span(SecSums &sum, const SecRoot &st, int j0,
+                                    int cnt, int l, int tpr, int pmin, int r1,
+                                    LD ld) {
+    int lo_end = pmin - j0;
+    lo_end = lo_end < 0 ? 0 : (lo_end > cnt ? cnt : lo_end);
+    int mid_end = r1 + 1 - j0;
+    mid_end = mid_end < 0 ? 0 : (mid_end > cnt ? cnt : mid_end);
+#pragma unroll 4
+    for (int jj = l; jj < lo_end; jj += tpr) {
+        double dj, zj;
+        ld(jj, &dj, &zj);
+        sec_accum_left(sum, st, dj, zj);
+    }
+    for (int jj = seg_first(lo_end, l, tpr); jj < mid_end; jj += tpr) {
+        double dj, zj;
+        ld(jj, &dj, &zj);
+        sec_accum(sum, st, j0 + jj, dj, zj);
+    }
+#pragma unroll 4
+    for (int jj = seg_first(mid_end, l, tpr); jj < cnt; jj += tpr) {
+        double dj, zj;
+        ld(jj, &dj, &zj);
+        sec_accum_right(sum, st, dj, zj);
+    }
+}
+
+__device__ inline void sums_reduce(SecSums &sum, int tpr) {
+    for (int o = tpr >> 1; o > 0; o >>= 1) {
+        SecSums other;
+        other.psi = __shfl_xor_sync(0xffffffffu, sum.psi, o);
+        other.dpsi = __shfl_xor_sync(0xffffffffu, sum.dpsi, o);
+        other.phi = __shfl_xor_sync(0xffffffffu, sum.phi, o);
+        other.dphi = __shfl_xor_sync(0xffffffffu, sum.dphi, o);
+        other.err = __shfl_xor_sync(0xffffffffu, sum.err, o);
+        sec_combine(sum, other);
+    }
+}
+
+__device__ inline double group_sum(double v, int tpr) {
+    for (int o = tpr >> 1; o > 0; o >>= 1) {
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+    }
+    return v;
+}
+
+__device__ inline double group_prod(double v, int tpr) {
+    for (int o = tpr >> 1; o > 0; o >>= 1) {
+        v *= __shfl_xor_sync(0xffffffffu, v, o);
+    }
+    return v;
+}
+
+__device__ inline double lowner_value(const Ws &w, long long po, int i,
+                                      double prod, double rho) {
+    const double zi = w.pz[po + i];
+    const double mag = sqrt(fmax(-prod, 0.0));
+    double wi = zi < 0.0 ? -mag : mag;
+    if (!(mag > 0.0) || !isfinite(mag)) {
+        wi = zi * sqrt(rho);
+    }
+    return wi;
+}
+
+__device__ inline int block_role_setup(uint64_t *bars) {
     if (threadIdx.x == 0) {
         mbar_init(&bars[0], 1);
         mbar_init(&bars[1], 1);
         fence_mbar_init();
     }
     __syncthreads();
-    unsigned ph[2] = {0u, 0u};
+    return 0;
+}
 
-    for (int item = blockIdx.x; item < items; item += gridDim.x) {
-        const int g = item_node(w.pref_sec, a.nodes, item, &s_node);
+// ---------------------------------------------------------------- roots
+// Blocks [0, cta_blocks) serve the CTA-role merges, the others the warp-role
+// merges (8 warps per block, each on its own work item).
+constexpr int kWarpsPerBlock = kSweepThreads / 32;
+
+__global__ void __launch_bounds__(kSweepThreads)
+    k_secular(KArgs a, int cta_blocks) {
+    extern __shared__ __align__(16) double smem[];
+    __shared__ __align__(8) uint64_t bars[2];
+    const Ws &w = a.w;
+    const LevelCtl *ctl = &w.hdr->lvl[a.k];
+    const double eps = DBL_EPSILON;
+
+    if ((int)blockIdx.x >= cta_blocks) {
+        const int tpr = ctl->tpr_w;
+        const int Rw = 32 / tpr;
+        const int items = ctl->items_w;
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        const int grp = lane / tpr, l = lane % tpr;
+        const int stride = ((int)gridDim.x - cta_blocks) * kWarpsPerBlock;
+        for (int item = ((int)blockIdx.x - cta_blocks) * kWarpsPerBlock + warp;
+             item < items; item += stride) {
+            const int g = w.items_w[item];
+            const NodeGeom G = node_geom(a.F, a.k, g);
+            const int K = w.nK[g];
+            const double rho = w.nrho[g];
+            const long long po = G.poff;
+            if (K == 1) {
+                if (lane == 0) {
+                    secular_single(w, po, rho);
+                }
+                continue;
+            }
+            const int r0 = (item - w.pref_w[g]) * Rw;
+            const int r1 = (r0 + Rw < K) ? r0 + Rw : K;
+            const int pmin = (r0 < K - 2) ? r0 : K - 2;
+            const int r = r0 + grp;
+            const bool active = r < K;
+            const double *pd = w.pd + po;
+            const double *pz = w.pz + po;
+            SecRoot st;
+            if (active) {
+                sec_init(st, r, K, pd, pz, rho, w.nzn[g]);
+            } else {
+                st.stage = 2;
+            }
+            for (;;) {
+                SecSums sum;
+                sec_zero(sum);
+                if (active && st.stage != 2) {
+                    secular_span(sum, st, 0, K, l, tpr, pmin, r1,
+                                 [&](int j, double *dj, double *zj) {
+                                     *dj = __ldg(pd + j);
+                                     *zj = __ldg(pz + j);
+                                 });
+                }
+                sums_reduce(sum, tpr);
+                if (active && st.stage != 2) {
+                    sec_after_sweep(st, sum, eps);
+                }
+                if (__all_sync(0xffffffffu, (!active) || st.stage == 2)) {
+                    break;
+                }
+            }
+            if (active && l == 0) {
+                secular_store(w, a, po, r, st);
+            }
+        }
+        return;
+    }
+
+    block_role_setup(bars);
+    unsigned ph[2] = {0u, 0u};
+    const int tpr = ctl->tpr_c;
+    const int R = kSweepThreads / tpr;
+    const int items = ctl->items_c;
+    const int grp = threadIdx.x / tpr, lane = threadIdx.x % tpr;
+    for (int item = blockIdx.x; item < items; item += cta_blocks) {
+        const int g = item_node(w.items_c, item);
         const NodeGeom G = node_geom(a.F, a.k, g);
         const int K = w.nK[g];
         const double rho = w.nrho[g];
-        const double zn = w.nzn[g];
         const long long po = G.poff;
-        const int r = (item - w.pref_sec[g]) * R + grp;
+        const int r0 = (item - w.pref_c[g]) * R;
+        const int r1 = (r0 + R < K) ? r0 + R : K;
+        const int pmin = (r0 < K - 2) ? r0 : K - 2;
+        const int r = r0 + grp;
         const bool active = r < K;
-        const double *pd = w.pd + po;
-        const double *pz = w.pz + po;
-
-        if (K == 1) {
-            if (threadIdx.x == 0) {
-                const double z0 = pz[0];
-                const double t = rho * z0 * z0;
-                w.rorg[po] = 0;
-                w.rdo[po] = pd[0];
-                w.rtau[po] = t;
-                w.rlam[po] = pd[0] + t;
-            }
-            continue;
-        }
         SecRoot st;
         if (active) {
-            sec_init(st, r, K, pd, pz, rho, zn);
+            sec_init(st, r, K, w.pd + po, w.pz + po, rho, w.nzn[g]);
         } else {
             st.stage = 2;
-            st.iter = 0;
-            st.failed = 0;
         }
         TileSet<2> ts;
         const double *srcs[2] = {w.pd, w.pz};
@@ -678,28 +931,21 @@ __global__ void __launch_bounds__(kSweepThreads)
                 if (live) {
                     const double *bd = b[0];
                     const double *bz = b[1];
-                    for (int jj = lane; jj < cnt; jj += tpr) {
-                        sec_accum(sum, st, j0 + jj, bd[jj], bz[jj]);
-                    }
+                    secular_span(sum, st, j0, cnt, lane, tpr, pmin, r1,
+                                 [&](int jj, double *dj, double *zj) {
+                                     *dj = bd[jj];
+                                     *zj = bz[jj];
+                                 });
                 }
             });
             if (!ok) {
                 break;
             }
-            for (int o = tpr >> 1; o > 0; o >>= 1) {
-                SecSums other;
-                other.psi = __shfl_xor_sync(0xffffffffu, sum.psi, o);
-                other.dpsi = __shfl_xor_sync(0xffffffffu, sum.dpsi, o);
-                other.phi = __shfl_xor_sync(0xffffffffu, sum.phi, o);
-                other.dphi = __shfl_xor_sync(0xffffffffu, sum.dphi, o);
-                other.err = __shfl_xor_sync(0xffffffffu, sum.err, o);
-                sec_combine(sum, other);
-            }
+            sums_reduce(sum, tpr);
             if (live) {
                 sec_after_sweep(st, sum, eps);
             }
-            const int done = (!active) || st.stage == 2;
-            if (__syncthreads_and(done)) {
+            if (__syncthreads_and((!active) || st.stage == 2)) {
                 break;
             }
         }
@@ -710,18 +956,7 @@ __global__ void __launch_bounds__(kSweepThreads)
             return;
         }
         if (active && lane == 0) {
-            const long long o = po + r;
-            w.rorg[o] = st.org;
-            w.rdo[o] = st.dorg;
-            w.rtau[o] = st.tau;
-            w.rlam[o] = st.dorg + st.tau;
-            brdc_level_diagnostics *dg = &w.hdr->diag[a.k];
-            atomicAdd(&dg->secular_iter_sum, st.iter);
-            atomicMax(&dg->secular_iter_max, st.iter);
-            if (st.failed) {
-                atomicAdd(&dg->secular_iter_failed, 1);
-                atomicAdd(&w.hdr->nonconv, 1);
-            }
+            secular_store(w, a, po, r, st);
         }
         __syncthreads();
     }
@@ -730,37 +965,69 @@ __global__ void __launch_bounds__(kSweepThreads)
 // ------------------------------------------------------------- Loewner z
 // For every pole i:  w_i = sign(z_i) * sqrt(-prod_j delta_i(j) /
 // prod_{j != i} (d_i - d_j)),  delta_i(j) = (d_i - d_org(j)) - tau_j: the
-// recomputation of cpu/src/dlaed9_br.f:181-266 (WPROD), evaluated with one
-// lane group per pole sweeping tiles of the roots.
+// recomputation of cpu/src/dlaed9_br.f:181-266 (WPROD), one lane group per
+// pole sweeping the roots.  Instance roots are skipped (no parent reads
+// their rows).
 __global__ void __launch_bounds__(kSweepThreads)
-    k_lowner(KArgs a) {
+    k_lowner(KArgs a, int cta_blocks) {
     extern __shared__ __align__(16) double smem[];
     __shared__ __align__(8) uint64_t bars[2];
-    __shared__ int s_node;
     const Ws &w = a.w;
     const LevelCtl *ctl = &w.hdr->lvl[a.k];
-    const int tpr = ctl->tpr;
-    const int R = kSweepThreads / tpr;
-    const int items = ctl->items_sec;
-    const int grp = threadIdx.x / tpr, lane = threadIdx.x % tpr;
 
-    if (threadIdx.x == 0) {
-        mbar_init(&bars[0], 1);
-        mbar_init(&bars[1], 1);
-        fence_mbar_init();
+    if ((int)blockIdx.x >= cta_blocks) {
+        const int tpr = ctl->tpr_w;
+        const int Rw = 32 / tpr;
+        const int items = ctl->items_w;
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        const int grp = lane / tpr, l = lane % tpr;
+        const int stride = ((int)gridDim.x - cta_blocks) * kWarpsPerBlock;
+        for (int item = ((int)blockIdx.x - cta_blocks) * kWarpsPerBlock + warp;
+             item < items; item += stride) {
+            const int g = w.items_w[item];
+            const NodeGeom G = node_geom(a.F, a.k, g);
+            if (G.depth == 0) {
+                continue;
+            }
+            const int K = w.nK[g];
+            const long long po = G.poff;
+            const int i = (item - w.pref_w[g]) * Rw + grp;
+            const bool active = i < K;
+            double prod = 1.0;
+            if (active) {
+                const double di = w.pd[po + i];
+                const double *rdo = w.rdo + po;
+                const double *rtau = w.rtau + po;
+                const double *pd = w.pd + po;
+#pragma unroll 4
+                for (int j = l; j < K; j += tpr) {
+                    const double dl = (di - __ldg(rdo + j)) - __ldg(rtau + j);
+                    prod *= (j == i) ? dl : dl / (di - __ldg(pd + j));
+                }
+            }
+            prod = group_prod(prod, tpr);
+            if (active && l == 0) {
+                w.pw[po + i] = lowner_value(w, po, i, prod, w.nrho[g]);
+            }
+        }
+        return;
     }
-    __syncthreads();
-    unsigned ph[2] = {0u, 0u};
 
-    for (int item = blockIdx.x; item < items; item += gridDim.x) {
-        const int g = item_node(w.pref_sec, a.nodes, item, &s_node);
+    block_role_setup(bars);
+    unsigned ph[2] = {0u, 0u};
+    const int tpr = ctl->tpr_c;
+    const int R = kSweepThreads / tpr;
+    const int items = ctl->items_c;
+    const int grp = threadIdx.x / tpr, lane = threadIdx.x % tpr;
+    for (int item = blockIdx.x; item < items; item += cta_blocks) {
+        const int g = item_node(w.items_c, item);
         const NodeGeom G = node_geom(a.F, a.k, g);
         if (G.depth == 0) {
-            continue; // instance root: no parent needs its rows
+            continue;
         }
         const int K = w.nK[g];
         const long long po = G.poff;
-        const int i = (item - w.pref_sec[g]) * R + grp;
+        const int i = (item - w.pref_c[g]) * R + grp;
         const bool active = i < K;
         const double di = active ? w.pd[po + i] : 0.0;
         double prod = 1.0;
@@ -784,130 +1051,180 @@ __global__ void __launch_bounds__(kSweepThreads)
             record_error(w.hdr, kErrBarrierTimeout);
             return;
         }
-        for (int o = tpr >> 1; o > 0; o >>= 1) {
-            prod *= __shfl_xor_sync(0xffffffffu, prod, o);
-        }
+        prod = group_prod(prod, tpr);
         if (active && lane == 0) {
-            const double zi = w.pz[po + i];
-            const double mag = sqrt(fmax(-prod, 0.0));
-            double wi = zi < 0.0 ? -mag : mag;
-            if (!(mag > 0.0) || !isfinite(mag)) {
-                wi = zi * sqrt(w.nrho[g]);
-            }
-            w.pw[po + i] = wi;
+            w.pw[po + i] = lowner_value(w, po, i, prod, w.nrho[g]);
         }
         __syncthreads();
     }
 }
 
-// ------------------------------------------------- rows and placement
-// Slot s < K is root s: its eigenvector u_i = w_i / delta_i(s), normalised,
-// gives new_first = sum_i f_i u_i and new_last = sum_i l_i u_i (the streamed
-// update of cpu/src/dlaed9_br.f:272-334 with the compact delta).  Slots
-// K.. are the deflated eigenvalues.  Every slot is written to its place in
-// the ascending spectrum of the node: roots and the two deflated lists are
-// merged by rank (ties: roots, then small-z, then rotated).
+// ----------------------------------------------------------- boundary rows
+// Root s: u_i = w_i / delta_i(s), normalised; new first row = sum_i f_i u_i,
+// new last row = sum_i l_i u_i: the streamed update of
+// cpu/src/dlaed9_br.f:272-334 with the compact delta.  Written to rf/rl;
+// k_place puts them in order.
 __global__ void __launch_bounds__(kSweepThreads)
-    k_rows_place(KArgs a) {
+    k_rows(KArgs a, int cta_blocks) {
     extern __shared__ __align__(16) double smem[];
     __shared__ __align__(8) uint64_t bars[2];
-    __shared__ int s_node;
     const Ws &w = a.w;
     const LevelCtl *ctl = &w.hdr->lvl[a.k];
-    const int tpr = ctl->tpr;
-    const int R = kSweepThreads / tpr;
-    const int items = ctl->items_rows;
-    const int grp = threadIdx.x / tpr, lane = threadIdx.x % tpr;
 
-    if (threadIdx.x == 0) {
-        mbar_init(&bars[0], 1);
-        mbar_init(&bars[1], 1);
-        fence_mbar_init();
-    }
-    __syncthreads();
-    unsigned ph[2] = {0u, 0u};
-
-    for (int item = blockIdx.x; item < items; item += gridDim.x) {
-        const int g = item_node(w.pref_rows, a.nodes, item, &s_node);
-        const NodeGeom G = node_geom(a.F, a.k, g);
-        const int K = w.nK[g];
-        const int Kz = w.nKz[g];
-        const int m = G.m;
-        const int ndz = m - Kz, ndg = Kz - K;
-        const long long po = G.poff, gs = G.gstart;
-        const int b0 = (item - w.pref_rows[g]) * R;
-        const int s = b0 + grp;
-        const bool top = (G.depth == 0);
-        double a1 = 0.0, a2 = 0.0, s2 = 0.0;
-        if (!top && b0 < K) {
-            const bool root = s < K;
-            const double dorg = root ? w.rdo[po + s] : 0.0;
-            const double tau = root ? w.rtau[po + s] : 0.0;
-            TileSet<4> ts;
-            const double *srcs[4] = {w.pd, w.pw, w.pf, w.pl};
-            tiles_setup<4>(ts, smem, bars, srcs, po, K);
-            ts.phase[0] = ph[0];
-            ts.phase[1] = ph[1];
-            const bool ok = tiles_sweep<4>(ts, [&](int j0, int cnt, double *const *b) {
-                if (root) {
-                    for (int jj = lane; jj < cnt; jj += tpr) {
-                        const double dl = (b[0][jj] - dorg) - tau;
-                        const double u = (dl != 0.0) ? b[1][jj] / dl : 0.0;
-                        s2 += u * u;
-                        a1 += b[2][jj] * u;
-                        a2 += b[3][jj] * u;
-                    }
-                }
-            });
-            ph[0] = ts.phase[0];
-            ph[1] = ts.phase[1];
-            if (!ok) {
-                record_error(w.hdr, kErrBarrierTimeout);
-                return;
+    if ((int)blockIdx.x >= cta_blocks) {
+        const int tpr = ctl->tpr_w;
+        const int Rw = 32 / tpr;
+        const int items = ctl->items_w;
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        const int grp = lane / tpr, l = lane % tpr;
+        const int stride = ((int)gridDim.x - cta_blocks) * kWarpsPerBlock;
+        for (int item = ((int)blockIdx.x - cta_blocks) * kWarpsPerBlock + warp;
+             item < items; item += stride) {
+            const int g = w.items_w[item];
+            const NodeGeom G = node_geom(a.F, a.k, g);
+            if (G.depth == 0) {
+                continue;
             }
-            for (int o = tpr >> 1; o > 0; o >>= 1) {
-                s2 += __shfl_xor_sync(0xffffffffu, s2, o);
-                a1 += __shfl_xor_sync(0xffffffffu, a1, o);
-                a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+            const int K = w.nK[g];
+            const long long po = G.poff;
+            const int s = (item - w.pref_w[g]) * Rw + grp;
+            const bool root = s < K;
+            double a1 = 0.0, a2 = 0.0, s2 = 0.0;
+            if (root) {
+                const double dorg = w.rdo[po + s];
+                const double tau = w.rtau[po + s];
+                const double *pd = w.pd + po;
+                const double *pw = w.pw + po;
+                const double *pf = w.pf + po;
+                const double *pl = w.pl + po;
+#pragma unroll 4
+                for (int i = l; i < K; i += tpr) {
+                    const double dl = (__ldg(pd + i) - dorg) - tau;
+                    const double u = (dl != 0.0) ? __ldg(pw + i) / dl : 0.0;
+                    s2 += u * u;
+                    a1 += __ldg(pf + i) * u;
+                    a2 += __ldg(pl + i) * u;
+                }
+            }
+            s2 = group_sum(s2, tpr);
+            a1 = group_sum(a1, tpr);
+            a2 = group_sum(a2, tpr);
+            if (root && l == 0) {
+                const double nrm = sqrt(s2);
+                w.rf[po + s] = nrm > 0.0 ? a1 / nrm : 0.0;
+                w.rl[po + s] = nrm > 0.0 ? a2 / nrm : 0.0;
             }
         }
-        if (s < m && lane == 0) {
-            double val, fo = 0.0, lo = 0.0;
-            int pos;
-            const double *zdl = w.zd + gs;
-            const double *gdl = w.gd + gs;
-            const double *rl = w.rlam + po;
-            if (s < K) {
-                val = rl[s];
-                pos = s + lower_bound_d(zdl, ndz, val) + lower_bound_d(gdl, ndg, val);
-                if (!top) {
-                    const double nrm = sqrt(s2);
-                    fo = (nrm > 0.0) ? a1 / nrm : 0.0;
-                    lo = (nrm > 0.0) ? a2 / nrm : 0.0;
+        return;
+    }
+
+    block_role_setup(bars);
+    unsigned ph[2] = {0u, 0u};
+    const int tpr = ctl->tpr_c;
+    const int R = kSweepThreads / tpr;
+    const int items = ctl->items_c;
+    const int grp = threadIdx.x / tpr, lane = threadIdx.x % tpr;
+    for (int item = blockIdx.x; item < items; item += cta_blocks) {
+        const int g = item_node(w.items_c, item);
+        const NodeGeom G = node_geom(a.F, a.k, g);
+        if (G.depth == 0) {
+            continue;
+        }
+        const int K = w.nK[g];
+        const long long po = G.poff;
+        const int s = (item - w.pref_c[g]) * R + grp;
+        const bool root = s < K;
+        const double dorg = root ? w.rdo[po + s] : 0.0;
+        const double tau = root ? w.rtau[po + s] : 0.0;
+        double a1 = 0.0, a2 = 0.0, s2 = 0.0;
+        TileSet<4> ts;
+        const double *srcs[4] = {w.pd, w.pw, w.pf, w.pl};
+        tiles_setup<4>(ts, smem, bars, srcs, po, K);
+        ts.phase[0] = ph[0];
+        ts.phase[1] = ph[1];
+        const bool ok = tiles_sweep<4>(ts, [&](int j0, int cnt, double *const *b) {
+            if (root) {
+                for (int jj = lane; jj < cnt; jj += tpr) {
+                    const double dl = (b[0][jj] - dorg) - tau;
+                    const double u = (dl != 0.0) ? b[1][jj] / dl : 0.0;
+                    s2 += u * u;
+                    a1 += b[2][jj] * u;
+                    a2 += b[3][jj] * u;
                 }
-            } else if (s < K + ndz) {
-                const int q = s - K;
-                val = zdl[q];
-                pos = q + upper_bound_d(rl, K, val) + lower_bound_d(gdl, ndg, val);
-                fo = w.zf[gs + q];
-                lo = w.zl[gs + q];
-            } else {
-                const int q = s - K - ndz;
-                val = gdl[q];
-                pos = q + upper_bound_d(rl, K, val) + upper_bound_d(zdl, ndz, val);
-                fo = w.gf[gs + q];
-                lo = w.gl[gs + q];
             }
-            const long long o = gs + pos;
-            if (top) {
-                a.W[o] = val;
-            } else {
-                w.nd[o] = val;
-                w.nf[o] = fo;
-                w.nl[o] = lo;
-            }
+        });
+        ph[0] = ts.phase[0];
+        ph[1] = ts.phase[1];
+        if (!ok) {
+            record_error(w.hdr, kErrBarrierTimeout);
+            return;
+        }
+        s2 = group_sum(s2, tpr);
+        a1 = group_sum(a1, tpr);
+        a2 = group_sum(a2, tpr);
+        if (root && lane == 0) {
+            const double nrm = sqrt(s2);
+            w.rf[po + s] = nrm > 0.0 ? a1 / nrm : 0.0;
+            w.rl[po + s] = nrm > 0.0 ? a2 / nrm : 0.0;
         }
         __syncthreads();
+    }
+}
+
+// --------------------------------------------------------------- placement
+// One thread per row of the level: every eigenvalue of a merged node (root,
+// small-z deflated, rotated out) goes to its place in the node's ascending
+// spectrum by rank among the three sorted lists (ties: roots, then small-z,
+// then rotated), with its first and last boundary-row entries; instance
+// roots write the final eigenvalues to W.
+__global__ void __launch_bounds__(256) k_place(KArgs a, long long total_n) {
+    const Ws &w = a.w;
+    for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x; x < total_n;
+         x += (long long)gridDim.x * blockDim.x) {
+        int g, m, depth;
+        long long gs;
+        if (!elem_node(a.F, a.k, x, &g, &gs, &m, &depth)) {
+            continue;
+        }
+        const long long po = (gs + g + 1) & ~1LL;
+        const int s = (int)(x - gs);
+        const int K = w.nK[g];
+        const int Kz = w.nKz[g];
+        const int ndz = m - Kz, ndg = Kz - K;
+        const bool top = (depth == 0);
+        const double *zdl = w.zd + gs;
+        const double *gdl = w.gd + gs;
+        const double *rl = w.rlam + po;
+        double val, fo = 0.0, lo = 0.0;
+        int pos;
+        if (s < K) {
+            val = rl[s];
+            pos = s + lower_bound_d(zdl, ndz, val) + lower_bound_d(gdl, ndg, val);
+            if (!top) {
+                fo = w.rf[po + s];
+                lo = w.rl[po + s];
+            }
+        } else if (s < K + ndz) {
+            const int q = s - K;
+            val = zdl[q];
+            pos = q + upper_bound_d(rl, K, val) + lower_bound_d(gdl, ndg, val);
+            fo = w.zf[gs + q];
+            lo = w.zl[gs + q];
+        } else {
+            const int q = s - K - ndz;
+            val = gdl[q];
+            pos = q + upper_bound_d(rl, K, val) + upper_bound_d(zdl, ndz, val);
+            fo = w.gf[gs + q];
+            lo = w.gl[gs + q];
+        }
+        const long long o = gs + pos;
+        if (top) {
+            a.W[o] = val;
+        } else {
+            w.nd[o] = val;
+            w.nf[o] = fo;
+            w.nl[o] = lo;
+        }
     }
 }
 
@@ -927,9 +1244,10 @@ __global__ void k_init(WsHeader *h, int levels, int B, long long total_n,
     }
     for (int k = t; k < BRDC_MAX_LEVELS; k += blockDim.x) {
         h->lvl[k].ticket = 0;
-        h->lvl[k].tpr = 1;
-        h->lvl[k].items_sec = 0;
-        h->lvl[k].items_rows = 0;
+        h->lvl[k].tpr_w = 1;
+        h->lvl[k].tpr_c = 1;
+        h->lvl[k].items_w = 0;
+        h->lvl[k].items_c = 0;
         h->lvl[k].total_k = 0;
         brdc_level_diagnostics z = {};
         z.level = k;

@@ -135,6 +135,28 @@ __host__ __device__ inline void sec_accum(SecSums &s, const SecRoot &r, int j,
     s.err += skip ? 0.0 : (left ? -s.psi : s.phi);
 }
 
+// The same term for a pole known to lie left of p (j < p) or right of p+1
+// (j > p+1): callers use these for tiles wholly on one side of every root
+// they serve, which removes the per-element selects of sec_accum.  The
+// arithmetic is identical to sec_accum's for such poles.
+__host__ __device__ inline void sec_accum_left(SecSums &s, const SecRoot &r,
+                                               double dj, double zj) {
+    const double delta = (dj - r.eorg_d) - r.etau;
+    const double t = zj / delta;
+    s.psi += zj * t;
+    s.dpsi += t * t;
+    s.err -= s.psi;
+}
+
+__host__ __device__ inline void sec_accum_right(SecSums &s, const SecRoot &r,
+                                                double dj, double zj) {
+    const double delta = (dj - r.eorg_d) - r.etau;
+    const double t = zj / delta;
+    s.phi += zj * t;
+    s.dphi += t * t;
+    s.err += s.phi;
+}
+
 // Combine partial sums of two lanes (the tree adds its own rounding).  Every
 // operation is commutative in (a, b), so the lanes of a butterfly reduction
 // end with bit-identical sums and take identical branches afterwards.

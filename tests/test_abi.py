@@ -67,3 +67,9 @@ def test_batched_workspace_query(built_lib):
     assert brdc.batched_workspace_size([0, 10, 50, 4146]) > brdc.workspace_size(4096)
     with pytest.raises(brdc.BrdcError):
         brdc.batched_workspace_size([0, 10, 10])
+
+
+def test_noalloc_scratch_covers_its_limit(built_lib):
+    # brdc_dstebr_noalloc solves n <= 16384 in a 6 MiB static device array
+    # (brdc_capi.cu kNoAllocBytes); the workspace layout must stay within it.
+    assert brdc.workspace_size(16384) <= 6 * 2**20

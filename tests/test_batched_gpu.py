@@ -1,0 +1,122 @@
+"""Batched (forest) solves and CUDA-graph capture of the solve."""
+import numpy as np
+import pytest
+
+import oracle
+from brdc import families
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+
+
+def per_instance_errors(off, W, D, E):
+    errs = []
+    for b in range(len(off) - 1):
+        lo, hi = int(off[b]), int(off[b + 1])
+        ref = oracle.dstedc_dc_br(D[lo:hi], E[lo:hi - 1])
+        errs.append(float(np.max(np.abs(W[lo:hi] - ref)) / max(np.max(np.abs(ref)), 1e-300)))
+    return np.array(errs)
+
+
+def test_batched_mixed_orders_and_families(solver):
+    import torch
+
+    off, D, E, orders, fams = families.batch(96, 32, 3000, seed=1)
+    W = solver.dstebr_batched(off, torch.tensor(D, device="cuda"),
+                              torch.tensor(E, device="cuda")).cpu().numpy()
+    errs = per_instance_errors(off, W, D, E)
+    assert errs.max() < TOL, (errs.argmax(), errs.max())
+
+
+def test_batched_includes_tiny_instances(solver):
+    import torch
+
+    orders = [1, 2, 16, 17, 5, 100, 33, 1, 64, 15]
+    off = np.concatenate([[0], np.cumsum(orders)])
+    rng = np.random.default_rng(9)
+    D = rng.standard_normal(off[-1])
+    E = rng.standard_normal(off[-1])
+    for b in range(len(orders)):
+        E[off[b + 1] - 1] = 7.0  # the slot between instances is ignored
+    W = solver.dstebr_batched(off, torch.tensor(D, device="cuda"),
+                              torch.tensor(E, device="cuda")).cpu().numpy()
+    errs = per_instance_errors(off, W, D, E)
+    assert errs.max() < TOL
+
+
+def test_batched_agrees_with_single_solves(solver):
+    # Lanes per root follow the level's K statistics, which differ between a
+    # batch and a lone solve, so sums may be ordered differently: agreement
+    # is to the parity tolerance, not bitwise.
+    import torch
+
+    off, D, E, orders, _ = families.batch(20, 17, 2000, seed=2)
+    Wb = solver.dstebr_batched(off, torch.tensor(D, device="cuda"),
+                               torch.tensor(E, device="cuda")).cpu().numpy()
+    for b in range(len(orders)):
+        lo, hi = int(off[b]), int(off[b + 1])
+        ws = solver.dstebr(torch.tensor(D[lo:hi], device="cuda"),
+                           torch.tensor(E[lo:hi - 1] if hi - lo > 1 else np.zeros(1), device="cuda"))
+        w1 = ws.cpu().numpy()
+        assert np.max(np.abs(w1 - Wb[lo:hi])) <= TOL * np.max(np.abs(w1))
+
+
+def test_graph_capture_single_solve(solver):
+    import torch
+
+    n = 30000
+    d, e = families.generate("normal", n)
+    D = torch.tensor(d, device="cuda")
+    E = torch.tensor(e, device="cuda")
+    W = torch.empty(n, dtype=torch.float64, device="cuda")
+    ws = solver.workspace(n)
+    stream = torch.cuda.Stream()
+    stream.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(stream):
+        solver.set_stream(stream)
+        solver.dstebr(D, E, W=W, workspace=ws)  # eager warm-up outside capture
+        stream.synchronize()
+        ref = W.clone()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=stream):
+            solver.dstebr(D, E, W=W, workspace=ws)
+    torch.cuda.current_stream().wait_stream(stream)
+    solver.set_stream()
+    W.zero_()
+    g.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(W, ref)
+    # new input values flow through the captured graph
+    d2, e2 = families.generate("uniform", n)
+    D.copy_(torch.tensor(d2, device="cuda"))
+    E.copy_(torch.tensor(e2, device="cuda"))
+    g.replay()
+    torch.cuda.synchronize()
+    ref2 = oracle.dstedc_dc_br(d2, e2)
+    assert np.max(np.abs(W.cpu().numpy() - ref2)) < TOL * np.max(np.abs(ref2))
+
+
+def test_graph_capture_batched(solver):
+    import torch
+
+    off, D, E, _, _ = families.batch(64, 32, 1500, seed=3)
+    Dt = torch.tensor(D, device="cuda")
+    Et = torch.tensor(E, device="cuda")
+    W = torch.empty(int(off[-1]), dtype=torch.float64, device="cuda")
+    ws = solver.batched_workspace(off)
+    stream = torch.cuda.Stream()
+    stream.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(stream):
+        solver.set_stream(stream)
+        solver.dstebr_batched(off, Dt, Et, W=W, workspace=ws)  # uploads tables
+        stream.synchronize()
+        ref = W.clone()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=stream):
+            solver.dstebr_batched(off, Dt, Et, W=W, workspace=ws)
+    torch.cuda.current_stream().wait_stream(stream)
+    solver.set_stream()
+    W.zero_()
+    g.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(W, ref)
