@@ -77,6 +77,7 @@ struct HostForest {
     long long leaves = 0;
     std::vector<int> level_nodes; // nodes per level
     std::vector<int> level_mmax;  // largest node per level
+    std::vector<long long> level_rows; // rows of instances merging at a level
     long long nn0 = 0;            // max nodes of a level
 };
 
@@ -101,12 +102,14 @@ bool build_forest(int B, const long long *off, HostForest *f) {
     }
     f->level_nodes.assign(f->max_levels, 0);
     f->level_mmax.assign(f->max_levels, 0);
+    f->level_rows.assign(f->max_levels, 0);
     for (int b = 0; b < B; ++b) {
         const long long n = off[b + 1] - off[b];
         const int L = f->lev[b];
         for (int k = 0; k < L; ++k) {
             const int depth = L - 1 - k;
             f->level_nodes[k] += 1 << depth;
+            f->level_rows[k] += n;
             const long long mm = (n + (1LL << depth) - 1) >> depth;
             f->level_mmax[k] = std::max<long long>(f->level_mmax[k], mm);
         }
@@ -312,6 +315,7 @@ brdc_status run_forest(brdc_handle h, const HostForest &hf, const Forest &F,
     for (int k = 0; k < hf.max_levels; ++k) {
         a.k = k;
         a.nodes = hf.level_nodes[k];
+        a.level_rows = hf.level_rows[k];
         // CTA-role blocks exist only where a merge can exceed kWarpMaxK poles
         const int cta_blocks = hf.level_mmax[k] > kWarpMaxK ? h->sm_count * 2 : 0;
         const int grid = cta_blocks + warp_blocks;

@@ -35,6 +35,7 @@ struct KArgs {
     double *W;          // final eigenvalues
     int k;              // forest level
     int nodes;          // merges at this level
+    long long level_rows; // rows of the instances that merge at this level
 };
 
 // ------------------------------------------------------------------ leaves
@@ -311,6 +312,7 @@ __global__ void __launch_bounds__(256) k_merge(KArgs a, long long total_n) {
 
 template <int T>
 __global__ void __launch_bounds__(T) k_merge_deflate(KArgs a) {
+    constexpr int EPT = 4; // rows per thread per chunk
     __shared__ double red[32];
     __shared__ int iscan[32];
     __shared__ int s_last;
@@ -333,45 +335,53 @@ __global__ void __launch_bounds__(T) k_merge_deflate(KArgs a) {
     const double maxz = block_max<T>(lz, red);
     const double tol = kDeflTolScale * eps * fmax(maxd, maxz);
 
-    // compaction 1: small-z survivors (sorted) and small-z deflated (sorted)
+    // compaction 1: small-z survivors (sorted) and small-z deflated (sorted).
+    // Every value a thread moves is loaded before the scan, so a chunk
+    // costs one round trip to L2 instead of one per row.
     int carry_a = 0, carry_z = 0;
-    for (int base = 0; base < m; base += 4 * T) {
-        int fl[4];
+    for (int base = 0; base < m; base += EPT * T) {
+        int fl[EPT];
+        double vd[EPT], vz[EPT], vf[EPT], vl[EPT];
         int cnt = 0;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int idx = base + 4 * threadIdx.x + q;
-            fl[q] = (idx < m) ? (fabs(rho * w.mz[gs + idx]) > tol) : 0;
+        for (int q = 0; q < EPT; ++q) {
+            const int idx = base + EPT * threadIdx.x + q;
+            const bool ok = idx < m;
+            const long long src = gs + (ok ? idx : 0);
+            vd[q] = w.md[src];
+            vz[q] = w.mz[src];
+            vf[q] = w.mf[src];
+            vl[q] = w.ml[src];
+            fl[q] = ok ? (fabs(rho * vz[q]) > tol) : 0;
             cnt += fl[q];
         }
         int tot;
         const int ex = block_exscan<T>(cnt, iscan, &tot);
         int ra = carry_a + ex;
-        int rz = carry_z + (4 * threadIdx.x - ex);
+        int rz = carry_z + (EPT * threadIdx.x - ex);
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int idx = base + 4 * threadIdx.x + q;
+        for (int q = 0; q < EPT; ++q) {
+            const int idx = base + EPT * threadIdx.x + q;
             if (idx < m) {
-                const long long src = gs + idx;
                 if (fl[q]) {
                     const long long o = gs + ra;
-                    w.ad[o] = w.md[src];
-                    w.az[o] = w.mz[src];
-                    w.af[o] = w.mf[src];
-                    w.al[o] = w.ml[src];
+                    w.ad[o] = vd[q];
+                    w.az[o] = vz[q];
+                    w.af[o] = vf[q];
+                    w.al[o] = vl[q];
                     w.amap[o] = idx;
                     w.gmark[o] = 0;
                     ++ra;
                 } else {
                     const long long o = gs + rz;
-                    w.zd[o] = w.md[src];
-                    w.zf[o] = w.mf[src];
-                    w.zl[o] = w.ml[src];
+                    w.zd[o] = vd[q];
+                    w.zf[o] = vf[q];
+                    w.zl[o] = vl[q];
                     ++rz;
                 }
             }
         }
-        const int valid = (m - base) < 4 * T ? (m - base) : 4 * T;
+        const int valid = (m - base) < EPT * T ? (m - base) : EPT * T;
         carry_a += tot;
         carry_z += valid - tot;
     }
@@ -434,44 +444,49 @@ __global__ void __launch_bounds__(T) k_merge_deflate(KArgs a) {
     int carry_p = 0, carry_g = 0;
     double zn = 0.0;
     const long long po = G.poff;
-    for (int base = 0; base < Kz; base += 4 * T) {
-        int fl[4];
+    for (int base = 0; base < Kz; base += EPT * T) {
+        int fl[EPT];
+        double vd[EPT], vz[EPT], vf[EPT], vl[EPT];
         int cnt = 0;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int idx = base + 4 * threadIdx.x + q;
-            fl[q] = (idx < Kz) ? (w.gmark[gs + idx] == 0) : 0;
+        for (int q = 0; q < EPT; ++q) {
+            const int idx = base + EPT * threadIdx.x + q;
+            const bool ok = idx < Kz;
+            const long long src = gs + (ok ? idx : 0);
+            vd[q] = w.ad[src];
+            vz[q] = w.az[src];
+            vf[q] = w.af[src];
+            vl[q] = w.al[src];
+            fl[q] = ok ? (w.gmark[src] == 0) : 0;
             cnt += fl[q];
         }
         int tot;
         const int ex = block_exscan<T>(cnt, iscan, &tot);
         int rp = carry_p + ex;
-        int rg = carry_g + (4 * threadIdx.x - ex);
+        int rg = carry_g + (EPT * threadIdx.x - ex);
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int idx = base + 4 * threadIdx.x + q;
+        for (int q = 0; q < EPT; ++q) {
+            const int idx = base + EPT * threadIdx.x + q;
             if (idx < Kz) {
-                const long long src = gs + idx;
                 if (fl[q]) {
                     const long long o = po + rp;
-                    const double zv = w.az[src];
-                    w.pd[o] = w.ad[src];
-                    w.pz[o] = zv;
-                    w.pf[o] = w.af[src];
-                    w.pl[o] = w.al[src];
+                    w.pd[o] = vd[q];
+                    w.pz[o] = vz[q];
+                    w.pf[o] = vf[q];
+                    w.pl[o] = vl[q];
                     w.pmap[o] = idx;
-                    zn += zv * zv;
+                    zn += vz[q] * vz[q];
                     ++rp;
                 } else {
                     const long long o = gs + rg;
-                    w.gd[o] = w.ad[src];
-                    w.gf[o] = w.af[src];
-                    w.gl[o] = w.al[src];
+                    w.gd[o] = vd[q];
+                    w.gf[o] = vf[q];
+                    w.gl[o] = vl[q];
                     ++rg;
                 }
             }
         }
-        const int valid = (Kz - base) < 4 * T ? (Kz - base) : 4 * T;
+        const int valid = (Kz - base) < EPT * T ? (Kz - base) : EPT * T;
         carry_p += tot;
         carry_g += valid - tot;
     }
@@ -484,14 +499,6 @@ __global__ void __launch_bounds__(T) k_merge_deflate(KArgs a) {
         w.nrho[g] = rho;
         w.ntol[g] = tol;
         w.nzn[g] = zn;
-        brdc_level_diagnostics *dg = &w.hdr->diag[a.k];
-        atomicAdd(&dg->merge_count, 1);
-        atomicAdd(&dg->size_sum, m);
-        atomicAdd(&dg->dd_before_sum, Kz);
-        atomicAdd(&dg->dd_after_sum, K);
-        atomicMax(&dg->dd_after_max, K);
-        atomicAdd(reinterpret_cast<unsigned long long *>(&dg->dd_after_sq_sum),
-                  (unsigned long long)K * (unsigned long long)K);
         __threadfence();
         const int t = atomicAdd(&w.hdr->lvl[a.k].ticket, 1);
         s_last = (t == (int)gridDim.x - 1);
@@ -505,8 +512,10 @@ __global__ void __launch_bounds__(T) k_merge_deflate(KArgs a) {
     // CTAs that stage pole tiles in shared memory.
     __threadfence();
     double tkw = 0.0, tkc = 0.0, cw = 0.0, cc = 0.0;
+    double skz = 0.0, sk2 = 0.0, kmax = 0.0;
     for (int i = threadIdx.x; i < a.nodes; i += T) {
-        const int kk = ((volatile int *)w.nK)[i];
+        const int kk = __ldcg(w.nK + i);
+        const int kz = __ldcg(w.nKz + i);
         if (kk > kWarpMaxK) {
             tkc += kk;
             cc += 1.0;
@@ -514,11 +523,28 @@ __global__ void __launch_bounds__(T) k_merge_deflate(KArgs a) {
             tkw += kk;
             cw += 1.0;
         }
+        skz += kz;
+        sk2 += (double)kk * (double)kk;
+        kmax = fmax(kmax, (double)kk);
     }
     tkw = block_sum<T>(tkw, red);
     tkc = block_sum<T>(tkc, red);
     cw = block_sum<T>(cw, red);
     cc = block_sum<T>(cc, red);
+    skz = block_sum<T>(skz, red);
+    sk2 = block_sum<T>(sk2, red);
+    kmax = block_max<T>(kmax, red);
+    if (threadIdx.x == 0) {
+        // level counters of the reference's diagnostics
+        // (gpu/src/tridiag_solver.cu:1166-1260), gathered once per level
+        brdc_level_diagnostics *dg = &w.hdr->diag[a.k];
+        dg->merge_count = a.nodes;
+        dg->size_sum = (int)(a.level_rows);
+        dg->dd_before_sum = (int)skz;
+        dg->dd_after_sum = (int)(tkw + tkc);
+        dg->dd_after_max = (int)kmax;
+        dg->dd_after_sq_sum = (long long)sk2;
+    }
     // warp role: each root's sweeps form a serial latency chain, so spread
     // the roots over enough lanes to keep every scheduler busy (~75k
     // threads); with one root per warp the warp also never diverges.
@@ -540,27 +566,32 @@ __global__ void __launch_bounds__(T) k_merge_deflate(KArgs a) {
     tpr_c = tpr_c < cap ? tpr_c : cap;
     const int Rw = 32 / tpr_w;
     const int Rc = kSweepThreads / tpr_c;
-    int carry_w = 0, carry_c = 0;
-    for (int base = 0; base < a.nodes; base += T) {
-        const int i = base + threadIdx.x;
-        int iw = 0, ic = 0;
-        if (i < a.nodes) {
-            const int kk = ((volatile int *)w.nK)[i];
-            if (kk > kWarpMaxK) {
-                ic = (kk + Rc - 1) / Rc;
-            } else {
-                iw = (kk + Rw - 1) / Rw;
-            }
+    // each thread owns a contiguous run of nodes: serial prefix of its run,
+    // one block scan across threads, then the run's prefixes
+    const int per = (a.nodes + T - 1) / T;
+    const int i0 = threadIdx.x * per;
+    const int i1 = (i0 + per < a.nodes) ? i0 + per : a.nodes;
+    int sw = 0, sc = 0;
+    for (int i = i0; i < i1; ++i) {
+        const int kk = __ldcg(w.nK + i);
+        if (kk > kWarpMaxK) {
+            sc += (kk + Rc - 1) / Rc;
+        } else {
+            sw += (kk + Rw - 1) / Rw;
         }
-        int tw, tc;
-        const int ew = block_exscan<T>(iw, iscan, &tw);
-        const int ec = block_exscan<T>(ic, iscan, &tc);
-        if (i < a.nodes) {
-            w.pref_w[i] = carry_w + ew;
-            w.pref_c[i] = carry_c + ec;
+    }
+    int carry_w, carry_c;
+    int rw = block_exscan<T>(sw, iscan, &carry_w);
+    int rc = block_exscan<T>(sc, iscan, &carry_c);
+    for (int i = i0; i < i1; ++i) {
+        const int kk = __ldcg(w.nK + i);
+        w.pref_w[i] = rw;
+        w.pref_c[i] = rc;
+        if (kk > kWarpMaxK) {
+            rc += (kk + Rc - 1) / Rc;
+        } else {
+            rw += (kk + Rw - 1) / Rw;
         }
-        carry_w += tw;
-        carry_c += tc;
     }
     __syncthreads();
     for (int i = threadIdx.x; i < a.nodes; i += T) {
