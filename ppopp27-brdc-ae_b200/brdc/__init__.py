@@ -280,6 +280,34 @@ class Solver:
         _check(st, "brdc_dstebr", self.h)
         return W
 
+    def checkpoint_workspace(self, n: int):
+        """Workspace that also records the per-level state the adjoint reads."""
+        return self.workspace(n, FLAG_KEEP_CHECKPOINTS)
+
+    def dstebr_backward(self, D, E, G, workspace=None, keep_forward: bool = False,
+                        gD=None, gE=None):
+        """dL/dD, dL/dE for L = sum(G * W).  With keep_forward the workspace
+        must hold the checkpoints of a brdc_dstebr call on the same D, E;
+        otherwise the forward solve is re-run first."""
+        torch = self._torch
+        n = D.shape[0]
+        D = D.contiguous()
+        E = E.contiguous() if E is not None and E.numel() > 0 else D
+        G = G.contiguous()
+        if gD is None:
+            gD = torch.empty(n, dtype=torch.float64, device=D.device)
+        if gE is None:
+            gE = torch.empty(max(n - 1, 1), dtype=torch.float64, device=D.device)
+        ws = self.checkpoint_workspace(n) if workspace is None else workspace
+        st = load().brdc_dstebr_backward(
+            self.h, n, ctypes.c_void_p(D.data_ptr()), ctypes.c_void_p(E.data_ptr()),
+            ctypes.c_void_p(G.data_ptr()), ctypes.c_void_p(gD.data_ptr()),
+            ctypes.c_void_p(gE.data_ptr()), ctypes.c_void_p(ws.data_ptr()), ws.numel(),
+            1 if keep_forward else 0,
+        )
+        _check(st, "brdc_dstebr_backward", self.h)
+        return gD, gE[: max(n - 1, 0)]
+
     def dstebr_noalloc(self, D, E, W=None):
         """Solve with the library's static scratch (n <= 16384); no
         workspace is allocated by anyone."""

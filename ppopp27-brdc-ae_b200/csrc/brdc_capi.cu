@@ -18,7 +18,7 @@
 #include <new>
 #include <vector>
 
-#include "brdc_kernels.cuh"
+#include "brdc_backward.cuh"
 
 using namespace brdc;
 
@@ -121,108 +121,144 @@ bool build_forest(int B, const long long *off, HostForest *f) {
     return true;
 }
 
-enum DArr {
-    A_cd, A_cf, A_cl, A_nd, A_nf, A_nl, A_md, A_mz, A_mf, A_ml, A_ad, A_az,
-    A_af, A_al, A_gc, A_gs, A_zd, A_zf, A_zl, A_gd, A_gf, A_gl, A_NDN
-};
-enum PArr { P_pd, P_pz, P_pf, P_pl, P_pw, P_rdo, P_rtau, P_rlam, P_rf, P_rl, P_NDP };
-enum IArr { I_mflag, I_morig, I_amap, I_gmark, I_gbase, I_NIN };
-enum QArr { Q_pmap, Q_rorg, Q_NIP };
+// Workspace descriptor: every array with its element size, its length
+// class and whether a checkpointing workspace keeps one slice per level
+// (the arrays the adjoint reads back).
+enum CountKind { CN_NT, CN_NP, CN_NN, CN_NN1, CN_ITW, CN_ITC, CN_B1, CN_B, CN_NODEPRE };
 
-Layout make_layout(const HostForest &f) {
+struct SlotDesc {
+    int kind;        // 0 double*, 1 int*, 2 long long*
+    double *Ws::*fd;
+    int *Ws::*fi;
+    long long *Ws::*fl;
+    CountKind count;
+    bool per_level;
+    bool adjoint;
+};
+
+#define SD(field, cnt, pl, adj) {0, &Ws::field, nullptr, nullptr, cnt, pl, adj}
+#define SI(field, cnt, pl, adj) {1, nullptr, &Ws::field, nullptr, cnt, pl, adj}
+#define SL(field, cnt, pl, adj) {2, nullptr, nullptr, &Ws::field, cnt, pl, adj}
+
+const SlotDesc kSlots[] = {
+    SD(cd, CN_NT, false, false), SD(cf, CN_NT, false, false), SD(cl, CN_NT, false, false),
+    SD(nd, CN_NT, false, false), SD(nf, CN_NT, false, false), SD(nl, CN_NT, false, false),
+    SD(md, CN_NT, false, false), SD(mz, CN_NT, false, false), SD(mf, CN_NT, false, false),
+    SD(ml, CN_NT, false, false), SI(morig, CN_NT, true, false),
+    SD(ad, CN_NT, false, false), SD(az, CN_NT, false, false), SD(af, CN_NT, true, false),
+    SD(al, CN_NT, true, false), SI(amap, CN_NT, true, false), SI(gmark, CN_NT, true, false),
+    SI(gbase, CN_NT, true, false), SI(gpos, CN_NT, true, false), SD(gc, CN_NT, true, false), SD(gs, CN_NT, true, false),
+    SD(gr, CN_NT, true, false),
+    SD(zd, CN_NT, true, false), SD(zf, CN_NT, true, false), SD(zl, CN_NT, true, false),
+    SI(zmap, CN_NT, true, false),
+    SD(gd, CN_NT, true, false), SD(gf, CN_NT, false, false), SD(gl, CN_NT, false, false),
+    SD(pd, CN_NP, true, false), SD(pz, CN_NP, true, false), SD(pf, CN_NP, true, false),
+    SD(pl, CN_NP, true, false), SD(pw, CN_NP, true, false), SI(pmap, CN_NP, true, false),
+    SI(rorg, CN_NP, true, false), SD(rdo, CN_NP, true, false), SD(rtau, CN_NP, true, false),
+    SD(rlam, CN_NP, true, false), SD(rf, CN_NP, false, false), SD(rl, CN_NP, false, false),
+    SI(nK, CN_NN, true, false), SI(nKz, CN_NN, true, false), SD(nrho, CN_NN, true, false),
+    SD(ntol, CN_NN, false, false), SD(nzn, CN_NN, false, false),
+    SI(pref_w, CN_NN1, true, false), SI(pref_c, CN_NN1, true, false),
+    SI(items_w, CN_ITW, true, false), SI(items_c, CN_ITC, true, false),
+    SL(f_off, CN_B1, false, false), SI(f_lev, CN_B, false, false),
+    SI(f_node_prefix, CN_NODEPRE, false, false), SI(f_leaf_prefix, CN_B1, false, false),
+    // adjoint
+    SD(bcd, CN_NT, false, true), SD(bcf, CN_NT, false, true), SD(bcl, CN_NT, false, true),
+    SD(bnd, CN_NT, false, true), SD(bnf, CN_NT, false, true), SD(bnl, CN_NT, false, true),
+    SD(bmd, CN_NT, false, true), SD(bmz, CN_NT, false, true), SD(bmf, CN_NT, false, true),
+    SD(bml, CN_NT, false, true), SD(bad, CN_NT, false, true), SD(baz, CN_NT, false, true),
+    SD(baf, CN_NT, false, true), SD(bal, CN_NT, false, true), SD(bzd, CN_NT, false, true),
+    SD(bzf, CN_NT, false, true), SD(bzl, CN_NT, false, true), SD(bgd, CN_NT, false, true),
+    SD(bgf, CN_NT, false, true), SD(bgl, CN_NT, false, true),
+    SD(blam, CN_NP, false, true), SD(bfr, CN_NP, false, true), SD(blr, CN_NP, false, true),
+    SD(rinvn, CN_NP, false, true), SD(rh, CN_NP, false, true), SD(rkap, CN_NP, false, true),
+    SD(rcdo, CN_NP, false, true), SD(rczo, CN_NP, false, true),
+    SD(rfp, CN_NP, false, true), SD(rlp, CN_NP, false, true),
+    SD(bzz, CN_NT, false, true), SD(bgw, CN_NT, false, true),
+    SD(bpd, CN_NP, false, true), SD(bpz, CN_NP, false, true), SD(bpf, CN_NP, false, true),
+    SD(bpl, CN_NP, false, true), SD(rkr, CN_NP, false, true), SD(wtmp, CN_NT, false, true),
+};
+
+long long slot_count(CountKind c, const HostForest &f, const Layout &L) {
+    switch (c) {
+    case CN_NT: return L.nt;
+    case CN_NP: return L.np;
+    case CN_NN: return L.nn0;
+    case CN_NN1: return L.nn0 + 1;
+    case CN_ITW: return L.nt + L.nn0 + 2;
+    case CN_ITC: return L.nt / 8 + L.nn0 + 2;
+    case CN_B1: return f.B > 1 ? f.B + 1 : 0;
+    case CN_B: return f.B > 1 ? f.B : 0;
+    case CN_NODEPRE: return f.B > 1 ? (long long)(f.B + 1) * std::max(f.max_levels, 1) : 0;
+    }
+    return 0;
+}
+
+// Compute the layout; when base is given, also point every Ws array at it.
+Layout plan_workspace(const HostForest &f, bool ckpt, void *base, Ws *w) {
     Layout L{};
     L.nt = f.total_n;
     L.nn0 = f.nn0;
     L.np = f.total_n + f.nn0 + 4;
-    size_t cur = 0;
-    L.o_hdr = cur;
-    cur = align_up(cur + sizeof(WsHeader));
-    for (int i = 0; i < A_NDN; ++i) {
-        L.o_d[i] = cur;
-        cur = align_up(cur + sizeof(double) * (size_t)L.nt);
+    L.levels = f.max_levels;
+    L.ckpt = ckpt;
+    size_t cur = align_up(sizeof(WsHeader));
+    char *b = static_cast<char *>(base);
+    if (w != nullptr) {
+        *w = Ws{};
+        w->hdr = reinterpret_cast<WsHeader *>(b);
     }
-    for (int i = 0; i < P_NDP; ++i) {
-        L.o_d[A_NDN + i] = cur;
-        cur = align_up(cur + sizeof(double) * (size_t)L.np);
-    }
-    for (int i = 0; i < I_NIN; ++i) {
-        L.o_i[i] = cur;
-        cur = align_up(cur + sizeof(int) * (size_t)L.nt);
-    }
-    for (int i = 0; i < Q_NIP; ++i) {
-        L.o_i[I_NIN + i] = cur;
-        cur = align_up(cur + sizeof(int) * (size_t)L.np);
-    }
-    // per-node arrays: nK, nKz (int), nrho, ntol, nzn (double), prefixes
-    L.o_i[I_NIN + Q_NIP + 0] = cur;
-    cur = align_up(cur + sizeof(int) * (size_t)L.nn0);
-    L.o_i[I_NIN + Q_NIP + 1] = cur;
-    cur = align_up(cur + sizeof(int) * (size_t)L.nn0);
-    L.o_i[I_NIN + Q_NIP + 2] = cur;
-    cur = align_up(cur + sizeof(int) * (size_t)(L.nn0 + 1));
-    L.o_i[I_NIN + Q_NIP + 3] = cur;
-    cur = align_up(cur + sizeof(int) * (size_t)(L.nn0 + 1));
-    L.o_i[I_NIN + Q_NIP + 4] = cur;
-    cur = align_up(cur + sizeof(int) * (size_t)(L.nt + L.nn0 + 2));
-    L.o_i[I_NIN + Q_NIP + 5] = cur;
-    cur = align_up(cur + sizeof(int) * (size_t)(L.nt / 8 + L.nn0 + 2));
-    L.o_d[A_NDN + P_NDP + 0] = cur;
-    cur = align_up(cur + sizeof(double) * (size_t)L.nn0);
-    L.o_d[A_NDN + P_NDP + 1] = cur;
-    cur = align_up(cur + sizeof(double) * (size_t)L.nn0);
-    L.o_d[A_NDN + P_NDP + 2] = cur;
-    cur = align_up(cur + sizeof(double) * (size_t)L.nn0);
-    // forest tables (batched only)
-    if (f.B > 1) {
-        L.o_f_off = cur;
-        cur = align_up(cur + sizeof(long long) * (size_t)(f.B + 1));
-        L.o_f_lev = cur;
-        cur = align_up(cur + sizeof(int) * (size_t)f.B);
-        L.o_f_node_prefix = cur;
-        cur = align_up(cur + sizeof(int) * (size_t)(f.B + 1) *
-                                 (size_t)std::max(f.max_levels, 1));
-        L.o_f_leaf_prefix = cur;
-        cur = align_up(cur + sizeof(int) * (size_t)(f.B + 1));
+    for (const SlotDesc &sd : kSlots) {
+        if (sd.adjoint && !ckpt) {
+            continue;
+        }
+        const long long cnt = slot_count(sd.count, f, L);
+        if (cnt == 0) {
+            continue;
+        }
+        const size_t elem = sd.kind == 0 ? sizeof(double) : (sd.kind == 1 ? sizeof(int) : sizeof(long long));
+        const long long reps = (ckpt && sd.per_level) ? std::max(f.max_levels, 1) : 1;
+        if (w != nullptr) {
+            char *p = b + cur;
+            if (sd.kind == 0) {
+                w->*(sd.fd) = reinterpret_cast<double *>(p);
+            } else if (sd.kind == 1) {
+                w->*(sd.fi) = reinterpret_cast<int *>(p);
+            } else {
+                w->*(sd.fl) = reinterpret_cast<long long *>(p);
+            }
+        }
+        cur = align_up(cur + elem * (size_t)cnt * (size_t)reps);
     }
     L.bytes = align_up(cur);
     return L;
 }
 
-Ws carve(void *base, const Layout &L) {
-    char *b = static_cast<char *>(base);
-    Ws w{};
-    w.hdr = reinterpret_cast<WsHeader *>(b + L.o_hdr);
-    double **dp[A_NDN] = {&w.cd, &w.cf, &w.cl, &w.nd, &w.nf, &w.nl, &w.md, &w.mz,
-                          &w.mf, &w.ml, &w.ad, &w.az, &w.af, &w.al, &w.gc, &w.gs,
-                          &w.zd, &w.zf, &w.zl, &w.gd, &w.gf, &w.gl};
-    for (int i = 0; i < A_NDN; ++i) {
-        *dp[i] = reinterpret_cast<double *>(b + L.o_d[i]);
+// Point the checkpointed arrays of *w at level k's slice.
+void level_view(const HostForest &f, const Layout &L, const Ws &base, int k, Ws *w) {
+    if (!L.ckpt) {
+        return;
     }
-    double **pp[P_NDP] = {&w.pd, &w.pz, &w.pf, &w.pl, &w.pw, &w.rdo, &w.rtau, &w.rlam, &w.rf, &w.rl};
-    for (int i = 0; i < P_NDP; ++i) {
-        *pp[i] = reinterpret_cast<double *>(b + L.o_d[A_NDN + i]);
+    for (const SlotDesc &sd : kSlots) {
+        if (!sd.per_level || sd.adjoint) {
+            continue;
+        }
+        const long long cnt = slot_count(sd.count, f, L);
+        if (sd.kind == 0) {
+            w->*(sd.fd) = base.*(sd.fd) + (size_t)k * (size_t)cnt;
+        } else if (sd.kind == 1) {
+            w->*(sd.fi) = base.*(sd.fi) + (size_t)k * (size_t)cnt;
+        }
     }
-    int **ip[I_NIN] = {&w.mflag, &w.morig, &w.amap, &w.gmark, &w.gbase};
-    for (int i = 0; i < I_NIN; ++i) {
-        *ip[i] = reinterpret_cast<int *>(b + L.o_i[i]);
-    }
-    w.pmap = reinterpret_cast<int *>(b + L.o_i[I_NIN + Q_pmap]);
-    w.rorg = reinterpret_cast<int *>(b + L.o_i[I_NIN + Q_rorg]);
-    w.nK = reinterpret_cast<int *>(b + L.o_i[I_NIN + Q_NIP + 0]);
-    w.nKz = reinterpret_cast<int *>(b + L.o_i[I_NIN + Q_NIP + 1]);
-    w.pref_w = reinterpret_cast<int *>(b + L.o_i[I_NIN + Q_NIP + 2]);
-    w.pref_c = reinterpret_cast<int *>(b + L.o_i[I_NIN + Q_NIP + 3]);
-    w.items_w = reinterpret_cast<int *>(b + L.o_i[I_NIN + Q_NIP + 4]);
-    w.items_c = reinterpret_cast<int *>(b + L.o_i[I_NIN + Q_NIP + 5]);
-    w.nrho = reinterpret_cast<double *>(b + L.o_d[A_NDN + P_NDP + 0]);
-    w.ntol = reinterpret_cast<double *>(b + L.o_d[A_NDN + P_NDP + 1]);
-    w.nzn = reinterpret_cast<double *>(b + L.o_d[A_NDN + P_NDP + 2]);
-    if (L.o_f_off != 0) {
-        w.f_off = reinterpret_cast<long long *>(b + L.o_f_off);
-        w.f_lev = reinterpret_cast<int *>(b + L.o_f_lev);
-        w.f_node_prefix = reinterpret_cast<int *>(b + L.o_f_node_prefix);
-        w.f_leaf_prefix = reinterpret_cast<int *>(b + L.o_f_leaf_prefix);
-    }
+}
+
+Layout make_layout(const HostForest &f, bool ckpt = false) {
+    return plan_workspace(f, ckpt, nullptr, nullptr);
+}
+
+Ws carve(void *base, const HostForest &f, bool ckpt) {
+    Ws w;
+    plan_workspace(f, ckpt, base, &w);
     return w;
 }
 
@@ -280,8 +316,9 @@ void mark(brdc_handle h, int slot) {
 }
 
 // Enqueue the whole forward solve.
-brdc_status run_forest(brdc_handle h, const HostForest &hf, const Forest &F,
-                       const Ws &w, const double *D, const double *E, double *W) {
+brdc_status run_forest(brdc_handle h, const HostForest &hf, const Layout &L,
+                       const Forest &F, const Ws &w, const double *D,
+                       const double *E, double *W) {
     cudaStream_t s = h->stream;
     BRDC_CUDA(h, "brdc.set_attributes", set_attrs());
     h->ev_used = 0;
@@ -316,6 +353,7 @@ brdc_status run_forest(brdc_handle h, const HostForest &hf, const Forest &F,
         a.k = k;
         a.nodes = hf.level_nodes[k];
         a.level_rows = hf.level_rows[k];
+        level_view(hf, L, w, k, &a.w);
         // CTA-role blocks exist only where a merge can exceed kWarpMaxK poles
         const int cta_blocks = hf.level_mmax[k] > kWarpMaxK ? h->sm_count * 2 : 0;
         const int grid = cta_blocks + warp_blocks;
@@ -466,13 +504,12 @@ extern "C" brdc_status brdc_dstebr_workspace_size(int64_t n, int flags,
     if (n <= 0 || n > (1LL << 30)) {
         return BRDC_STATUS_INVALID_VALUE;
     }
-    (void)flags;
     const long long off[2] = {0, (long long)n};
     HostForest f;
     if (!build_forest(1, off, &f)) {
         return BRDC_STATUS_INVALID_VALUE;
     }
-    *bytes = make_layout(f).bytes;
+    *bytes = make_layout(f, (flags & BRDC_FLAG_KEEP_CHECKPOINTS) != 0).bytes;
     return BRDC_STATUS_SUCCESS;
 }
 
@@ -493,17 +530,21 @@ extern "C" brdc_status brdc_dstebr(brdc_handle h, int64_t n, const double *d_D,
     if (!build_forest(1, off, &hf)) {
         return BRDC_STATUS_INVALID_VALUE;
     }
-    const Layout L = make_layout(hf);
+    // A workspace sized with BRDC_FLAG_KEEP_CHECKPOINTS records the
+    // per-level state that brdc_dstebr_backward reads.
+    const Layout Lc = make_layout(hf, true);
+    const bool ckpt = workspace != nullptr && workspace_size >= Lc.bytes;
+    const Layout L = ckpt ? Lc : make_layout(hf, false);
     if (workspace == nullptr || workspace_size < L.bytes) {
         return BRDC_STATUS_INVALID_WORKSPACE;
     }
-    const Ws w = carve(workspace, L);
+    const Ws w = carve(workspace, hf, ckpt);
     Forest F{};
     F.B = 1;
     F.max_levels = hf.max_levels;
     F.n0 = n;
     F.L0 = hf.max_levels;
-    return run_forest(h, hf, F, w, d_D, d_E, d_W);
+    return run_forest(h, hf, L, F, w, d_D, d_E, d_W);
 }
 
 extern "C" brdc_status brdc_get_info(brdc_handle h, const void *workspace,
@@ -654,7 +695,7 @@ extern "C" brdc_status brdc_dstebr_batched(brdc_handle h, int64_t count,
     if (workspace == nullptr || workspace_size < L.bytes) {
         return BRDC_STATUS_INVALID_WORKSPACE;
     }
-    const Ws w = carve(workspace, L);
+    const Ws w = carve(workspace, hf, false);
     Forest F{};
     F.B = hf.B;
     F.max_levels = hf.max_levels;
@@ -707,29 +748,144 @@ extern "C" brdc_status brdc_dstebr_batched(brdc_handle h, int64_t count,
         F.node_prefix = w.f_node_prefix;
         F.leaf_prefix = w.f_leaf_prefix;
     }
-    return run_forest(h, hf, F, w, d_D, d_E, d_W);
+    return run_forest(h, hf, L, F, w, d_D, d_E, d_W);
 }
 
 // -------------------------------------------------------------- backward
+namespace {
+
+template <int T>
+void launch_undeflate(const BArgs &b, int grid, cudaStream_t s) {
+    k_bw_undeflate<T><<<grid, T, 0, s>>>(b);
+}
+
+void launch_undeflate_sized(const BArgs &b, int mmax, cudaStream_t s) {
+    int t = 32;
+    while (t < 1024 && t * 4 < mmax) {
+        t <<= 1;
+    }
+    switch (t) {
+    case 32: launch_undeflate<32>(b, b.nodes, s); break;
+    case 64: launch_undeflate<64>(b, b.nodes, s); break;
+    case 128: launch_undeflate<128>(b, b.nodes, s); break;
+    case 256: launch_undeflate<256>(b, b.nodes, s); break;
+    case 512: launch_undeflate<512>(b, b.nodes, s); break;
+    default: launch_undeflate<1024>(b, b.nodes, s); break;
+    }
+}
+
+// Reverse pass over a workspace holding the forward solve's checkpoints.
+brdc_status run_backward(brdc_handle h, const HostForest &hf, const Layout &L,
+                         const Forest &F, const Ws &w, const double *D,
+                         const double *E, const double *G, double *gD, double *gE) {
+    cudaStream_t s = h->stream;
+    const long long nt = hf.total_n;
+    long long eg = (nt + 255) / 256;
+    eg = std::max<long long>(1, std::min<long long>(eg, (long long)h->sm_count * 8));
+    if (nt > 1) {
+        k_bw_zero<<<(unsigned)eg, 256, 0, s>>>(gE, nt - 1);
+        BRDC_CUDA(h, "brdc.bw.zero_ge", cudaGetLastError());
+    }
+    double *par[3] = {w.bnd, w.bnf, w.bnl};
+    double *out[3] = {w.bcd, w.bcf, w.bcl};
+    const int wgrid = h->sm_count * 2;
+    long long dgrid = (nt + 7) / 8;
+    dgrid = std::max<long long>(1, std::min<long long>(dgrid, (long long)h->sm_count * 16));
+    for (int k = hf.max_levels - 1; k >= 0; --k) {
+        Ws wl = w;
+        level_view(hf, L, w, k, &wl);
+        wl.bnd = par[0];
+        wl.bnf = par[1];
+        wl.bnl = par[2];
+        wl.bcd = out[0];
+        wl.bcf = out[1];
+        wl.bcl = out[2];
+        BArgs b{};
+        b.F = F;
+        b.w = wl;
+        b.D = D;
+        b.E = E;
+        b.G = G;
+        b.gD = gD;
+        b.gE = gE;
+        b.k = k;
+        b.nodes = hf.level_nodes[k];
+        k_bw_unplace<<<(unsigned)eg, 256, 0, s>>>(b, nt);
+        k_bw_roots<<<wgrid, kSweepThreads, 0, s>>>(b);
+        k_bw_poles<<<wgrid, kSweepThreads, 0, s>>>(b);
+        if (k + 1 < hf.max_levels || hf.B > 1) {
+            k_bw_defl<<<(unsigned)dgrid, 256, 0, s>>>(b, nt);
+        }
+        launch_undeflate_sized(b, hf.level_mmax[k], s);
+        BRDC_CUDA(h, "brdc.bw.level", cudaGetLastError());
+        std::swap(par[0], out[0]);
+        std::swap(par[1], out[1]);
+        std::swap(par[2], out[2]);
+    }
+    Ws wl = w;
+    wl.bcd = par[0];
+    wl.bcf = par[1];
+    wl.bcl = par[2];
+    BArgs b{};
+    b.F = F;
+    b.w = wl;
+    b.D = D;
+    b.E = E;
+    b.G = G;
+    b.gD = gD;
+    b.gE = gE;
+    const long long per = 2LL * kLeafWarps;
+    long long grid = (hf.leaves + per - 1) / per;
+    grid = std::max<long long>(1, std::min<long long>(grid, (long long)h->sm_count * 16));
+    k_bw_leaf<<<(unsigned)grid, kLeafWarps * 32, 0, s>>>(b, hf.leaves);
+    BRDC_CUDA(h, "brdc.bw.leaf", cudaGetLastError());
+    long long cg = (hf.leaves + 255) / 256;
+    cg = std::max<long long>(1, std::min<long long>(cg, (long long)h->sm_count * 8));
+    k_bw_cuts<<<(unsigned)cg, 256, 0, s>>>(b, hf.leaves);
+    BRDC_CUDA(h, "brdc.bw.cuts", cudaGetLastError());
+    return BRDC_STATUS_SUCCESS;
+}
+
+} // namespace
+
 extern "C" brdc_status brdc_dstebr_backward(brdc_handle h, int64_t n,
                                             const double *d_D, const double *d_E,
                                             const double *d_G, double *d_gD,
                                             double *d_gE, void *workspace,
                                             size_t workspace_size,
                                             int keep_forward) {
-    (void)n;
-    (void)d_D;
-    (void)d_E;
-    (void)d_G;
-    (void)d_gD;
-    (void)d_gE;
-    (void)workspace;
-    (void)workspace_size;
-    (void)keep_forward;
     if (h == nullptr) {
         return BRDC_STATUS_INVALID_HANDLE;
     }
-    return BRDC_STATUS_NOT_IMPLEMENTED;
+    if (d_D == nullptr || d_G == nullptr || d_gD == nullptr ||
+        (n > 1 && (d_E == nullptr || d_gE == nullptr))) {
+        return BRDC_STATUS_INVALID_POINTER;
+    }
+    if (n <= 0 || n > (1LL << 30)) {
+        return BRDC_STATUS_INVALID_VALUE;
+    }
+    const long long off[2] = {0, (long long)n};
+    HostForest hf;
+    if (!build_forest(1, off, &hf)) {
+        return BRDC_STATUS_INVALID_VALUE;
+    }
+    const Layout L = make_layout(hf, true);
+    if (workspace == nullptr || workspace_size < L.bytes) {
+        return BRDC_STATUS_INVALID_WORKSPACE;
+    }
+    const Ws w = carve(workspace, hf, true);
+    Forest F{};
+    F.B = 1;
+    F.max_levels = hf.max_levels;
+    F.n0 = n;
+    F.L0 = hf.max_levels;
+    if (!keep_forward) {
+        const brdc_status st = run_forest(h, hf, L, F, w, d_D, d_E, w.wtmp);
+        if (st != BRDC_STATUS_SUCCESS) {
+            return st;
+        }
+    }
+    return run_backward(h, hf, L, F, w, d_D, d_E, d_G, d_gD, d_gE);
 }
 
 // ------------------------------------------------- LAPACK-style host entry
@@ -911,11 +1067,11 @@ extern "C" brdc_status brdc_dstebr_noalloc(brdc_handle h, int64_t n,
     // Every array the solve reads is written earlier in the same solve and
     // k_init clears the header counters, so the contents left by a previous
     // call need no clearing here.
-    const Ws w = carve(scratch, L);
+    const Ws w = carve(scratch, hf, false);
     Forest F{};
     F.B = 1;
     F.max_levels = hf.max_levels;
     F.n0 = n;
     F.L0 = hf.max_levels;
-    return run_forest(h, hf, F, w, d_D, d_E, d_W);
+    return run_forest(h, hf, L, F, w, d_D, d_E, d_W);
 }

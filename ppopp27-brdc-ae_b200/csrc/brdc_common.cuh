@@ -20,7 +20,7 @@
 // node's slice starts 16-byte aligned for cp.async.bulk):
 //   cur_{d,f,l} / nxt_{d,f,l}  node eigenvalues (ascending) with the first
 //                              and last rows of the node eigenvector matrix
-//   m{d,z,f,l}, mflag         merged child lists (sorted) with z and rows
+//   m{d,z,f,l}, morig         merged child lists (sorted) with z and rows
 //   a{d,z,f,l}                poles that survived the small-z test
 //   z{d,f,l}, g{d,f,l}        deflated by the small-z test / by rotation
 //   p{d,z,f,l}, pw            the K secular poles, their z and Loewner z
@@ -110,27 +110,42 @@ struct Ws {
     double *nd, *nf, *nl;
     // merged lists
     double *md, *mz, *mf, *ml;
-    int *mflag, *morig;
+    int *morig;                  // merged position -> row within the node
     // small-z survivors, deflated lists
     double *ad, *az, *af, *al;
-    int *amap, *gmark, *gbase;
-    double *gc, *gs;
+    int *amap;                   // active position -> merged position
+    int *gmark, *gbase;          // rotated-out flag, cluster base
+    int *gpos;                   // rotated-out list index -> active index
+    double *gc, *gs, *gr;        // rotation of each rotated-out pole
     double *zd, *zf, *zl;
+    int *zmap;                   // small-z list index -> merged position
     double *gd, *gf, *gl;
     // poles and roots (padded layout)
     double *pd, *pz, *pf, *pl, *pw;
-    int *pmap;
+    int *pmap;                   // pole -> active position
     int *rorg;
     double *rdo, *rtau, *rlam;
+    double *rf, *rl;             // new boundary rows of each root (padded)
     // per node at one level
     int *nK, *nKz;
     double *nrho, *ntol, *nzn;
     int *pref_w, *pref_c;        // first work item of each merge (per role)
     int *items_w, *items_c;      // work item -> merge node (per role)
-    double *rf, *rl;             // new boundary rows of each root (padded)
     // forest tables (batched)
     long long *f_off;
     int *f_lev, *f_node_prefix, *f_leaf_prefix;
+    // adjoint (present when the workspace keeps checkpoints)
+    double *bcd, *bcf, *bcl, *bnd, *bnf, *bnl;   // cotangents, ping-pong
+    double *bmd, *bmz, *bmf, *bml;               // at merged positions
+    double *bad, *baz, *baf, *bal;               // at active positions
+    double *bzd, *bzf, *bzl, *bgd, *bgf, *bgl;   // deflated lists
+    double *blam, *bfr, *blr;                    // per root (padded)
+    double *rinvn, *rh, *rkap, *rcdo, *rczo;     // per root (padded)
+    double *rfp, *rlp;                           // per root: new rows
+    double *bzz, *bgw;                           // deflated: dL/dz, dL/domega
+    double *bpd, *bpz, *bpf, *bpl;               // per pole (padded)
+    double *rkr;                                 // per root: its drho term
+    double *wtmp;                                // eigenvalues of the re-run
 };
 
 struct Layout {
@@ -138,10 +153,8 @@ struct Layout {
     long long nt;     // total rows
     long long np;     // padded pole-array length
     long long nn0;    // nodes of the widest level
-    size_t o_hdr;
-    size_t o_d[40];
-    size_t o_i[16];
-    size_t o_f_off, o_f_lev, o_f_node_prefix, o_f_leaf_prefix;
+    int levels;
+    bool ckpt;
 };
 
 #if defined(__CUDACC__)
@@ -177,6 +190,19 @@ __device__ inline int upper_bound_int(const int *a, int n, int x) {
     while (lo < hi) {
         const int mid = (lo + hi) >> 1;
         if (a[mid] <= x) {
+            lo = mid + 1;
+        } else {
+            hi = mid;
+        }
+    }
+    return lo;
+}
+
+__device__ inline int lower_bound_int(const int *a, int n, int x) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (a[mid] < x) {
             lo = mid + 1;
         } else {
             hi = mid;

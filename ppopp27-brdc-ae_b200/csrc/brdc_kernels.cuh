@@ -377,6 +377,7 @@ __global__ void __launch_bounds__(T) k_merge_deflate(KArgs a) {
                     w.zd[o] = vd[q];
                     w.zf[o] = vf[q];
                     w.zl[o] = vl[q];
+                    w.zmap[o] = idx;
                     ++rz;
                 }
             }
@@ -431,6 +432,7 @@ __global__ void __launch_bounds__(T) k_merge_deflate(KArgs a) {
             w.gmark[gs + x] = 1;
             w.gc[gs + x] = c;
             w.gs[gs + x] = s;
+            w.gr[gs + x] = r;
             w.gbase[gs + x] = base;
             ++x;
         }
@@ -482,6 +484,7 @@ __global__ void __launch_bounds__(T) k_merge_deflate(KArgs a) {
                     w.gd[o] = vd[q];
                     w.gf[o] = vf[q];
                     w.gl[o] = vl[q];
+                    w.gpos[o] = idx;
                     ++rg;
                 }
             }
