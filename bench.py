@@ -358,6 +358,10 @@ def collect_extras(torch, brdc, families, solver, D, E, W, ws, d, e, flush, args
                   "h2d_bytes_per_step": int(hD.numel() * 8 + hE.numel() * 8),
                   "d2h_bytes_per_step": int(hW.numel() * 8)}
 
+    out["fwd_bwd"] = bench_fwd_bwd(torch, families, solver, flush, args)
+    out["batched"] = bench_batched(torch, brdc, families, solver, flush)
+    out["fit"] = bench_fit(torch, brdc, families, flush)
+
     # CPU baseline: the oracle on a bounded sample of the same workload
     cpu_t, threads = cpu_reference_times(d, e, args.cpu_budget)
     out["cpu_baseline"] = {"value": float(np.median(cpu_t)), "unit": "ms", "cores": threads,
@@ -365,6 +369,211 @@ def collect_extras(torch, brdc, families, solver, D, E, W, ws, d, e, flush, args
                            "sample": f"{len(cpu_t)} full solves of the headline input "
                                      f"(oracle restatement of DSTEDC_DC_BR, OpenMP)"}
     return out
+
+
+def _event_ms(torch, fn, reps, flush, stream=None):
+    stream = stream or torch.cuda.current_stream()
+    out = []
+    for _ in range(reps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        out.append(e0.elapsed_time(e1))
+    return float(np.mean(out))
+
+
+def bench_fwd_bwd(torch, families, solver, flush, args):
+    """Differentiated solve, normal family, L = sum g_i lambda_i: forward
+    with checkpoints plus the adjoint, against the plain forward."""
+    res = {}
+    for n in (4096, 16384, N_HEAD):
+        d, e = families.generate("normal", n)
+        D = torch.tensor(d, device="cuda")
+        E = torch.tensor(e, device="cuda")
+        G = torch.tensor(np.random.Generator(np.random.PCG64([2, n, 1])).standard_normal(n),
+                         device="cuda")
+        W = torch.empty(n, dtype=torch.float64, device="cuda")
+        gD = torch.empty(n, dtype=torch.float64, device="cuda")
+        gE = torch.empty(n, dtype=torch.float64, device="cuda")
+        ws = solver.workspace(n)
+        wsc = solver.checkpoint_workspace(n)
+
+        def fwd():
+            solver.dstebr(D, E, W=W, workspace=ws)
+
+        def fwd_c():
+            solver.dstebr(D, E, W=W, workspace=wsc)
+
+        def bwd():
+            solver.dstebr_backward(D, E, G, workspace=wsc, keep_forward=True, gD=gD, gE=gE)
+
+        def both():
+            fwd_c()
+            bwd()
+
+        for _ in range(3):
+            both()
+            fwd()
+        torch.cuda.synchronize()
+        reps = 10
+        t_f = _event_ms(torch, fwd, reps, flush)
+        t_fc = _event_ms(torch, fwd_c, reps, flush)
+        t_fb = _event_ms(torch, both, reps, flush)
+        res[str(n)] = {"fwd_ms": t_f, "fwd_checkpointed_ms": t_fc, "fwd_bwd_ms": t_fb,
+                       "bwd_ms": t_fb - t_fc, "ratio_fwd_bwd_to_fwd": t_fb / t_f,
+                       "workspace_bytes": ws.numel(), "checkpoint_workspace_bytes": wsc.numel()}
+        del ws, wsc
+        solver._ws.clear()
+    return {"family": "normal", "loss": "sum g_i lambda_i, g ~ N(0,1)",
+            "l2": "flushed before every timed call", "by_n": res}
+
+
+def bench_batched(torch, brdc, families, solver, flush):
+    """4096 tridiagonals, N log-uniform in [32, 8192], the four families
+    mixed: one batched solve replayed from a CUDA graph, against looping the
+    plain single-matrix entry over the same instances."""
+    count = 4096
+    off, D, E, orders, fams = families.batch(count, 32, 8192, seed=3)
+    Dt = torch.tensor(D, device="cuda")
+    Et = torch.tensor(E, device="cuda")
+    W = torch.empty(int(off[-1]), dtype=torch.float64, device="cuda")
+    ws = solver.batched_workspace(off)
+    stream = torch.cuda.Stream()
+    stream.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(stream):
+        solver.set_stream(stream)
+        solver.dstebr_batched(off, Dt, Et, W=W, workspace=ws)  # uploads the forest tables
+        stream.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=stream):
+            solver.dstebr_batched(off, Dt, Et, W=W, workspace=ws)
+        g.replay()
+        stream.synchronize()
+        t_graph = _event_ms(torch, g.replay, 5, flush, stream)
+        t_eager = _event_ms(torch, lambda: solver.dstebr_batched(off, Dt, Et, W=W, workspace=ws),
+                            5, flush, stream)
+    solver.set_stream(torch.cuda.current_stream())
+    torch.cuda.synchronize()
+    Wb = W.cpu().numpy()
+    del g
+
+    # the plain entry looped over the instances, one shared workspace
+    nmax = int(np.max(orders))
+    ws1 = solver.workspace(nmax)
+    W1 = torch.empty_like(W)
+    views = [(Dt[int(off[b]):int(off[b + 1])], Et[int(off[b]):int(off[b + 1]) - 1],
+              W1[int(off[b]):int(off[b + 1])]) for b in range(count)]
+
+    def loop():
+        for Db, Eb, Wb_ in views:
+            solver.dstebr(Db, Eb if Eb.numel() else Db, W=Wb_, workspace=ws1)
+
+    loop()
+    torch.cuda.synchronize()
+    t_loop = _event_ms(torch, loop, 1, flush)
+    same = float(np.max(np.abs(W1.cpu().numpy() - Wb)))
+
+    # per-instance error against LAPACK on every 16th instance
+    import scipy.linalg
+
+    errs = []
+    for b in range(0, count, 16):
+        lo, hi = int(off[b]), int(off[b + 1])
+        ref = scipy.linalg.eigvalsh_tridiagonal(D[lo:hi], E[lo:hi - 1])
+        errs.append(float(np.max(np.abs(Wb[lo:hi] - ref)) / np.max(np.abs(ref))))
+    return {"count": count, "orders": "log-uniform [32, 8192]", "rows": int(off[-1]),
+            "families": "uniform, normal, toeplitz, clustered in turn",
+            "graph_ms": t_graph, "eager_batched_ms": t_eager, "looped_plain_ms": t_loop,
+            "solves_per_s": count * 1e3 / t_graph,
+            "looped_solves_per_s": count * 1e3 / t_loop,
+            "speedup_vs_looped": t_loop / t_graph,
+            "max_abs_diff_batched_vs_looped": same,
+            "max_rel_err_vs_lapack": max(errs),
+            "lapack_sample": f"{len(errs)} instances (every 16th)",
+            "workspace_bytes": ws.numel()}
+
+
+def bench_fit(torch, brdc, families, flush, steps=200, lr=0.1):
+    """Inverse eigenvalue fit: 1024 tridiagonals, N log-uniform in [64,
+    4096], normal family; loss sum (lambda_i - t_i)^2 with targets the
+    eigenvalues of a second seeded tridiagonal of the same N; 200 gradient
+    steps (batched forward with checkpoints, batched adjoint, update of D
+    and E) captured in one CUDA graph."""
+    count = 1024
+    orders = families.batch_orders(count, 64, 4096, seed=4)
+    off = np.zeros(count + 1, dtype=np.int64)
+    off[1:] = np.cumsum(orders)
+    tot = int(off[-1])
+    D = np.empty(tot)
+    E = np.zeros(tot)
+    D2 = np.empty(tot)
+    E2 = np.zeros(tot)
+    for b, n in enumerate(orders):
+        d, e = families.generate("normal", int(n), instance=1 + b)
+        d2, e2 = families.generate("normal", int(n), instance=100001 + b)
+        D[off[b]:off[b + 1]] = d
+        E[off[b]:off[b + 1] - 1] = e
+        D2[off[b]:off[b + 1]] = d2
+        E2[off[b]:off[b + 1] - 1] = e2
+    s = brdc.Solver()
+    stream = torch.cuda.Stream()
+    stream.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(stream):
+        s.set_stream(stream)
+        T = s.dstebr_batched(off, torch.tensor(D2, device="cuda"), torch.tensor(E2, device="cuda"))
+        Dt = torch.tensor(D, device="cuda")
+        Et = torch.tensor(E, device="cuda")
+        D0, E0 = Dt.clone(), Et.clone()
+        W = torch.empty(tot, dtype=torch.float64, device="cuda")
+        G = torch.empty_like(W)
+        gD = torch.empty_like(W)
+        gE = torch.empty_like(W)
+        hist = torch.zeros(steps + 1, dtype=torch.float64, device="cuda")
+        ws = s.batched_workspace(off, checkpoints=True)
+
+        def step(i):
+            s.dstebr_batched(off, Dt, Et, W=W, workspace=ws)
+            torch.sub(W, T, out=G)
+            hist[i].copy_(torch.dot(G, G))
+            G.mul_(2.0)
+            s.dstebr_batched_backward(off, Dt, Et, G, workspace=ws, keep_forward=True, gD=gD, gE=gE)
+            Dt.add_(gD, alpha=-lr)
+            Et.add_(gE, alpha=-lr)
+
+        step(0)  # uploads the forest tables
+        stream.synchronize()
+        t_eager = _event_ms(torch, lambda: step(0), 3, flush, stream)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=stream):
+            for i in range(steps):
+                step(i)
+        Dt.copy_(D0)
+        Et.copy_(E0)
+        stream.synchronize()
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        g.replay()
+        e1.record(stream)
+        e1.synchronize()
+        t_graph = e0.elapsed_time(e1)
+        s.dstebr_batched(off, Dt, Et, W=W, workspace=ws)
+        torch.sub(W, T, out=G)
+        hist[steps].copy_(torch.dot(G, G))
+        stream.synchronize()
+        h = hist.cpu().numpy()
+    del g
+    s.close()
+    return {"count": count, "orders": "log-uniform [64, 4096]", "rows": tot, "steps": steps,
+            "lr": lr, "graph_ms_total": t_graph, "ms_per_step_graph": t_graph / steps,
+            "ms_per_step_eager": t_eager, "loss_first": float(h[0]), "loss_last": float(h[steps]),
+            "loss_at": {str(k): float(h[k]) for k in (1, 10, 50, 100, 199)},
+            "checkpoint_workspace_bytes": ws.numel()}
 
 
 def roofline(diag, phase, n, total_ms=None):

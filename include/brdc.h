@@ -225,6 +225,22 @@ brdc_status brdc_dstebr_batched(brdc_handle handle, int64_t count,
                                 const double *d_E, double *d_W,
                                 void *workspace, size_t workspace_size);
 
+/* Batched adjoint, the batch form of brdc_dstebr_backward: dL/dD and dL/dE
+ * of L = sum G_i W_i over all instances, packed like D and E (the ignored E
+ * slot of each instance gets 0).  The workspace must have the size from
+ * brdc_dstebr_batched_checkpoint_workspace_size; brdc_dstebr_batched run
+ * with such a workspace records the checkpoints (keep_forward = 1 reuses
+ * them), otherwise the forward solve is re-run first.  No reference
+ * counterpart. */
+brdc_status brdc_dstebr_batched_checkpoint_workspace_size(int64_t count,
+                                                          const int64_t *offsets,
+                                                          size_t *bytes);
+brdc_status brdc_dstebr_batched_backward(brdc_handle handle, int64_t count,
+                                         const int64_t *offsets, const double *d_D,
+                                         const double *d_E, const double *d_G,
+                                         double *d_gD, double *d_gE, void *workspace,
+                                         size_t workspace_size, int keep_forward);
+
 /* Library version string. */
 const char *brdc_version(void);
 

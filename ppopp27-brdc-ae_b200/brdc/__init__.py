@@ -63,6 +63,8 @@ EXPORTS = (
     "brdc_set_timing",
     "brdc_get_last_timings",
     "brdc_dstebr_noalloc",
+    "brdc_dstebr_batched_checkpoint_workspace_size",
+    "brdc_dstebr_batched_backward",
 )
 
 
@@ -164,6 +166,10 @@ def load() -> ctypes.CDLL:
     lib.brdc_dstedc_dc_br_.restype = None
     lib.brdc_dstebr_batched_workspace_size.argtypes = [i64, ctypes.POINTER(i64), ctypes.POINTER(sz)]
     lib.brdc_dstebr_batched.argtypes = [vp, i64, ctypes.POINTER(i64), vp, vp, vp, vp, sz]
+    lib.brdc_dstebr_batched_checkpoint_workspace_size.argtypes = [
+        i64, ctypes.POINTER(i64), ctypes.POINTER(sz)]
+    lib.brdc_dstebr_batched_backward.argtypes = [
+        vp, i64, ctypes.POINTER(i64), vp, vp, vp, vp, vp, vp, sz, ctypes.c_int]
     lib.brdc_version.restype = ctypes.c_char_p
     lib.brdc_set_timing.argtypes = [vp, ctypes.c_int]
     lib.brdc_dstebr_noalloc.argtypes = [vp, i64, vp, vp, vp]
@@ -172,7 +178,8 @@ def load() -> ctypes.CDLL:
               "brdc_get_last_error", "brdc_dstebr_workspace_size", "brdc_dstebr",
               "brdc_dstebr_backward", "brdc_get_info", "brdc_get_diagnostics",
               "brdc_dstebr_batched_workspace_size", "brdc_dstebr_batched",
-              "brdc_set_timing", "brdc_get_last_timings", "brdc_dstebr_noalloc"):
+              "brdc_set_timing", "brdc_get_last_timings", "brdc_dstebr_noalloc",
+              "brdc_dstebr_batched_checkpoint_workspace_size", "brdc_dstebr_batched_backward"):
         getattr(lib, f).restype = ctypes.c_int
     _lib = lib
     return lib
@@ -198,15 +205,15 @@ def workspace_size(n: int, flags: int = 0) -> int:
     return int(out.value)
 
 
-def batched_workspace_size(offsets: Sequence[int]) -> int:
+def batched_workspace_size(offsets: Sequence[int], checkpoints: bool = False) -> int:
+    """Bytes of device workspace for one batched solve; with checkpoints,
+    the size that also records what the batched backward reads."""
     off = np.ascontiguousarray(np.asarray(offsets, dtype=np.int64))
     out = ctypes.c_size_t()
-    _check(
-        load().brdc_dstebr_batched_workspace_size(
-            len(off) - 1, off.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), ctypes.byref(out)
-        ),
-        "batched_workspace_size",
-    )
+    fn = (load().brdc_dstebr_batched_checkpoint_workspace_size if checkpoints
+          else load().brdc_dstebr_batched_workspace_size)
+    _check(fn(len(off) - 1, off.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), ctypes.byref(out)),
+           "batched_workspace_size")
     return int(out.value)
 
 
@@ -338,12 +345,12 @@ class Solver:
         return d.as_dict()
 
     # ------------------------------------------------------------ batched
-    def batched_workspace(self, offsets):
+    def batched_workspace(self, offsets, checkpoints: bool = False):
         off = tuple(int(x) for x in offsets)
-        key = ("batched", off)
+        key = ("batched", checkpoints, off)
         ws = self._ws.get(key)
         if ws is None:
-            nbytes = batched_workspace_size(off)
+            nbytes = batched_workspace_size(off, checkpoints)
             ws = self._torch.empty(nbytes, dtype=self._torch.uint8, device="cuda")
             self._ws[key] = ws
         return ws
@@ -364,6 +371,29 @@ class Solver:
         )
         _check(st, "brdc_dstebr_batched", self.h)
         return W
+
+    def dstebr_batched_backward(self, offsets, D, E, G, workspace=None,
+                                keep_forward: bool = False, gD=None, gE=None):
+        """dL/dD, dL/dE of L = sum(G * W) for a packed batch (layout of
+        dstebr_batched).  keep_forward reuses the checkpoints that a
+        dstebr_batched call with the same checkpoint workspace recorded."""
+        torch = self._torch
+        off = np.ascontiguousarray(np.asarray(offsets, dtype=np.int64))
+        total = int(off[-1])
+        if gD is None:
+            gD = torch.empty(total, dtype=torch.float64, device=D.device)
+        if gE is None:
+            gE = torch.empty(total, dtype=torch.float64, device=D.device)
+        ws = self.batched_workspace(off, True) if workspace is None else workspace
+        st = load().brdc_dstebr_batched_backward(
+            self.h, len(off) - 1, off.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+            ctypes.c_void_p(D.data_ptr()), ctypes.c_void_p(E.data_ptr()),
+            ctypes.c_void_p(G.data_ptr()), ctypes.c_void_p(gD.data_ptr()),
+            ctypes.c_void_p(gE.data_ptr()), ctypes.c_void_p(ws.data_ptr()), ws.numel(),
+            1 if keep_forward else 0,
+        )
+        _check(st, "brdc_dstebr_batched_backward", self.h)
+        return gD, gE
 
 
 def dstedc_dc_br(d, e) -> np.ndarray:

@@ -32,6 +32,7 @@ struct brdc_handle_struct {
     int device;
     // batched: signature of the forest whose tables sit in a workspace
     const void *prep_ws;
+    bool prep_ckpt = false;
     std::vector<long long> prep_off;
     // phase timing (off by default)
     int timing;
@@ -656,20 +657,107 @@ extern "C" brdc_status brdc_get_last_timings(brdc_handle h, brdc_timings *out) {
 
 // --------------------------------------------------------------- batched
 
-extern "C" brdc_status brdc_dstebr_batched_workspace_size(int64_t count,
-                                                          const int64_t *offsets,
-                                                          size_t *bytes) {
-    if (bytes == nullptr || offsets == nullptr) {
+namespace {
+
+// Forest descriptor of a batch.  With more than one instance the
+// per-instance tables live in the workspace; they are uploaded once per
+// (workspace, layout, offsets), so later calls with the same triple only
+// enqueue kernels and can be captured in a CUDA graph.
+brdc_status prepare_forest(brdc_handle h, const HostForest &hf, const Ws &w,
+                           const void *workspace, bool ckpt, Forest *F) {
+    *F = Forest{};
+    F->B = hf.B;
+    F->max_levels = hf.max_levels;
+    if (hf.B == 1) {
+        F->n0 = hf.total_n;
+        F->L0 = hf.max_levels;
+        return BRDC_STATUS_SUCCESS;
+    }
+    const bool same = h->prep_ws == workspace && h->prep_ckpt == ckpt &&
+                      h->prep_off.size() == (size_t)hf.B + 1 &&
+                      std::equal(h->prep_off.begin(), h->prep_off.end(), hf.off.begin());
+    if (!same) {
+        std::vector<int> node_prefix((size_t)(hf.B + 1) * std::max(hf.max_levels, 1), 0);
+        for (int k = 0; k < hf.max_levels; ++k) {
+            int *row = node_prefix.data() + (size_t)k * (hf.B + 1);
+            row[0] = 0;
+            for (int b = 0; b < hf.B; ++b) {
+                const int L = hf.lev[b];
+                row[b + 1] = row[b] + (L > k ? (1 << (L - 1 - k)) : 0);
+            }
+        }
+        std::vector<int> leaf_prefix(hf.B + 1, 0);
+        for (int b = 0; b < hf.B; ++b) {
+            leaf_prefix[b + 1] = leaf_prefix[b] + (1 << hf.lev[b]);
+        }
+        BRDC_CUDA(h, "brdc.batched.upload_off",
+                  cudaMemcpyAsync(w.f_off, hf.off.data(), sizeof(long long) * (hf.B + 1),
+                                  cudaMemcpyHostToDevice, h->stream));
+        BRDC_CUDA(h, "brdc.batched.upload_lev",
+                  cudaMemcpyAsync(w.f_lev, hf.lev.data(), sizeof(int) * hf.B,
+                                  cudaMemcpyHostToDevice, h->stream));
+        BRDC_CUDA(h, "brdc.batched.upload_nodes",
+                  cudaMemcpyAsync(w.f_node_prefix, node_prefix.data(),
+                                  sizeof(int) * node_prefix.size(), cudaMemcpyHostToDevice,
+                                  h->stream));
+        BRDC_CUDA(h, "brdc.batched.upload_leaves",
+                  cudaMemcpyAsync(w.f_leaf_prefix, leaf_prefix.data(),
+                                  sizeof(int) * leaf_prefix.size(), cudaMemcpyHostToDevice,
+                                  h->stream));
+        BRDC_CUDA(h, "brdc.batched.upload_sync", cudaStreamSynchronize(h->stream));
+        h->prep_ws = workspace;
+        h->prep_ckpt = ckpt;
+        h->prep_off = hf.off;
+    }
+    F->off = w.f_off;
+    F->lev = w.f_lev;
+    F->node_prefix = w.f_node_prefix;
+    F->leaf_prefix = w.f_leaf_prefix;
+    return BRDC_STATUS_SUCCESS;
+}
+
+brdc_status batch_forest(int64_t count, const int64_t *offsets, HostForest *hf) {
+    if (offsets == nullptr) {
         return BRDC_STATUS_INVALID_POINTER;
     }
     if (count <= 0 || count > (1LL << 28) || offsets[0] != 0) {
         return BRDC_STATUS_INVALID_VALUE;
     }
-    HostForest f;
-    if (!build_forest((int)count, reinterpret_cast<const long long *>(offsets), &f)) {
+    if (!build_forest((int)count, reinterpret_cast<const long long *>(offsets), hf)) {
         return BRDC_STATUS_INVALID_VALUE;
     }
+    return BRDC_STATUS_SUCCESS;
+}
+
+} // namespace
+
+extern "C" brdc_status brdc_dstebr_batched_workspace_size(int64_t count,
+                                                          const int64_t *offsets,
+                                                          size_t *bytes) {
+    if (bytes == nullptr) {
+        return BRDC_STATUS_INVALID_POINTER;
+    }
+    HostForest f;
+    const brdc_status st = batch_forest(count, offsets, &f);
+    if (st != BRDC_STATUS_SUCCESS) {
+        return st;
+    }
     *bytes = make_layout(f).bytes;
+    return BRDC_STATUS_SUCCESS;
+}
+
+extern "C" brdc_status brdc_dstebr_batched_checkpoint_workspace_size(int64_t count,
+                                                                     const int64_t *offsets,
+                                                                     size_t *bytes) {
+    if (bytes == nullptr) {
+        return BRDC_STATUS_INVALID_POINTER;
+    }
+    HostForest f;
+    const brdc_status st = batch_forest(count, offsets, &f);
+    if (st != BRDC_STATUS_SUCCESS) {
+        return st;
+    }
+    *bytes = make_layout(f, true).bytes;
     return BRDC_STATUS_SUCCESS;
 }
 
@@ -681,72 +769,26 @@ extern "C" brdc_status brdc_dstebr_batched(brdc_handle h, int64_t count,
     if (h == nullptr) {
         return BRDC_STATUS_INVALID_HANDLE;
     }
-    if (offsets == nullptr || d_D == nullptr || d_W == nullptr || d_E == nullptr) {
+    if (d_D == nullptr || d_W == nullptr || d_E == nullptr) {
         return BRDC_STATUS_INVALID_POINTER;
     }
-    if (count <= 0 || count > (1LL << 28) || offsets[0] != 0) {
-        return BRDC_STATUS_INVALID_VALUE;
-    }
     HostForest hf;
-    if (!build_forest((int)count, reinterpret_cast<const long long *>(offsets), &hf)) {
-        return BRDC_STATUS_INVALID_VALUE;
+    brdc_status st = batch_forest(count, offsets, &hf);
+    if (st != BRDC_STATUS_SUCCESS) {
+        return st;
     }
-    const Layout L = make_layout(hf);
+    // a workspace of the checkpoint size records what the backward reads
+    const Layout Lc = make_layout(hf, true);
+    const bool ckpt = workspace != nullptr && workspace_size >= Lc.bytes;
+    const Layout L = ckpt ? Lc : make_layout(hf, false);
     if (workspace == nullptr || workspace_size < L.bytes) {
         return BRDC_STATUS_INVALID_WORKSPACE;
     }
-    const Ws w = carve(workspace, hf, false);
-    Forest F{};
-    F.B = hf.B;
-    F.max_levels = hf.max_levels;
-    if (hf.B == 1) {
-        F.n0 = hf.total_n;
-        F.L0 = hf.max_levels;
-    } else {
-        // Tables are uploaded once per (workspace, offsets); later calls with
-        // the same pair enqueue kernels only and can be graph-captured.
-        const bool same = h->prep_ws == workspace &&
-                          h->prep_off.size() == (size_t)hf.B + 1 &&
-                          std::equal(h->prep_off.begin(), h->prep_off.end(),
-                                     hf.off.begin());
-        if (!same) {
-            std::vector<int> node_prefix((size_t)(hf.B + 1) *
-                                         std::max(hf.max_levels, 1), 0);
-            for (int k = 0; k < hf.max_levels; ++k) {
-                int *row = node_prefix.data() + (size_t)k * (hf.B + 1);
-                row[0] = 0;
-                for (int b = 0; b < hf.B; ++b) {
-                    const int L = hf.lev[b];
-                    row[b + 1] = row[b] + (L > k ? (1 << (L - 1 - k)) : 0);
-                }
-            }
-            std::vector<int> leaf_prefix(hf.B + 1, 0);
-            for (int b = 0; b < hf.B; ++b) {
-                leaf_prefix[b + 1] = leaf_prefix[b] + (1 << hf.lev[b]);
-            }
-            BRDC_CUDA(h, "brdc.batched.upload_off",
-                      cudaMemcpyAsync(w.f_off, hf.off.data(),
-                                      sizeof(long long) * (hf.B + 1),
-                                      cudaMemcpyHostToDevice, h->stream));
-            BRDC_CUDA(h, "brdc.batched.upload_lev",
-                      cudaMemcpyAsync(w.f_lev, hf.lev.data(), sizeof(int) * hf.B,
-                                      cudaMemcpyHostToDevice, h->stream));
-            BRDC_CUDA(h, "brdc.batched.upload_nodes",
-                      cudaMemcpyAsync(w.f_node_prefix, node_prefix.data(),
-                                      sizeof(int) * node_prefix.size(),
-                                      cudaMemcpyHostToDevice, h->stream));
-            BRDC_CUDA(h, "brdc.batched.upload_leaves",
-                      cudaMemcpyAsync(w.f_leaf_prefix, leaf_prefix.data(),
-                                      sizeof(int) * leaf_prefix.size(),
-                                      cudaMemcpyHostToDevice, h->stream));
-            BRDC_CUDA(h, "brdc.batched.upload_sync", cudaStreamSynchronize(h->stream));
-            h->prep_ws = workspace;
-            h->prep_off = hf.off;
-        }
-        F.off = w.f_off;
-        F.lev = w.f_lev;
-        F.node_prefix = w.f_node_prefix;
-        F.leaf_prefix = w.f_leaf_prefix;
+    const Ws w = carve(workspace, hf, ckpt);
+    Forest F;
+    st = prepare_forest(h, hf, w, workspace, ckpt, &F);
+    if (st != BRDC_STATUS_SUCCESS) {
+        return st;
     }
     return run_forest(h, hf, L, F, w, d_D, d_E, d_W);
 }
@@ -782,8 +824,11 @@ brdc_status run_backward(brdc_handle h, const HostForest &hf, const Layout &L,
     const long long nt = hf.total_n;
     long long eg = (nt + 255) / 256;
     eg = std::max<long long>(1, std::min<long long>(eg, (long long)h->sm_count * 8));
-    if (nt > 1) {
-        k_bw_zero<<<(unsigned)eg, 256, 0, s>>>(gE, nt - 1);
+    // E holds n-1 entries for one instance, one per row (the last of each
+    // instance unused and returned as 0) for a batch
+    const long long ne = hf.B > 1 ? nt : nt - 1;
+    if (ne > 0) {
+        k_bw_zero<<<(unsigned)eg, 256, 0, s>>>(gE, ne);
         BRDC_CUDA(h, "brdc.bw.zero_ge", cudaGetLastError());
     }
     double *par[3] = {w.bnd, w.bnf, w.bnl};
@@ -881,6 +926,44 @@ extern "C" brdc_status brdc_dstebr_backward(brdc_handle h, int64_t n,
     F.L0 = hf.max_levels;
     if (!keep_forward) {
         const brdc_status st = run_forest(h, hf, L, F, w, d_D, d_E, w.wtmp);
+        if (st != BRDC_STATUS_SUCCESS) {
+            return st;
+        }
+    }
+    return run_backward(h, hf, L, F, w, d_D, d_E, d_G, d_gD, d_gE);
+}
+
+extern "C" brdc_status brdc_dstebr_batched_backward(brdc_handle h, int64_t count,
+                                                    const int64_t *offsets,
+                                                    const double *d_D, const double *d_E,
+                                                    const double *d_G, double *d_gD,
+                                                    double *d_gE, void *workspace,
+                                                    size_t workspace_size,
+                                                    int keep_forward) {
+    if (h == nullptr) {
+        return BRDC_STATUS_INVALID_HANDLE;
+    }
+    if (d_D == nullptr || d_E == nullptr || d_G == nullptr || d_gD == nullptr ||
+        d_gE == nullptr) {
+        return BRDC_STATUS_INVALID_POINTER;
+    }
+    HostForest hf;
+    brdc_status st = batch_forest(count, offsets, &hf);
+    if (st != BRDC_STATUS_SUCCESS) {
+        return st;
+    }
+    const Layout L = make_layout(hf, true);
+    if (workspace == nullptr || workspace_size < L.bytes) {
+        return BRDC_STATUS_INVALID_WORKSPACE;
+    }
+    const Ws w = carve(workspace, hf, true);
+    Forest F;
+    st = prepare_forest(h, hf, w, workspace, true, &F);
+    if (st != BRDC_STATUS_SUCCESS) {
+        return st;
+    }
+    if (!keep_forward) {
+        st = run_forest(h, hf, L, F, w, d_D, d_E, w.wtmp);
         if (st != BRDC_STATUS_SUCCESS) {
             return st;
         }

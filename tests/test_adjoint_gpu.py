@@ -171,3 +171,88 @@ def test_keep_forward_matches_rerun(solver):
     a1, b1 = solver.dstebr_backward(D, E, G, workspace=ws, keep_forward=True)
     a2, b2 = solver.dstebr_backward(D, E, G, workspace=ws, keep_forward=False)
     assert torch.equal(a1, a2) and torch.equal(b1, b2)
+
+
+def test_central_differences_normal_n512(solver):
+    """Central differences with h = 1e-6 ||T|| on the normal family at
+    N = 512.  Where the spectrum has a gap near h (this instance's smallest
+    is 4e-6) the difference quotient itself is off by O(1); each entry is
+    therefore checked against its own truncation estimate, the Richardson
+    difference |FD(2h) - FD(h)| (the O(h^2) error of FD(h) is a third of
+    it), besides a floor of 1e-6 of the gradient's scale."""
+    import torch
+
+    n = 512
+    d, e = families.generate("normal", n)
+    rng = np.random.Generator(np.random.PCG64([2, n, 1]))
+    g = rng.standard_normal(n)
+    gd, ge = grads(solver, d, e, g)
+    h = 1e-6 * float(np.max(np.abs(scipy.linalg.eigvalsh_tridiagonal(d, e))))
+    Gt = torch.tensor(g, device="cuda")
+
+    def loss(dd, ee):
+        W = solver.dstebr(torch.tensor(dd, device="cuda"), torch.tensor(ee, device="cuda"))
+        return float((W * Gt).sum())
+
+    def fd_pair(base, j, other, first):
+        v = {}
+        for k in (2, 1, -1, -2):
+            p = base.copy()
+            p[j] += k * h
+            v[k] = loss(p, other) if first else loss(other, p)
+        return (v[1] - v[-1]) / (2 * h), (v[2] - v[-2]) / (4 * h)
+
+    sc = max(np.max(np.abs(gd)), np.max(np.abs(ge)))
+    resolved = 0
+    for ours, base, other, first in ((gd, d, e, True), (ge, e, d, False)):
+        for j in range(base.shape[0]):
+            f1, f2 = fd_pair(base, j, other, first)
+            bound = 1e-6 * sc + 2.0 * abs(f2 - f1)
+            assert abs(ours[j] - f1) < bound, (first, j, ours[j], f1, f2)
+            resolved += abs(f2 - f1) < 1e-6 * sc
+    # the estimate only widens the bar where FD cannot resolve the gradient
+    assert resolved > 0.95 * (2 * n - 1)
+
+
+def test_batched_backward_matches_single(solver):
+    """The batched adjoint equals the single-instance adjoint of every
+    instance (to the parity tolerance: lanes per root follow the batch's K
+    statistics) and the LAPACK eigenvector gradient."""
+    import torch
+
+    off, D, E, orders, fams = families.batch(24, 17, 1500, seed=5)
+    rng = np.random.default_rng(11)
+    G = rng.standard_normal(off[-1])
+    Dt, Et, Gt = (torch.tensor(x, device="cuda") for x in (D, E, G))
+    gD, gE = solver.dstebr_batched_backward(off, Dt, Et, Gt)
+    gD, gE = gD.cpu().numpy(), gE.cpu().numpy()
+    for b in range(len(orders)):
+        lo, hi = int(off[b]), int(off[b + 1])
+        d, e, g = D[lo:hi], E[lo:hi - 1], G[lo:hi]
+        sd, se = grads(solver, d, e, g)
+        rd, re = eig_ref_grads(d, e, g)
+        sc = max(np.max(np.abs(rd)), np.max(np.abs(re)), 1e-300)
+        # clustered spectra (gaps ~1e-13) amplify rounding differences and
+        # defeat double-precision eigenvectors; see the multiprecision test
+        tol = 1e-6 if fams[b] == "clustered" else 1e-11
+        assert np.max(np.abs(gD[lo:hi] - sd)) < tol * sc, b
+        assert np.max(np.abs(gE[lo:hi - 1] - se)) < tol * sc, b
+        if fams[b] != "clustered":
+            assert np.max(np.abs(gD[lo:hi] - rd)) < 1e-9 * sc, b
+            assert np.max(np.abs(gE[lo:hi - 1] - re)) < 1e-9 * sc, b
+        assert gE[hi - 1] == 0.0
+
+
+def test_batched_backward_keep_forward(solver):
+    import torch
+
+    off, D, E, orders, _ = families.batch(16, 40, 900, seed=6)
+    G = np.random.default_rng(12).standard_normal(off[-1])
+    Dt, Et, Gt = (torch.tensor(x, device="cuda") for x in (D, E, G))
+    ws = solver.batched_workspace(off, checkpoints=True)
+    W = solver.dstebr_batched(off, Dt, Et, workspace=ws)
+    a1, b1 = solver.dstebr_batched_backward(off, Dt, Et, Gt, workspace=ws, keep_forward=True)
+    a2, b2 = solver.dstebr_batched_backward(off, Dt, Et, Gt, workspace=ws, keep_forward=False)
+    assert torch.equal(a1, a2) and torch.equal(b1, b2)
+    W2 = solver.dstebr_batched(off, Dt, Et)
+    assert torch.equal(W, W2)
