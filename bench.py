@@ -174,6 +174,31 @@ def run_reference_arm(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_profile_case(spec):
+    """One or more plain solves of a seeded instance, nothing else on the
+    GPU: solve i launches k_init, k_leaf, then per level k_merge,
+    k_merge_deflate, k_secular, k_lowner and k_rows (below the top level)
+    and k_place, so a kernel's launch index is known in advance."""
+    import torch
+
+    import brdc
+    from brdc import families
+
+    parts = spec.split(":")
+    fam, n = parts[0], int(parts[1])
+    solves = int(parts[2]) if len(parts) > 2 else 1
+    d, e = families.generate(fam, n)
+    solver = brdc.Solver()
+    D = torch.tensor(d, device="cuda")
+    E = torch.tensor(e, device="cuda")
+    W = torch.empty(n, dtype=torch.float64, device="cuda")
+    ws = solver.workspace(n)
+    for _ in range(solves):
+        solver.dstebr(D, E, W=W, workspace=ws)
+    torch.cuda.synchronize()
+    solver.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -182,7 +207,13 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=12.0)
+    ap.add_argument("--profile-case", default=None,
+                    help="family:n[:solves] -- run that many plain solves (default 1) of the "
+                         "seeded instance and exit; a fixed launch sequence for profilers")
     args = ap.parse_args()
+    if args.profile_case:
+        run_profile_case(args.profile_case)
+        return
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
     rank = int(os.environ.get("RANK", "0"))
