@@ -52,7 +52,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
         subprocess.run(cmd, check=True)
-    pdeps = [os.path.join(CSRC, "probe_fp64.cu")]
+    pdeps = [os.path.join(CSRC, "probe_fp64.cu"), os.path.join(CSRC, "brdc_secular.cuh")]
     if force or _stale(PROBELIB, pdeps):
         subprocess.run([_nvcc(), *NVCC_FLAGS, "-o", PROBELIB, pdeps[0]], check=True)
     hdeps = [os.path.join(CSRC, "host_check.cpp"), os.path.join(CSRC, "brdc_secular.cuh")]

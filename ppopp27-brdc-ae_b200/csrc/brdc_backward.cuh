@@ -187,7 +187,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_bw_roots(BArgs a) {
                 if (i == o) {
                     continue;
                 }
-                const double r = 1.0 / ((__ldg(pd + i) - dorg) - tau);
+                const double r = brdc_rcp((__ldg(pd + i) - dorg) - tau);
                 const double u = __ldg(zz + i) * r;
                 S2x += u * u;
                 S3x += u * u * r;
@@ -284,7 +284,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_bw_poles(BArgs a) {
                     if (j == sk0 || j == sk1) {
                         continue;
                     }
-                    const double r = 1.0 / ((di - __ldg(rdo + j)) - __ldg(rtau + j));
+                    const double r = brdc_rcp((di - __ldg(rdo + j)) - __ldg(rtau + j));
                     const double in = __ldg(rin + j);
                     const double u = zi * r * in;
                     const double kj = __ldg(rk + j);
@@ -299,7 +299,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_bw_poles(BArgs a) {
                     if (j == sk0 || j == sk1) {
                         continue;
                     }
-                    const double r = 1.0 / ((di - __ldg(rdo + j)) - __ldg(rtau + j));
+                    const double r = brdc_rcp((di - __ldg(rdo + j)) - __ldg(rtau + j));
                     const double in = __ldg(rin + j);
                     const double u = zi * r * in;
                     const double kj = __ldg(rk + j);
@@ -397,7 +397,7 @@ __global__ void __launch_bounds__(256) k_bw_defl(BArgs a, long long total_n) {
         }
         double acc = 0.0;
         for (int j = lane; j < K; j += 32) {
-            const double r = 1.0 / ((di - __ldg(w.rdo + po + j)) - __ldg(w.rtau + po + j));
+            const double r = brdc_rcp((di - __ldg(w.rdo + po + j)) - __ldg(w.rtau + po + j));
             const double t = __ldg(w.bfr + po + j) * fi + __ldg(w.blr + po + j) * li -
                              gfi * __ldg(w.rfp + po + j) - gli * __ldg(w.rlp + po + j);
             acc += __ldg(w.rinvn + po + j) * r * (small ? t : -t * r);

@@ -1027,19 +1027,30 @@ __global__ void __launch_bounds__(kSweepThreads)
             const long long po = G.poff;
             const int i = (item - w.pref_w[g]) * Rw + grp;
             const bool active = i < K;
-            double prod = 1.0;
+            // two interleaved products halve the serial multiply chain
+            double prod = 1.0, prod2 = 1.0;
             if (active) {
                 const double di = w.pd[po + i];
                 const double *rdo = w.rdo + po;
                 const double *rtau = w.rtau + po;
                 const double *pd = w.pd + po;
-#pragma unroll 4
-                for (int j = l; j < K; j += tpr) {
+                int j = l;
+#pragma unroll 2
+                for (; j + tpr < K; j += 2 * tpr) {
+                    const int j2 = j + tpr;
                     const double dl = (di - __ldg(rdo + j)) - __ldg(rtau + j);
-                    prod *= (j == i) ? dl : dl / (di - __ldg(pd + j));
+                    const double dl2 = (di - __ldg(rdo + j2)) - __ldg(rtau + j2);
+                    const double q = brdc_rcp(j == i ? 1.0 : di - __ldg(pd + j));
+                    const double q2 = brdc_rcp(j2 == i ? 1.0 : di - __ldg(pd + j2));
+                    prod *= dl * q;
+                    prod2 *= dl2 * q2;
+                }
+                if (j < K) {
+                    const double dl = (di - __ldg(rdo + j)) - __ldg(rtau + j);
+                    prod *= dl * brdc_rcp(j == i ? 1.0 : di - __ldg(pd + j));
                 }
             }
-            prod = group_prod(prod, tpr);
+            prod = group_prod(prod * prod2, tpr);
             if (active && l == 0) {
                 w.pw[po + i] = lowner_value(w, po, i, prod, w.nrho[g]);
             }
@@ -1064,7 +1075,7 @@ __global__ void __launch_bounds__(kSweepThreads)
         const int i = (item - w.pref_c[g]) * R + grp;
         const bool active = i < K;
         const double di = active ? w.pd[po + i] : 0.0;
-        double prod = 1.0;
+        double prod = 1.0, prod2 = 1.0;
         TileSet<3> ts;
         const double *srcs[3] = {w.rdo, w.rtau, w.pd};
         tiles_setup<3>(ts, smem, bars, srcs, po, K);
@@ -1072,10 +1083,19 @@ __global__ void __launch_bounds__(kSweepThreads)
         ts.phase[1] = ph[1];
         const bool ok = tiles_sweep<3>(ts, [&](int j0, int cnt, double *const *b) {
             if (active) {
-                for (int jj = lane; jj < cnt; jj += tpr) {
-                    const int j = j0 + jj;
+                int jj = lane;
+                for (; jj + tpr < cnt; jj += 2 * tpr) {
+                    const int j = j0 + jj, jj2 = jj + tpr;
                     const double dl = (di - b[0][jj]) - b[1][jj];
-                    prod *= (j == i) ? dl : dl / (di - b[2][jj]);
+                    const double dl2 = (di - b[0][jj2]) - b[1][jj2];
+                    const double q = brdc_rcp(j == i ? 1.0 : di - b[2][jj]);
+                    const double q2 = brdc_rcp(j + tpr == i ? 1.0 : di - b[2][jj2]);
+                    prod *= dl * q;
+                    prod2 *= dl2 * q2;
+                }
+                if (jj < cnt) {
+                    const double dl = (di - b[0][jj]) - b[1][jj];
+                    prod *= dl * brdc_rcp(j0 + jj == i ? 1.0 : di - b[2][jj]);
                 }
             }
         });
@@ -1085,7 +1105,7 @@ __global__ void __launch_bounds__(kSweepThreads)
             record_error(w.hdr, kErrBarrierTimeout);
             return;
         }
-        prod = group_prod(prod, tpr);
+        prod = group_prod(prod * prod2, tpr);
         if (active && lane == 0) {
             w.pw[po + i] = lowner_value(w, po, i, prod, w.nrho[g]);
         }
@@ -1134,7 +1154,7 @@ __global__ void __launch_bounds__(kSweepThreads)
 #pragma unroll 4
                 for (int i = l; i < K; i += tpr) {
                     const double dl = (__ldg(pd + i) - dorg) - tau;
-                    const double u = (dl != 0.0) ? __ldg(pw + i) / dl : 0.0;
+                    const double u = (dl != 0.0) ? __ldg(pw + i) * brdc_rcp(dl) : 0.0;
                     s2 += u * u;
                     a1 += __ldg(pf + i) * u;
                     a2 += __ldg(pl + i) * u;
@@ -1180,7 +1200,7 @@ __global__ void __launch_bounds__(kSweepThreads)
             if (root) {
                 for (int jj = lane; jj < cnt; jj += tpr) {
                     const double dl = (b[0][jj] - dorg) - tau;
-                    const double u = (dl != 0.0) ? b[1][jj] / dl : 0.0;
+                    const double u = (dl != 0.0) ? b[1][jj] * brdc_rcp(dl) : 0.0;
                     s2 += u * u;
                     a1 += b[2][jj] * u;
                     a2 += b[3][jj] * u;

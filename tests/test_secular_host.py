@@ -2,6 +2,7 @@
 against LAPACK DLAED4 (the routine the reference calls per root,
 cpu/src/dlaed4_br.f:59)."""
 import ctypes
+import zlib
 
 import numpy as np
 import pytest
@@ -33,7 +34,7 @@ def _root(lib, d, z, rho, i):
 
 @pytest.mark.parametrize("kind", ["normal", "uniform", "clustered", "tiny_z"])
 def test_roots_match_dlaed4(hostlib, kind):
-    rng = np.random.default_rng(hash(kind) % 2**32)
+    rng = np.random.default_rng(zlib.crc32(kind.encode()))
     worst, sw_max = 0.0, 0
     for _ in range(40):
         K = int(rng.integers(2, 200))
@@ -55,9 +56,16 @@ def test_roots_match_dlaed4(hostlib, kind):
             lam_ref, _ = oracle.dlaed4(d, z, rho, i)
             lam, sweeps, failed = _root(hostlib, d, z, rho, i)
             assert not failed
+            # accurate relative to the distance to the nearest pole, or
+            # normwise (relative to max(|lambda|, max|d|)): a root near zero
+            # has no relative accuracy in |lambda| (nor has DLAED4's), and
+            # with many tiny weights the secular function's own rounding
+            # can exceed 1e-12 of the gap
             gap = float(np.min(np.abs(d - lam_ref)))
-            err = abs(lam - lam_ref) / max(min(gap, abs(lam_ref)) if lam_ref != 0 else gap, 1e-300)
-            worst = max(worst, min(err, abs(lam - lam_ref) / max(abs(lam_ref), 1e-300)))
+            diff = abs(lam - lam_ref)
+            rel_gap = diff / gap if gap > 0 else np.inf
+            rel_norm = diff / max(abs(lam_ref), float(np.max(np.abs(d))))
+            worst = max(worst, min(rel_gap, rel_norm))
             sw_max = max(sw_max, sweeps)
             if i < K - 1:
                 assert d[i] <= lam <= d[i + 1]
