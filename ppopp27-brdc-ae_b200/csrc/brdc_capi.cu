@@ -268,12 +268,17 @@ void launch_md(const KArgs &a, int grid, cudaStream_t s) {
     k_merge_deflate<T><<<grid, T, 0, s>>>(a);
 }
 
-void launch_merge_deflate(const KArgs &a, int mmax, cudaStream_t s) {
+// Returns the number of kernels launched.
+int launch_merge_deflate(const KArgs &a0, int mmax, cudaStream_t s) {
     // about 4 rows per thread, 32..1024 threads
     int t = 32;
     while (t < 1024 && t * 4 < mmax) {
         t <<= 1;
     }
+    // the level plan walks every node; the last deflation CTA does it while
+    // that is at most one node per thread, a 1024-thread k_plan otherwise
+    KArgs a = a0;
+    a.plan_inline = a.nodes <= t ? 1 : 0;
     switch (t) {
     case 32: launch_md<32>(a, a.nodes, s); break;
     case 64: launch_md<64>(a, a.nodes, s); break;
@@ -282,6 +287,11 @@ void launch_merge_deflate(const KArgs &a, int mmax, cudaStream_t s) {
     case 512: launch_md<512>(a, a.nodes, s); break;
     default: launch_md<1024>(a, a.nodes, s); break;
     }
+    if (!a.plan_inline) {
+        k_plan<1024><<<1, 1024, 0, s>>>(a);
+        return 2;
+    }
+    return 1;
 }
 
 constexpr size_t smem_tiles(int na) { return sizeof(double) * 2 * na * kTile; }
@@ -360,9 +370,8 @@ brdc_status run_forest(brdc_handle h, const HostForest &hf, const Layout &L,
         const int grid = cta_blocks + warp_blocks;
         k_merge<<<(unsigned)elem_grid, 256, 0, s>>>(a, hf.total_n);
         BRDC_CUDA(h, "brdc.merge", cudaGetLastError());
-        launch_merge_deflate(a, hf.level_mmax[k], s);
+        h->launches += 1 + launch_merge_deflate(a, hf.level_mmax[k], s);
         BRDC_CUDA(h, "brdc.merge_deflate", cudaGetLastError());
-        h->launches += 2;
         mark(h, 3 + 4 * k);
         k_secular<<<grid, kSweepThreads, cta_blocks ? smem_tiles(2) : 0, s>>>(a, cta_blocks);
         BRDC_CUDA(h, "brdc.secular", cudaGetLastError());

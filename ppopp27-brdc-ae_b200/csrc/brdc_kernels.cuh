@@ -36,6 +36,7 @@ struct KArgs {
     int k;              // forest level
     int nodes;          // merges at this level
     long long level_rows; // rows of the instances that merge at this level
+    int plan_inline;    // the last deflation CTA writes the level plan (else k_plan)
 };
 
 // ------------------------------------------------------------------ leaves
@@ -310,6 +311,130 @@ __global__ void __launch_bounds__(256) k_merge(KArgs a, long long total_n) {
     }
 }
 
+// Work plan of the sweep kernels for level a.k, from the node scalars the
+// deflation wrote: the level diagnostics, lanes per root, and the item
+// tables.  Merges with K <= kWarpMaxK are served one warp per work item;
+// larger ones by whole CTAs that stage pole tiles in shared memory.  Run by
+// the last deflation CTA of the level, or by k_plan where the level has
+// many nodes and that CTA would be narrow.
+template <int T>
+__device__ void level_plan(const KArgs &a, double *red, int *iscan) {
+    const Ws &w = a.w;
+    double tkw = 0.0, tkc = 0.0, cw = 0.0, cc = 0.0;
+    double skz = 0.0, sk2 = 0.0, kmax = 0.0;
+    for (int i = threadIdx.x; i < a.nodes; i += T) {
+        const int kk = __ldcg(w.nK + i);
+        const int kz = __ldcg(w.nKz + i);
+        if (kk > kWarpMaxK) {
+            tkc += kk;
+            cc += 1.0;
+        } else if (kk > 0) {
+            tkw += kk;
+            cw += 1.0;
+        }
+        skz += kz;
+        sk2 += (double)kk * (double)kk;
+        kmax = fmax(kmax, (double)kk);
+    }
+    tkw = block_sum<T>(tkw, red);
+    tkc = block_sum<T>(tkc, red);
+    cw = block_sum<T>(cw, red);
+    cc = block_sum<T>(cc, red);
+    skz = block_sum<T>(skz, red);
+    sk2 = block_sum<T>(sk2, red);
+    kmax = block_max<T>(kmax, red);
+    if (threadIdx.x == 0) {
+        // level counters of the reference's diagnostics
+        // (gpu/src/tridiag_solver.cu:1166-1260), gathered once per level
+        brdc_level_diagnostics *dg = &w.hdr->diag[a.k];
+        dg->merge_count = a.nodes;
+        dg->size_sum = (int)(a.level_rows);
+        dg->dd_before_sum = (int)skz;
+        dg->dd_after_sum = (int)(tkw + tkc);
+        dg->dd_after_max = (int)kmax;
+        dg->dd_after_sq_sum = (long long)sk2;
+    }
+    // warp role: each root's sweeps form a serial latency chain, so spread
+    // the roots over enough lanes to keep every scheduler busy (~75k
+    // threads); with one root per warp the warp also never diverges.
+    int tpr_w = 1;
+    while (tpr_w < 32 && (double)tpr_w * tkw < 75776.0) {
+        tpr_w <<= 1;
+    }
+    // CTA role: enough lanes to fill the GPU (~75k threads), at least ~16
+    // poles per lane and sweep
+    const double kavg_c = tkc / fmax(cc, 1.0);
+    int tpr_c = 1;
+    while (tpr_c < 32 && (double)tpr_c * tkc < 75776.0) {
+        tpr_c <<= 1;
+    }
+    int cap = 1;
+    while (cap < 32 && (double)(cap * 2) * 16.0 <= kavg_c) {
+        cap <<= 1;
+    }
+    tpr_c = tpr_c < cap ? tpr_c : cap;
+    const int Rw = 32 / tpr_w;
+    const int Rc = kSweepThreads / tpr_c;
+    // each thread owns a contiguous run of nodes: serial prefix of its run,
+    // one block scan across threads, then the run's prefixes
+    const int per = (a.nodes + T - 1) / T;
+    const int i0 = threadIdx.x * per;
+    const int i1 = (i0 + per < a.nodes) ? i0 + per : a.nodes;
+    int sw = 0, sc = 0;
+    for (int i = i0; i < i1; ++i) {
+        const int kk = __ldcg(w.nK + i);
+        if (kk > kWarpMaxK) {
+            sc += (kk + Rc - 1) / Rc;
+        } else {
+            sw += (kk + Rw - 1) / Rw;
+        }
+    }
+    int carry_w, carry_c;
+    int rw = block_exscan<T>(sw, iscan, &carry_w);
+    int rc = block_exscan<T>(sc, iscan, &carry_c);
+    for (int i = i0; i < i1; ++i) {
+        const int kk = __ldcg(w.nK + i);
+        w.pref_w[i] = rw;
+        w.pref_c[i] = rc;
+        if (kk > kWarpMaxK) {
+            rc += (kk + Rc - 1) / Rc;
+        } else {
+            rw += (kk + Rw - 1) / Rw;
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < a.nodes; i += T) {
+        const int s0 = w.pref_w[i];
+        const int s1 = (i + 1 < a.nodes) ? w.pref_w[i + 1] : carry_w;
+        for (int q = s0; q < s1; ++q) {
+            w.items_w[q] = i;
+        }
+        const int c0 = w.pref_c[i];
+        const int c1 = (i + 1 < a.nodes) ? w.pref_c[i + 1] : carry_c;
+        for (int q = c0; q < c1; ++q) {
+            w.items_c[q] = i;
+        }
+    }
+    if (threadIdx.x == 0) {
+        w.pref_w[a.nodes] = carry_w;
+        w.pref_c[a.nodes] = carry_c;
+        LevelCtl *c = &w.hdr->lvl[a.k];
+        c->tpr_w = tpr_w;
+        c->tpr_c = tpr_c;
+        c->items_w = carry_w;
+        c->items_c = carry_c;
+        c->total_k = (int)(tkw + tkc);
+        w.hdr->diag[a.k].threads_per_root = carry_c > 0 ? tpr_c : tpr_w;
+    }
+}
+
+template <int T>
+__global__ void __launch_bounds__(T) k_plan(KArgs a) {
+    __shared__ double red[32];
+    __shared__ int iscan[32];
+    level_plan<T>(a, red, iscan);
+}
+
 template <int T>
 __global__ void __launch_bounds__(T) k_merge_deflate(KArgs a) {
     constexpr int EPT = 4; // rows per thread per chunk
@@ -502,6 +627,11 @@ __global__ void __launch_bounds__(T) k_merge_deflate(KArgs a) {
         w.nrho[g] = rho;
         w.ntol[g] = tol;
         w.nzn[g] = zn;
+    }
+    if (!a.plan_inline) {
+        return;
+    }
+    if (threadIdx.x == 0) {
         __threadfence();
         const int t = atomicAdd(&w.hdr->lvl[a.k].ticket, 1);
         s_last = (t == (int)gridDim.x - 1);
@@ -510,116 +640,8 @@ __global__ void __launch_bounds__(T) k_merge_deflate(KArgs a) {
     if (!s_last) {
         return;
     }
-    // Last CTA of the level: work plan of the sweep kernels.  Merges with
-    // K <= kWarpMaxK are served one warp per work item; larger ones by whole
-    // CTAs that stage pole tiles in shared memory.
     __threadfence();
-    double tkw = 0.0, tkc = 0.0, cw = 0.0, cc = 0.0;
-    double skz = 0.0, sk2 = 0.0, kmax = 0.0;
-    for (int i = threadIdx.x; i < a.nodes; i += T) {
-        const int kk = __ldcg(w.nK + i);
-        const int kz = __ldcg(w.nKz + i);
-        if (kk > kWarpMaxK) {
-            tkc += kk;
-            cc += 1.0;
-        } else if (kk > 0) {
-            tkw += kk;
-            cw += 1.0;
-        }
-        skz += kz;
-        sk2 += (double)kk * (double)kk;
-        kmax = fmax(kmax, (double)kk);
-    }
-    tkw = block_sum<T>(tkw, red);
-    tkc = block_sum<T>(tkc, red);
-    cw = block_sum<T>(cw, red);
-    cc = block_sum<T>(cc, red);
-    skz = block_sum<T>(skz, red);
-    sk2 = block_sum<T>(sk2, red);
-    kmax = block_max<T>(kmax, red);
-    if (threadIdx.x == 0) {
-        // level counters of the reference's diagnostics
-        // (gpu/src/tridiag_solver.cu:1166-1260), gathered once per level
-        brdc_level_diagnostics *dg = &w.hdr->diag[a.k];
-        dg->merge_count = a.nodes;
-        dg->size_sum = (int)(a.level_rows);
-        dg->dd_before_sum = (int)skz;
-        dg->dd_after_sum = (int)(tkw + tkc);
-        dg->dd_after_max = (int)kmax;
-        dg->dd_after_sq_sum = (long long)sk2;
-    }
-    // warp role: each root's sweeps form a serial latency chain, so spread
-    // the roots over enough lanes to keep every scheduler busy (~75k
-    // threads); with one root per warp the warp also never diverges.
-    int tpr_w = 1;
-    while (tpr_w < 32 && (double)tpr_w * tkw < 75776.0) {
-        tpr_w <<= 1;
-    }
-    // CTA role: enough lanes to fill the GPU (~75k threads), at least ~16
-    // poles per lane and sweep
-    const double kavg_c = tkc / fmax(cc, 1.0);
-    int tpr_c = 1;
-    while (tpr_c < 32 && (double)tpr_c * tkc < 75776.0) {
-        tpr_c <<= 1;
-    }
-    int cap = 1;
-    while (cap < 32 && (double)(cap * 2) * 16.0 <= kavg_c) {
-        cap <<= 1;
-    }
-    tpr_c = tpr_c < cap ? tpr_c : cap;
-    const int Rw = 32 / tpr_w;
-    const int Rc = kSweepThreads / tpr_c;
-    // each thread owns a contiguous run of nodes: serial prefix of its run,
-    // one block scan across threads, then the run's prefixes
-    const int per = (a.nodes + T - 1) / T;
-    const int i0 = threadIdx.x * per;
-    const int i1 = (i0 + per < a.nodes) ? i0 + per : a.nodes;
-    int sw = 0, sc = 0;
-    for (int i = i0; i < i1; ++i) {
-        const int kk = __ldcg(w.nK + i);
-        if (kk > kWarpMaxK) {
-            sc += (kk + Rc - 1) / Rc;
-        } else {
-            sw += (kk + Rw - 1) / Rw;
-        }
-    }
-    int carry_w, carry_c;
-    int rw = block_exscan<T>(sw, iscan, &carry_w);
-    int rc = block_exscan<T>(sc, iscan, &carry_c);
-    for (int i = i0; i < i1; ++i) {
-        const int kk = __ldcg(w.nK + i);
-        w.pref_w[i] = rw;
-        w.pref_c[i] = rc;
-        if (kk > kWarpMaxK) {
-            rc += (kk + Rc - 1) / Rc;
-        } else {
-            rw += (kk + Rw - 1) / Rw;
-        }
-    }
-    __syncthreads();
-    for (int i = threadIdx.x; i < a.nodes; i += T) {
-        const int s0 = w.pref_w[i];
-        const int s1 = (i + 1 < a.nodes) ? w.pref_w[i + 1] : carry_w;
-        for (int q = s0; q < s1; ++q) {
-            w.items_w[q] = i;
-        }
-        const int c0 = w.pref_c[i];
-        const int c1 = (i + 1 < a.nodes) ? w.pref_c[i + 1] : carry_c;
-        for (int q = c0; q < c1; ++q) {
-            w.items_c[q] = i;
-        }
-    }
-    if (threadIdx.x == 0) {
-        w.pref_w[a.nodes] = carry_w;
-        w.pref_c[a.nodes] = carry_c;
-        LevelCtl *c = &w.hdr->lvl[a.k];
-        c->tpr_w = tpr_w;
-        c->tpr_c = tpr_c;
-        c->items_w = carry_w;
-        c->items_c = carry_c;
-        c->total_k = (int)(tkw + tkc);
-        w.hdr->diag[a.k].threads_per_root = carry_c > 0 ? tpr_c : tpr_w;
-    }
+    level_plan<T>(a, red, iscan);
 }
 
 // ------------------------------------------------------------ sweep tiles
