@@ -268,12 +268,71 @@ void launch_md(const KArgs &a, int grid, cudaStream_t s) {
     k_merge_deflate<T><<<grid, T, 0, s>>>(a);
 }
 
+cudaLaunchConfig_t cluster_config(unsigned grid, int C, cudaStream_t s, cudaLaunchAttribute *at) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(1024);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)C;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cfg;
+}
+
+// Largest cluster (8, 4, 2) of 1024-thread deflation CTAs the device can
+// schedule; 1 when none.  Asked once per device.
+int max_defl_cluster(int device) {
+    static int cached[64];
+    static bool done[64];
+    if (device < 0 || device >= 64) {
+        return 1;
+    }
+    if (!done[device]) {
+        int best = 1;
+        for (int C = 8; C >= 2; C >>= 1) {
+            cudaLaunchAttribute at[1];
+            cudaLaunchConfig_t cfg = cluster_config((unsigned)C, C, nullptr, at);
+            int n = 0;
+            if (cudaOccupancyMaxActiveClusters(&n, k_merge_deflate_cl<1024>, &cfg) == cudaSuccess &&
+                n > 0) {
+                best = C;
+                break;
+            }
+            cudaGetLastError();
+        }
+        cached[device] = best;
+        done[device] = true;
+    }
+    return cached[device];
+}
+
 // Returns the number of kernels launched.
-int launch_merge_deflate(const KArgs &a0, int mmax, cudaStream_t s) {
+int launch_merge_deflate(brdc_handle h, const KArgs &a0, int mmax, cudaStream_t s) {
     // about 4 rows per thread, 32..1024 threads
     int t = 32;
     while (t < 1024 && t * 4 < mmax) {
         t <<= 1;
+    }
+    // merges of two or more 4096-row chunks: a cluster of CTAs per node
+    const int chunk = kDeflEPT * 1024;
+    if (mmax >= 2 * chunk) {
+        const int C = std::min(max_defl_cluster(h->device), std::min(8, mmax / chunk));
+        if (C >= 2) {
+            KArgs a = a0;
+            a.plan_inline = a.nodes <= 1024 ? 1 : 0;
+            cudaLaunchAttribute at[1];
+            cudaLaunchConfig_t cfg = cluster_config((unsigned)(a.nodes * C), C, s, at);
+            cudaLaunchKernelEx(&cfg, k_merge_deflate_cl<1024>, a);
+            if (!a.plan_inline) {
+                k_plan<1024><<<1, 1024, 0, s>>>(a);
+                return 2;
+            }
+            return 1;
+        }
     }
     // the level plan walks every node; the last deflation CTA does it while
     // that is at most one node per thread, a 1024-thread k_plan otherwise
@@ -370,7 +429,7 @@ brdc_status run_forest(brdc_handle h, const HostForest &hf, const Layout &L,
         const int grid = cta_blocks + warp_blocks;
         k_merge<<<(unsigned)elem_grid, 256, 0, s>>>(a, hf.total_n);
         BRDC_CUDA(h, "brdc.merge", cudaGetLastError());
-        h->launches += 1 + launch_merge_deflate(a, hf.level_mmax[k], s);
+        h->launches += 1 + launch_merge_deflate(h, a, hf.level_mmax[k], s);
         BRDC_CUDA(h, "brdc.merge_deflate", cudaGetLastError());
         mark(h, 3 + 4 * k);
         k_secular<<<grid, kSweepThreads, cta_blocks ? smem_tiles(2) : 0, s>>>(a, cta_blocks);

@@ -19,6 +19,8 @@
 // cyclic Jacobi).
 #pragma once
 
+#include <cooperative_groups.h>
+
 #include <cfloat>
 #include <cstdint>
 
@@ -435,44 +437,46 @@ __global__ void __launch_bounds__(T) k_plan(KArgs a) {
     level_plan<T>(a, red, iscan);
 }
 
+constexpr int kDeflEPT = 4; // rows per thread per deflation chunk
+
+// Deflation phases over a range of rows, shared by the one-CTA-per-node
+// kernel (whole node) and the cluster kernel (one slice per CTA).
+
+// Rows [r0, r1) of the merged node that survive the small-z test.
 template <int T>
-__global__ void __launch_bounds__(T) k_merge_deflate(KArgs a) {
-    constexpr int EPT = 4; // rows per thread per chunk
-    __shared__ double red[32];
-    __shared__ int iscan[32];
-    __shared__ int s_last;
-    const int g = blockIdx.x;
-    const NodeGeom G = node_geom(a.F, a.k, g);
-    const Ws &w = a.w;
-    const long long gs = G.gstart;
-    const int m = G.m, m1 = G.m1, m2 = G.m - G.m1;
-    const double eps = DBL_EPSILON;
-
-    const double *Ad = w.cd + gs;
-    const double *Bd = w.cd + gs + m1;
-    const double rho = 2.0 * fabs(a.E[gs + m1 - 1]);
-    double maxd = fmax(fmax(fabs(Ad[0]), fabs(Ad[m1 - 1])),
-                       fmax(fabs(Bd[0]), fabs(Bd[m2 - 1])));
-    double lz = 0.0;
-    for (int e = threadIdx.x; e < m; e += T) {
-        lz = fmax(lz, fabs(w.mz[gs + e]));
+__device__ int defl_count_active(const Ws &w, long long gs, int r0, int r1, double rho,
+                                 double tol, int *iscan) {
+    int cnt = 0;
+    for (int base = r0; base < r1; base += kDeflEPT * T) {
+#pragma unroll
+        for (int q = 0; q < kDeflEPT; ++q) {
+            const int idx = base + kDeflEPT * threadIdx.x + q;
+            cnt += (idx < r1 && fabs(rho * w.mz[gs + idx]) > tol) ? 1 : 0;
+        }
     }
-    const double maxz = block_max<T>(lz, red);
-    const double tol = kDeflTolScale * eps * fmax(maxd, maxz);
+    int tot;
+    block_exscan<T>(cnt, iscan, &tot);
+    return tot;
+}
 
-    // compaction 1: small-z survivors (sorted) and small-z deflated (sorted).
-    // Every value a thread moves is loaded before the scan, so a chunk
-    // costs one round trip to L2 instead of one per row.
-    int carry_a = 0, carry_z = 0;
-    for (int base = 0; base < m; base += EPT * T) {
+// Compaction 1 of rows [r0, r1): small-z survivors to the active list from
+// position carry_a, deflated rows to the small-z list from carry_z.  Every
+// value a thread moves is loaded before the scan, so a chunk costs one
+// round trip to L2 instead of one per row.  Returns carry_a plus the
+// survivors.
+template <int T>
+__device__ int defl_compact_active(const Ws &w, long long gs, int r0, int r1, double rho,
+                                   double tol, int carry_a, int carry_z, int *iscan) {
+    constexpr int EPT = kDeflEPT;
+    for (int base = r0; base < r1; base += EPT * T) {
         int fl[EPT];
         double vd[EPT], vz[EPT], vf[EPT], vl[EPT];
         int cnt = 0;
 #pragma unroll
         for (int q = 0; q < EPT; ++q) {
             const int idx = base + EPT * threadIdx.x + q;
-            const bool ok = idx < m;
-            const long long src = gs + (ok ? idx : 0);
+            const bool ok = idx < r1;
+            const long long src = gs + (ok ? idx : r0);
             vd[q] = w.md[src];
             vz[q] = w.mz[src];
             vf[q] = w.mf[src];
@@ -487,7 +491,7 @@ __global__ void __launch_bounds__(T) k_merge_deflate(KArgs a) {
 #pragma unroll
         for (int q = 0; q < EPT; ++q) {
             const int idx = base + EPT * threadIdx.x + q;
-            if (idx < m) {
+            if (idx < r1) {
                 if (fl[q]) {
                     const long long o = gs + ra;
                     w.ad[o] = vd[q];
@@ -507,15 +511,19 @@ __global__ void __launch_bounds__(T) k_merge_deflate(KArgs a) {
                 }
             }
         }
-        const int valid = (m - base) < EPT * T ? (m - base) : EPT * T;
+        const int valid = (r1 - base) < EPT * T ? (r1 - base) : EPT * T;
         carry_a += tot;
         carry_z += valid - tot;
     }
-    const int Kz = carry_a;
-    __syncthreads();
+    return carry_a;
+}
 
-    // close-pole clusters: one thread walks each run of gaps <= tol
-    for (int i = threadIdx.x; i < Kz; i += T) {
+// Close-pole clusters whose run starts at an active index in [i0, i1): one
+// thread walks each run of gaps <= tol (it may read and rotate entries past
+// i1; no other thread touches them).
+template <int T>
+__device__ void defl_close_walk(const Ws &w, long long gs, int Kz, double tol, int i0, int i1) {
+    for (int i = i0 + threadIdx.x; i < i1; i += T) {
         const double di = w.ad[gs + i];
         const bool nxt = (i + 1 < Kz) && (w.ad[gs + i + 1] - di <= tol);
         const bool prv = (i > 0) && (di - w.ad[gs + i - 1] <= tol);
@@ -565,21 +573,42 @@ __global__ void __launch_bounds__(T) k_merge_deflate(KArgs a) {
         w.af[gs + base] = fb;
         w.al[gs + base] = lb;
     }
-    __syncthreads();
+}
 
-    // compaction 2: secular poles (padded slice) and rotated-out members
-    int carry_p = 0, carry_g = 0;
+// Active entries [r0, r1) that remain poles (not rotated out).
+template <int T>
+__device__ int defl_count_poles(const Ws &w, long long gs, int r0, int r1, int *iscan) {
+    int cnt = 0;
+    for (int base = r0; base < r1; base += kDeflEPT * T) {
+#pragma unroll
+        for (int q = 0; q < kDeflEPT; ++q) {
+            const int idx = base + kDeflEPT * threadIdx.x + q;
+            cnt += (idx < r1 && w.gmark[gs + idx] == 0) ? 1 : 0;
+        }
+    }
+    int tot;
+    block_exscan<T>(cnt, iscan, &tot);
+    return tot;
+}
+
+// Compaction 2 of active entries [r0, r1): poles to the padded pole slice
+// from carry_p, rotated-out members to their list from carry_g.  Returns
+// this thread's part of sum z^2 over the poles it moved; *end_p gets
+// carry_p plus the poles.
+template <int T>
+__device__ double defl_compact_poles(const Ws &w, long long gs, long long po, int r0, int r1,
+                                     int carry_p, int carry_g, int *iscan, int *end_p) {
+    constexpr int EPT = kDeflEPT;
     double zn = 0.0;
-    const long long po = G.poff;
-    for (int base = 0; base < Kz; base += EPT * T) {
+    for (int base = r0; base < r1; base += EPT * T) {
         int fl[EPT];
         double vd[EPT], vz[EPT], vf[EPT], vl[EPT];
         int cnt = 0;
 #pragma unroll
         for (int q = 0; q < EPT; ++q) {
             const int idx = base + EPT * threadIdx.x + q;
-            const bool ok = idx < Kz;
-            const long long src = gs + (ok ? idx : 0);
+            const bool ok = idx < r1;
+            const long long src = gs + (ok ? idx : r0);
             vd[q] = w.ad[src];
             vz[q] = w.az[src];
             vf[q] = w.af[src];
@@ -594,7 +623,7 @@ __global__ void __launch_bounds__(T) k_merge_deflate(KArgs a) {
 #pragma unroll
         for (int q = 0; q < EPT; ++q) {
             const int idx = base + EPT * threadIdx.x + q;
-            if (idx < Kz) {
+            if (idx < r1) {
                 if (fl[q]) {
                     const long long o = po + rp;
                     w.pd[o] = vd[q];
@@ -614,14 +643,34 @@ __global__ void __launch_bounds__(T) k_merge_deflate(KArgs a) {
                 }
             }
         }
-        const int valid = (Kz - base) < EPT * T ? (Kz - base) : EPT * T;
+        const int valid = (r1 - base) < EPT * T ? (r1 - base) : EPT * T;
         carry_p += tot;
         carry_g += valid - tot;
     }
-    const int K = carry_p;
-    zn = block_sum<T>(zn, red);
+    *end_p = carry_p;
+    return zn;
+}
 
-    if (threadIdx.x == 0) {
+// Deflation tolerance inputs of node g: rho, max|d| from the ends of the two
+// sorted child spectra.
+__device__ inline void defl_node_scalars(const KArgs &a, const NodeGeom &G, double *rho,
+                                         double *maxd) {
+    const Ws &w = a.w;
+    const long long gs = G.gstart;
+    const double *Ad = w.cd + gs;
+    const double *Bd = w.cd + gs + G.m1;
+    const int m2 = G.m - G.m1;
+    *rho = 2.0 * fabs(a.E[gs + G.m1 - 1]);
+    *maxd = fmax(fmax(fabs(Ad[0]), fabs(Ad[G.m1 - 1])), fmax(fabs(Bd[0]), fabs(Bd[m2 - 1])));
+}
+
+// Node scalars, then the level plan by the last CTA to finish (unless the
+// level runs k_plan).
+template <int T>
+__device__ void defl_finish(const KArgs &a, int g, int K, int Kz, double rho, double tol,
+                            double zn, bool writer, double *red, int *iscan, int *s_last) {
+    const Ws &w = a.w;
+    if (writer && threadIdx.x == 0) {
         w.nK[g] = K;
         w.nKz[g] = Kz;
         w.nrho[g] = rho;
@@ -634,14 +683,144 @@ __global__ void __launch_bounds__(T) k_merge_deflate(KArgs a) {
     if (threadIdx.x == 0) {
         __threadfence();
         const int t = atomicAdd(&w.hdr->lvl[a.k].ticket, 1);
-        s_last = (t == (int)gridDim.x - 1);
+        *s_last = (t == (int)gridDim.x - 1);
     }
     __syncthreads();
-    if (!s_last) {
+    if (!*s_last) {
         return;
     }
     __threadfence();
     level_plan<T>(a, red, iscan);
+}
+
+// One CTA per merge node.
+template <int T>
+__global__ void __launch_bounds__(T) k_merge_deflate(KArgs a) {
+    __shared__ double red[32];
+    __shared__ int iscan[32];
+    __shared__ int s_last;
+    const int g = blockIdx.x;
+    const NodeGeom G = node_geom(a.F, a.k, g);
+    const Ws &w = a.w;
+    const long long gs = G.gstart;
+    const int m = G.m;
+    double rho, maxd;
+    defl_node_scalars(a, G, &rho, &maxd);
+    double lz = 0.0;
+    for (int e = threadIdx.x; e < m; e += T) {
+        lz = fmax(lz, fabs(w.mz[gs + e]));
+    }
+    const double maxz = block_max<T>(lz, red);
+    const double tol = kDeflTolScale * DBL_EPSILON * fmax(maxd, maxz);
+
+    const int Kz = defl_compact_active<T>(w, gs, 0, m, rho, tol, 0, 0, iscan);
+    __syncthreads();
+    defl_close_walk<T>(w, gs, Kz, tol, 0, Kz);
+    __syncthreads();
+    int K;
+    double zn = defl_compact_poles<T>(w, gs, G.poff, 0, Kz, 0, 0, iscan, &K);
+    zn = block_sum<T>(zn, red);
+    defl_finish<T>(a, g, K, Kz, rho, tol, zn, true, red, iscan, &s_last);
+}
+
+// A cluster of C CTAs per merge node (the large merges near the top of the
+// tree, which one CTA would stream alone).  CTA r of the cluster owns rows
+// [r S, (r+1) S) of the node (S a whole number of chunks), then the same
+// share of the active list.  The tolerance maximum and the compaction counts
+// are exchanged through distributed shared memory between cluster barriers,
+// so each CTA scatters from its exact offset and the lists come out exactly
+// as the one-CTA kernel writes them (only sum z^2 is added in another
+// order).  The close-pole walk reads the whole active list from global
+// memory after a barrier, which a fence before it makes cluster-visible.
+template <int T>
+__global__ void __launch_bounds__(T) k_merge_deflate_cl(KArgs a) {
+    namespace cg = cooperative_groups;
+    __shared__ double red[32];
+    __shared__ int iscan[32];
+    __shared__ int s_last;
+    __shared__ double s_val;
+    __shared__ int s_cnt;
+    cg::cluster_group cl = cg::this_cluster();
+    const int C = (int)cl.num_blocks();
+    const int rank = (int)cl.block_rank();
+    const int g = blockIdx.x / C;
+    const NodeGeom G = node_geom(a.F, a.k, g);
+    const Ws &w = a.w;
+    const long long gs = G.gstart;
+    const int m = G.m;
+    constexpr int chunk = kDeflEPT * T;
+    double rho, maxd;
+    defl_node_scalars(a, G, &rho, &maxd);
+
+    const int S = ((m + C - 1) / C + chunk - 1) / chunk * chunk;
+    const int r0 = min(m, rank * S), r1 = min(m, r0 + S);
+    double lz = 0.0;
+    for (int e = r0 + threadIdx.x; e < r1; e += T) {
+        lz = fmax(lz, fabs(w.mz[gs + e]));
+    }
+    lz = block_max<T>(lz, red);
+    if (threadIdx.x == 0) {
+        s_val = lz;
+    }
+    cl.sync();
+    double maxz = 0.0;
+    for (int r = 0; r < C; ++r) {
+        maxz = fmax(maxz, *cl.map_shared_rank(&s_val, r));
+    }
+    const double tol = kDeflTolScale * DBL_EPSILON * fmax(maxd, maxz);
+
+    // compaction 1
+    const int na = defl_count_active<T>(w, gs, r0, r1, rho, tol, iscan);
+    if (threadIdx.x == 0) {
+        s_cnt = na;
+    }
+    cl.sync();
+    int off_a = 0, Kz = 0;
+    for (int r = 0; r < C; ++r) {
+        const int c = *cl.map_shared_rank(&s_cnt, r);
+        off_a += r < rank ? c : 0;
+        Kz += c;
+    }
+    defl_compact_active<T>(w, gs, r0, r1, rho, tol, off_a, r0 - off_a, iscan);
+    __threadfence();
+    cl.sync();
+
+    // close-pole walk over this CTA's share of chain starts
+    const int A = (Kz + C - 1) / C;
+    defl_close_walk<T>(w, gs, Kz, tol, min(Kz, rank * A), min(Kz, rank * A + A));
+    __threadfence();
+    cl.sync();
+
+    // compaction 2
+    const int S2 = ((Kz + C - 1) / C + chunk - 1) / chunk * chunk;
+    const int q0 = min(Kz, rank * S2), q1 = min(Kz, q0 + S2);
+    const int np = defl_count_poles<T>(w, gs, q0, q1, iscan);
+    if (threadIdx.x == 0) {
+        s_cnt = np;
+    }
+    cl.sync();
+    int off_p = 0, K = 0;
+    for (int r = 0; r < C; ++r) {
+        const int c = *cl.map_shared_rank(&s_cnt, r);
+        off_p += r < rank ? c : 0;
+        K += c;
+    }
+    int end_p;
+    double zn = defl_compact_poles<T>(w, gs, G.poff, q0, q1, off_p, q0 - off_p, iscan, &end_p);
+    zn = block_sum<T>(zn, red);
+    if (threadIdx.x == 0) {
+        s_val = zn;
+    }
+    cl.sync();
+    double zt = 0.0;
+    if (rank == 0) {
+        for (int r = 0; r < C; ++r) {
+            zt += *cl.map_shared_rank(&s_val, r);
+        }
+    }
+    // no CTA leaves while a peer may still read its shared memory
+    cl.sync();
+    defl_finish<T>(a, g, K, Kz, rho, tol, zt, rank == 0, red, iscan, &s_last);
 }
 
 // ------------------------------------------------------------ sweep tiles
