@@ -731,7 +731,7 @@ __global__ void __launch_bounds__(T) k_merge_deflate(KArgs a) {
 // so each CTA scatters from its exact offset and the lists come out exactly
 // as the one-CTA kernel writes them (only sum z^2 is added in another
 // order).  The close-pole walk reads the whole active list from global
-// memory after a barrier, which a fence before it makes cluster-visible.
+// memory after a cluster barrier.
 template <int T>
 __global__ void __launch_bounds__(T) k_merge_deflate_cl(KArgs a) {
     namespace cg = cooperative_groups;
@@ -781,14 +781,14 @@ __global__ void __launch_bounds__(T) k_merge_deflate_cl(KArgs a) {
         off_a += r < rank ? c : 0;
         Kz += c;
     }
+    // the cluster barrier releases and acquires at cluster scope, which
+    // orders these global writes for the peer CTAs without a device fence
     defl_compact_active<T>(w, gs, r0, r1, rho, tol, off_a, r0 - off_a, iscan);
-    __threadfence();
     cl.sync();
 
     // close-pole walk over this CTA's share of chain starts
     const int A = (Kz + C - 1) / C;
     defl_close_walk<T>(w, gs, Kz, tol, min(Kz, rank * A), min(Kz, rank * A + A));
-    __threadfence();
     cl.sync();
 
     // compaction 2
@@ -955,12 +955,29 @@ __device__ inline void secular_store(const Ws &w, const KArgs &a, long long po,
     w.rdo[o] = st.dorg;
     w.rtau[o] = st.tau;
     w.rlam[o] = st.dorg + st.tau;
-    brdc_level_diagnostics *dg = &w.hdr->diag[a.k];
-    atomicAdd(&dg->secular_iter_sum, st.iter);
-    atomicMax(&dg->secular_iter_max, st.iter);
-    if (st.failed) {
-        atomicAdd(&dg->secular_iter_failed, 1);
-        atomicAdd(&w.hdr->nonconv, 1);
+}
+
+// Iteration counters of the level diagnostics, reduced over the warp first:
+// one atomic per warp instead of one per root keeps the same-address
+// traffic at L2 off the critical path.  Called by every lane of the warp;
+// `mine` marks the lanes that report a root.
+__device__ inline void secular_diag_warp(const Ws &w, int k, bool mine, const SecRoot &st) {
+    const unsigned full = 0xffffffffu;
+    const int it = mine ? st.iter : 0;
+    const int fl = mine ? st.failed : 0;
+    const int sum = __reduce_add_sync(full, it);
+    const int mx = __reduce_max_sync(full, it);
+    const int nf = __reduce_add_sync(full, fl);
+    if ((threadIdx.x & 31) == 0) {
+        brdc_level_diagnostics *dg = &w.hdr->diag[k];
+        if (sum != 0) {
+            atomicAdd(&dg->secular_iter_sum, sum);
+            atomicMax(&dg->secular_iter_max, mx);
+        }
+        if (nf != 0) {
+            atomicAdd(&dg->secular_iter_failed, nf);
+            atomicAdd(&w.hdr->nonconv, nf);
+        }
     }
 }
 
@@ -1125,6 +1142,7 @@ __global__ void __launch_bounds__(kSweepThreads)
             if (active && l == 0) {
                 secular_store(w, a, po, r, st);
             }
+            secular_diag_warp(w, a.k, active && l == 0, st);
         }
         return;
     }
@@ -1193,6 +1211,7 @@ __global__ void __launch_bounds__(kSweepThreads)
         if (active && lane == 0) {
             secular_store(w, a, po, r, st);
         }
+        secular_diag_warp(w, a.k, active && lane == 0, st);
         __syncthreads();
     }
 }
