@@ -195,6 +195,27 @@ typedef struct brdc_timings {
     float level_ms[BRDC_MAX_LEVELS][4]; /* merge, secular, lowner, rows */
 } brdc_timings;
 
+/* Launch-shape parameters of a handle's solves.  None changes a result
+ * beyond rounding: deflation decisions, roots and ordering follow the
+ * same rules under every setting.  No reference counterpart (the
+ * prototype's shapes are compile-time constants).
+ *   subtree_levels      merge levels solved inside the per-subtree kernel,
+ *                       with its leaves, in shared memory (0..4; 0 runs the
+ *                       leaves alone and every level with per-level kernels)
+ *   deflate_cluster     largest thread-block cluster that deflates one big
+ *                       merge (1, 2, 4 or 8; 1 = one CTA per merge)
+ *   sweep_lanes_target  threads the per-level root sweeps aim to keep busy
+ *                       (lanes per root = smallest power of two reaching it)
+ * brdc_autotune (below) picks them by timing; defaults: 4, 8, 75776. */
+typedef struct brdc_tuning {
+    int subtree_levels;
+    int deflate_cluster;
+    int sweep_lanes_target;
+} brdc_tuning;
+
+brdc_status brdc_set_tuning(brdc_handle handle, const brdc_tuning *tuning);
+brdc_status brdc_get_tuning(brdc_handle handle, brdc_tuning *tuning);
+
 brdc_status brdc_set_timing(brdc_handle handle, int enable);
 brdc_status brdc_get_last_timings(brdc_handle handle, brdc_timings *out);
 

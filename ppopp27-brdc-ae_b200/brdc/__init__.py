@@ -65,6 +65,8 @@ EXPORTS = (
     "brdc_dstebr_noalloc",
     "brdc_dstebr_batched_checkpoint_workspace_size",
     "brdc_dstebr_batched_backward",
+    "brdc_set_tuning",
+    "brdc_get_tuning",
 )
 
 
@@ -110,6 +112,17 @@ class Diagnostics(ctypes.Structure):
             lv = self.level[k]
             out["level"].append({f: getattr(lv, f) for f, _ in LevelDiag._fields_})
         return out
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [
+        ("subtree_levels", ctypes.c_int),
+        ("deflate_cluster", ctypes.c_int),
+        ("sweep_lanes_target", ctypes.c_int),
+    ]
+
+    def as_dict(self) -> dict:
+        return {f: getattr(self, f) for f, _ in self._fields_}
 
 
 class Timings(ctypes.Structure):
@@ -174,12 +187,15 @@ def load() -> ctypes.CDLL:
     lib.brdc_set_timing.argtypes = [vp, ctypes.c_int]
     lib.brdc_dstebr_noalloc.argtypes = [vp, i64, vp, vp, vp]
     lib.brdc_get_last_timings.argtypes = [vp, ctypes.POINTER(Timings)]
+    lib.brdc_set_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
+    lib.brdc_get_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
     for f in ("brdc_create", "brdc_destroy", "brdc_set_stream", "brdc_get_stream",
               "brdc_get_last_error", "brdc_dstebr_workspace_size", "brdc_dstebr",
               "brdc_dstebr_backward", "brdc_get_info", "brdc_get_diagnostics",
               "brdc_dstebr_batched_workspace_size", "brdc_dstebr_batched",
               "brdc_set_timing", "brdc_get_last_timings", "brdc_dstebr_noalloc",
-              "brdc_dstebr_batched_checkpoint_workspace_size", "brdc_dstebr_batched_backward"):
+              "brdc_dstebr_batched_checkpoint_workspace_size", "brdc_dstebr_batched_backward",
+              "brdc_set_tuning", "brdc_get_tuning"):
         getattr(lib, f).restype = ctypes.c_int
     _lib = lib
     return lib
@@ -250,6 +266,19 @@ class Solver:
         s = stream if stream is not None else torch.cuda.current_stream()
         self.stream = s
         _check(load().brdc_set_stream(self.h, ctypes.c_void_p(s.cuda_stream)), "set_stream", self.h)
+
+    def tuning(self) -> dict:
+        t = Tuning()
+        _check(load().brdc_get_tuning(self.h, ctypes.byref(t)), "get_tuning", self.h)
+        return t.as_dict()
+
+    def set_tuning(self, **kw) -> None:
+        """Change launch-shape parameters (subtree_levels, deflate_cluster,
+        sweep_lanes_target); the others keep their values."""
+        cur = self.tuning()
+        cur.update(kw)
+        t = Tuning(**cur)
+        _check(load().brdc_set_tuning(self.h, ctypes.byref(t)), "set_tuning", self.h)
 
     def set_timing(self, enable: bool) -> None:
         _check(load().brdc_set_timing(self.h, 1 if enable else 0), "set_timing", self.h)

@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "brdc_backward.cuh"
+#include "brdc_subtree.cuh"
 
 using namespace brdc;
 
@@ -33,6 +34,11 @@ struct brdc_handle_struct {
     // batched: signature of the forest whose tables sit in a workspace
     const void *prep_ws;
     bool prep_ckpt = false;
+    int prep_sub = -1;
+    // merge levels solved inside the subtree kernel (0: leaves alone)
+    int sub_levels = kSubMaxLevels;
+    int defl_cluster = 8;         // largest deflation cluster
+    int lanes_target = 75776;     // root-sweep parallelism target
     std::vector<long long> prep_off;
     // phase timing (off by default)
     int timing;
@@ -67,6 +73,13 @@ void set_error(brdc_handle h, int code, brdc_error_source src,
 constexpr size_t kAlign = 256; // gpu/src/workspace_align.hpp:9
 
 size_t align_up(size_t v) { return (v + kAlign - 1) / kAlign * kAlign; }
+
+// Subtrees of an instance with L merge levels when the subtree kernel
+// takes its lowest `fused` levels.
+long long subtrees_of(int L, int fused) {
+    const int Ls = L < fused ? L : fused;
+    return 1LL << (L - Ls);
+}
 
 // Host view of a forest.
 struct HostForest {
@@ -163,6 +176,7 @@ const SlotDesc kSlots[] = {
     SI(items_w, CN_ITW, true, false), SI(items_c, CN_ITC, true, false),
     SL(f_off, CN_B1, false, false), SI(f_lev, CN_B, false, false),
     SI(f_node_prefix, CN_NODEPRE, false, false), SI(f_leaf_prefix, CN_B1, false, false),
+    SI(f_sub_prefix, CN_B1, false, false),
     // adjoint
     SD(bcd, CN_NT, false, true), SD(bcf, CN_NT, false, true), SD(bcl, CN_NT, false, true),
     SD(bnd, CN_NT, false, true), SD(bnf, CN_NT, false, true), SD(bnl, CN_NT, false, true),
@@ -320,7 +334,8 @@ int launch_merge_deflate(brdc_handle h, const KArgs &a0, int mmax, cudaStream_t 
     // merges of two or more 4096-row chunks: a cluster of CTAs per node
     const int chunk = kDeflEPT * 1024;
     if (mmax >= 2 * chunk) {
-        const int C = std::min(max_defl_cluster(h->device), std::min(8, mmax / chunk));
+        const int C = std::min(std::min(max_defl_cluster(h->device), h->defl_cluster),
+                               std::min(8, mmax / chunk));
         if (C >= 2) {
             KArgs a = a0;
             a.plan_inline = a.nodes <= 1024 ? 1 : 0;
@@ -372,6 +387,10 @@ cudaError_t set_attrs() {
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem_tiles(4));
     }
+    if (e == cudaSuccess) {
+        e = cudaFuncSetAttribute(k_subtree, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(SubSmem));
+    }
     g_attr_done = (e == cudaSuccess);
     return e;
 }
@@ -406,7 +425,56 @@ brdc_status run_forest(brdc_handle h, const HostForest &hf, const Layout &L,
     a.D = D;
     a.E = E;
     a.W = W;
-    {
+    a.lanes_target = h->lanes_target;
+    // leaves and the lowest merge levels
+    const int fused = std::min(h->sub_levels, hf.max_levels);
+    if (h->sub_levels > 0) {
+        SubArgs A{};
+        A.a = a;
+        for (int k = 0; k < fused; ++k) {
+            A.lw[k] = w;
+            level_view(hf, L, w, k, &A.lw[k]);
+        }
+        // the first per-level merge (level `fused`) reads the buffer that
+        // `fused` ping-pong swaps leave in the child slot
+        A.out_d = (fused & 1) ? w.nd : w.cd;
+        A.out_f = (fused & 1) ? w.nf : w.cf;
+        A.out_l = (fused & 1) ? w.nl : w.cl;
+        A.levels = h->sub_levels;
+        A.ckpt = L.ckpt ? 1 : 0;
+        long long subs = 0;
+        for (int b = 0; b < hf.B; ++b) {
+            subs += subtrees_of(hf.lev[b], h->sub_levels);
+        }
+        k_subtree<<<(unsigned)subs, kSubRows, sizeof(SubSmem), s>>>(A);
+        BRDC_CUDA(h, "brdc.subtree", cudaGetLastError());
+        ++h->launches;
+        mark(h, 2);
+        for (int k = 0; k < fused; ++k) {
+            for (int q = 3; q <= 6; ++q) {
+                mark(h, q + 4 * k);
+            }
+            h->has_lowner[k] = 0;
+        }
+        if (L.ckpt) {
+            // item tables of the fused levels, which the adjoint's sweeps use
+            for (int k = 0; k < fused; ++k) {
+                KArgs ak = a;
+                ak.k = k;
+                ak.nodes = hf.level_nodes[k];
+                ak.level_rows = hf.level_rows[k];
+                level_view(hf, L, w, k, &ak.w);
+                k_plan<1024><<<1, 1024, 0, s>>>(ak);
+                ++h->launches;
+            }
+            BRDC_CUDA(h, "brdc.subtree_plan", cudaGetLastError());
+        }
+        if (fused & 1) {
+            std::swap(a.w.cd, a.w.nd);
+            std::swap(a.w.cf, a.w.nf);
+            std::swap(a.w.cl, a.w.nl);
+        }
+    } else {
         const long long per = 2LL * kLeafWarps; // leaves per block
         long long grid = (hf.leaves + per - 1) / per;
         grid = std::min<long long>(grid, (long long)h->sm_count * 16);
@@ -419,7 +487,7 @@ brdc_status run_forest(brdc_handle h, const HostForest &hf, const Layout &L,
     const int warp_blocks = h->sm_count * 2;
     long long elem_grid = (hf.total_n + 255) / 256;
     elem_grid = std::max<long long>(1, std::min<long long>(elem_grid, (long long)h->sm_count * 8));
-    for (int k = 0; k < hf.max_levels; ++k) {
+    for (int k = (h->sub_levels > 0 ? fused : 0); k < hf.max_levels; ++k) {
         a.k = k;
         a.nodes = hf.level_nodes[k];
         a.level_rows = hf.level_rows[k];
@@ -509,6 +577,38 @@ extern "C" brdc_status brdc_destroy(brdc_handle h) {
         cudaStreamDestroy(h->own_stream);
     }
     delete h;
+    return BRDC_STATUS_SUCCESS;
+}
+
+extern "C" brdc_status brdc_set_tuning(brdc_handle h, const brdc_tuning *t) {
+    if (h == nullptr) {
+        return BRDC_STATUS_INVALID_HANDLE;
+    }
+    if (t == nullptr) {
+        return BRDC_STATUS_INVALID_POINTER;
+    }
+    const int c = t->deflate_cluster;
+    if (t->subtree_levels < 0 || t->subtree_levels > kSubMaxLevels ||
+        !(c == 1 || c == 2 || c == 4 || c == 8) || t->sweep_lanes_target < 1024 ||
+        t->sweep_lanes_target > (1 << 24)) {
+        return BRDC_STATUS_INVALID_VALUE;
+    }
+    h->sub_levels = t->subtree_levels;
+    h->defl_cluster = c;
+    h->lanes_target = t->sweep_lanes_target;
+    return BRDC_STATUS_SUCCESS;
+}
+
+extern "C" brdc_status brdc_get_tuning(brdc_handle h, brdc_tuning *t) {
+    if (h == nullptr) {
+        return BRDC_STATUS_INVALID_HANDLE;
+    }
+    if (t == nullptr) {
+        return BRDC_STATUS_INVALID_POINTER;
+    }
+    t->subtree_levels = h->sub_levels;
+    t->deflate_cluster = h->defl_cluster;
+    t->sweep_lanes_target = h->lanes_target;
     return BRDC_STATUS_SUCCESS;
 }
 
@@ -742,6 +842,7 @@ brdc_status prepare_forest(brdc_handle h, const HostForest &hf, const Ws &w,
         return BRDC_STATUS_SUCCESS;
     }
     const bool same = h->prep_ws == workspace && h->prep_ckpt == ckpt &&
+                      h->prep_sub == h->sub_levels &&
                       h->prep_off.size() == (size_t)hf.B + 1 &&
                       std::equal(h->prep_off.begin(), h->prep_off.end(), hf.off.begin());
     if (!same) {
@@ -755,8 +856,10 @@ brdc_status prepare_forest(brdc_handle h, const HostForest &hf, const Ws &w,
             }
         }
         std::vector<int> leaf_prefix(hf.B + 1, 0);
+        std::vector<int> sub_prefix(hf.B + 1, 0);
         for (int b = 0; b < hf.B; ++b) {
             leaf_prefix[b + 1] = leaf_prefix[b] + (1 << hf.lev[b]);
+            sub_prefix[b + 1] = sub_prefix[b] + (int)subtrees_of(hf.lev[b], h->sub_levels);
         }
         BRDC_CUDA(h, "brdc.batched.upload_off",
                   cudaMemcpyAsync(w.f_off, hf.off.data(), sizeof(long long) * (hf.B + 1),
@@ -772,15 +875,21 @@ brdc_status prepare_forest(brdc_handle h, const HostForest &hf, const Ws &w,
                   cudaMemcpyAsync(w.f_leaf_prefix, leaf_prefix.data(),
                                   sizeof(int) * leaf_prefix.size(), cudaMemcpyHostToDevice,
                                   h->stream));
+        BRDC_CUDA(h, "brdc.batched.upload_subtrees",
+                  cudaMemcpyAsync(w.f_sub_prefix, sub_prefix.data(),
+                                  sizeof(int) * sub_prefix.size(), cudaMemcpyHostToDevice,
+                                  h->stream));
         BRDC_CUDA(h, "brdc.batched.upload_sync", cudaStreamSynchronize(h->stream));
         h->prep_ws = workspace;
         h->prep_ckpt = ckpt;
+        h->prep_sub = h->sub_levels;
         h->prep_off = hf.off;
     }
     F->off = w.f_off;
     F->lev = w.f_lev;
     F->node_prefix = w.f_node_prefix;
     F->leaf_prefix = w.f_leaf_prefix;
+    F->sub_prefix = w.f_sub_prefix;
     return BRDC_STATUS_SUCCESS;
 }
 

@@ -100,6 +100,7 @@ struct Forest {
     const int *lev;             // [B] levels per instance (B > 1)
     const int *node_prefix;     // [max_levels][B+1] node-count prefix (B > 1)
     const int *leaf_prefix;     // [B+1] leaf-count prefix (B > 1)
+    const int *sub_prefix;      // [B+1] subtree-count prefix (B > 1)
 };
 
 // Every device array of one workspace.
@@ -133,7 +134,7 @@ struct Ws {
     int *items_w, *items_c;      // work item -> merge node (per role)
     // forest tables (batched)
     long long *f_off;
-    int *f_lev, *f_node_prefix, *f_leaf_prefix;
+    int *f_lev, *f_node_prefix, *f_leaf_prefix, *f_sub_prefix;
     // adjoint (present when the workspace keeps checkpoints)
     double *bcd, *bcf, *bcl, *bnd, *bnf, *bnl;   // cotangents, ping-pong
     double *bmd, *bmz, *bmf, *bml;               // at merged positions

@@ -39,6 +39,7 @@ struct KArgs {
     int nodes;          // merges at this level
     long long level_rows; // rows of the instances that merge at this level
     int plan_inline;    // the last deflation CTA writes the level plan (else k_plan)
+    int lanes_target;   // threads the root sweeps aim to keep busy
 };
 
 // ------------------------------------------------------------------ leaves
@@ -141,12 +142,104 @@ __device__ __forceinline__ double half_max(double v) {
     return v;
 }
 
+// Jacobi solve of one leaf by a half-warp (lane x of the half owns column x;
+// both halves of the warp call this together, the other half on its own
+// leaf or with s = 0).  Returns the leaf's eigenvalue of rank x (ascending;
+// +inf for x >= s) with the first and last entries of its eigenvector, and
+// the number of sweeps taken.
+__device__ inline int leaf_solve(const KArgs &a, const LeafGeom &G, int s, int x,
+                                 double *key_out, double *v0_out, double *v1_out) {
+    const double eps = DBL_EPSILON;
+    double dx = 0.0, ex = 0.0, exm1 = 0.0;
+    if (x < s) {
+        dx = a.D[G.gstart + x];
+        if (x == 0 && G.gstart > G.istart) {
+            dx -= fabs(a.E[G.gstart - 1]);
+        }
+        if (x == s - 1 && G.gstart + s < G.iend) {
+            dx -= fabs(a.E[G.gstart + s - 1]);
+        }
+        if (x + 1 < s) {
+            ex = fabs(a.E[G.gstart + x]);
+        }
+        if (x >= 1) {
+            exm1 = fabs(a.E[G.gstart + x - 1]);
+        }
+    }
+    double reg[16];
+    const int jup = x ^ (x + 1);
+    const int jdn = x ^ (x - 1);
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        reg[j] = (j == 0) ? dx : ((j == jup) ? ex : ((j == jdn) ? exm1 : 0.0));
+    }
+    double v0 = (x == 0 && s > 0) ? 1.0 : 0.0;
+    double v1 = (x == s - 1) ? 1.0 : 0.0;
+    const double amax = half_max(fmax(fabs(dx), fmax(ex, exm1)));
+    const double th = 1.0e-3 * eps * amax;
+    int sweep = 0;
+    for (; sweep < 40; ++sweep) {
+        double off = 0.0;
+#pragma unroll
+        for (int j = 1; j < 16; ++j) {
+            off = fmax(off, fabs(reg[j]));
+        }
+        off = half_max(off);
+        if (!__any_sync(kFull, off > th)) {
+            break;
+        }
+        leaf_round<1>(reg, v0, v1, x, th);
+        leaf_round<2>(reg, v0, v1, x, th);
+        leaf_round<3>(reg, v0, v1, x, th);
+        leaf_round<4>(reg, v0, v1, x, th);
+        leaf_round<5>(reg, v0, v1, x, th);
+        leaf_round<6>(reg, v0, v1, x, th);
+        leaf_round<7>(reg, v0, v1, x, th);
+        leaf_round<8>(reg, v0, v1, x, th);
+        leaf_round<9>(reg, v0, v1, x, th);
+        leaf_round<10>(reg, v0, v1, x, th);
+        leaf_round<11>(reg, v0, v1, x, th);
+        leaf_round<12>(reg, v0, v1, x, th);
+        leaf_round<13>(reg, v0, v1, x, th);
+        leaf_round<14>(reg, v0, v1, x, th);
+        leaf_round<15>(reg, v0, v1, x, th);
+    }
+
+    // bitonic sort of (eigenvalue, column) within the half-warp
+    double key = (x < s) ? reg[0] : INFINITY;
+    int col = x;
+#pragma unroll
+    for (int size = 2; size <= 16; size <<= 1) {
+#pragma unroll
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            const double ok = __shfl_xor_sync(kFull, key, stride);
+            const int oc = __shfl_xor_sync(kFull, col, stride);
+            const double o0 = __shfl_xor_sync(kFull, v0, stride);
+            const double o1 = __shfl_xor_sync(kFull, v1, stride);
+            const bool up = (size == 16) || ((x & size) == 0);
+            const bool lower = ((x & stride) == 0);
+            const bool take_min = (up == lower);
+            const bool swap = take_min ? (ok < key || (ok == key && oc < col))
+                                       : (ok > key || (ok == key && oc > col));
+            if (swap) {
+                key = ok;
+                col = oc;
+                v0 = o0;
+                v1 = o1;
+            }
+        }
+    }
+    *key_out = key;
+    *v0_out = v0;
+    *v1_out = v1;
+    return sweep;
+}
+
 __global__ void __launch_bounds__(kLeafWarps * 32)
     k_leaf(KArgs a, long long total_leaves) {
     const int lane = threadIdx.x & 31;
     const int x = lane & 15;
     const int half = lane >> 4;
-    const double eps = DBL_EPSILON;
     int sweeps_max = 0;
     const long long pairs = (total_leaves + 1) / 2;
     for (long long pr = (long long)blockIdx.x * kLeafWarps + (threadIdx.x >> 5); pr < pairs;
@@ -159,86 +252,9 @@ __global__ void __launch_bounds__(kLeafWarps * 32)
             G = leaf_geom(a.F, leaf);
             s = G.s;
         }
-        double dx = 0.0, ex = 0.0, exm1 = 0.0;
-        if (x < s) {
-            dx = a.D[G.gstart + x];
-            if (x == 0 && G.gstart > G.istart) {
-                dx -= fabs(a.E[G.gstart - 1]);
-            }
-            if (x == s - 1 && G.gstart + s < G.iend) {
-                dx -= fabs(a.E[G.gstart + s - 1]);
-            }
-            if (x + 1 < s) {
-                ex = fabs(a.E[G.gstart + x]);
-            }
-            if (x >= 1) {
-                exm1 = fabs(a.E[G.gstart + x - 1]);
-            }
-        }
-        double reg[16];
-        const int jup = x ^ (x + 1);
-        const int jdn = x ^ (x - 1);
-#pragma unroll
-        for (int j = 0; j < 16; ++j) {
-            reg[j] = (j == 0) ? dx : ((j == jup) ? ex : ((j == jdn) ? exm1 : 0.0));
-        }
-        double v0 = (x == 0 && s > 0) ? 1.0 : 0.0;
-        double v1 = (x == s - 1) ? 1.0 : 0.0;
-        const double amax = half_max(fmax(fabs(dx), fmax(ex, exm1)));
-        const double th = 1.0e-3 * eps * amax;
-        int sweep = 0;
-        for (; sweep < 40; ++sweep) {
-            double off = 0.0;
-#pragma unroll
-            for (int j = 1; j < 16; ++j) {
-                off = fmax(off, fabs(reg[j]));
-            }
-            off = half_max(off);
-            if (!__any_sync(kFull, off > th)) {
-                break;
-            }
-            leaf_round<1>(reg, v0, v1, x, th);
-            leaf_round<2>(reg, v0, v1, x, th);
-            leaf_round<3>(reg, v0, v1, x, th);
-            leaf_round<4>(reg, v0, v1, x, th);
-            leaf_round<5>(reg, v0, v1, x, th);
-            leaf_round<6>(reg, v0, v1, x, th);
-            leaf_round<7>(reg, v0, v1, x, th);
-            leaf_round<8>(reg, v0, v1, x, th);
-            leaf_round<9>(reg, v0, v1, x, th);
-            leaf_round<10>(reg, v0, v1, x, th);
-            leaf_round<11>(reg, v0, v1, x, th);
-            leaf_round<12>(reg, v0, v1, x, th);
-            leaf_round<13>(reg, v0, v1, x, th);
-            leaf_round<14>(reg, v0, v1, x, th);
-            leaf_round<15>(reg, v0, v1, x, th);
-        }
+        double key, v0, v1;
+        const int sweep = leaf_solve(a, G, s, x, &key, &v0, &v1);
         sweeps_max = sweeps_max > sweep ? sweeps_max : sweep;
-
-        // bitonic sort of (eigenvalue, column) within the half-warp
-        double key = (x < s) ? reg[0] : INFINITY;
-        int col = x;
-#pragma unroll
-        for (int size = 2; size <= 16; size <<= 1) {
-#pragma unroll
-            for (int stride = size >> 1; stride > 0; stride >>= 1) {
-                const double ok = __shfl_xor_sync(kFull, key, stride);
-                const int oc = __shfl_xor_sync(kFull, col, stride);
-                const double o0 = __shfl_xor_sync(kFull, v0, stride);
-                const double o1 = __shfl_xor_sync(kFull, v1, stride);
-                const bool up = (size == 16) || ((x & size) == 0);
-                const bool lower = ((x & stride) == 0);
-                const bool take_min = (up == lower);
-                const bool swap = take_min ? (ok < key || (ok == key && oc < col))
-                                           : (ok > key || (ok == key && oc > col));
-                if (swap) {
-                    key = ok;
-                    col = oc;
-                    v0 = o0;
-                    v1 = o1;
-                }
-            }
-        }
         if (x < s) {
             const long long o = G.gstart + x;
             if (G.top) {
@@ -357,17 +373,17 @@ __device__ void level_plan(const KArgs &a, double *red, int *iscan) {
         dg->dd_after_sq_sum = (long long)sk2;
     }
     // warp role: each root's sweeps form a serial latency chain, so spread
-    // the roots over enough lanes to keep every scheduler busy (~75k
-    // threads); with one root per warp the warp also never diverges.
+    // the roots over enough lanes to keep every scheduler busy (by default
+    // ~75k threads); with one root per warp the warp also never diverges.
     int tpr_w = 1;
-    while (tpr_w < 32 && (double)tpr_w * tkw < 75776.0) {
+    while (tpr_w < 32 && (double)tpr_w * tkw < (double)a.lanes_target) {
         tpr_w <<= 1;
     }
-    // CTA role: enough lanes to fill the GPU (~75k threads), at least ~16
-    // poles per lane and sweep
+    // CTA role: enough lanes to fill the GPU, at least ~16 poles per lane
+    // and sweep
     const double kavg_c = tkc / fmax(cc, 1.0);
     int tpr_c = 1;
-    while (tpr_c < 32 && (double)tpr_c * tkc < 75776.0) {
+    while (tpr_c < 32 && (double)tpr_c * tkc < (double)a.lanes_target) {
         tpr_c <<= 1;
     }
     int cap = 1;

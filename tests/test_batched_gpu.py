@@ -120,3 +120,31 @@ def test_graph_capture_batched(solver):
     g.replay()
     torch.cuda.synchronize()
     assert torch.equal(W, ref)
+
+
+def test_batched_tunings_agree(solver):
+    """A batch of mixed orders (tiny ones solved wholly inside the subtree
+    kernel, large ones continuing with per-level kernels) gives the same
+    eigenvalues whatever the subtree depth."""
+    import torch
+
+    import brdc
+
+    off, D, E, orders, _ = families.batch(60, 17, 3000, seed=4)
+    Dt = torch.tensor(D, device="cuda")
+    Et = torch.tensor(E, device="cuda")
+    s = brdc.Solver()
+    try:
+        res = []
+        for sub in (0, 2, 4):
+            s.set_tuning(subtree_levels=sub)
+            res.append(s.dstebr_batched(off, Dt, Et).cpu().numpy())
+        for r in res[1:]:
+            for b in range(len(orders)):
+                lo, hi = int(off[b]), int(off[b + 1])
+                sc = max(np.max(np.abs(res[0][lo:hi])), 1e-300)
+                assert np.max(np.abs(r[lo:hi] - res[0][lo:hi])) < 1e-13 * sc, b
+        errs = per_instance_errors(off, res[-1], D, E)
+        assert errs.max() < TOL
+    finally:
+        s.close()

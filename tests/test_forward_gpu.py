@@ -119,3 +119,49 @@ def test_lapack_style_host_entry(built_lib):
     d, e = families.generate("normal", 5000)
     w = brdc.dstedc_dc_br(d, e)
     assert rel_err(w, np.sort(oracle.dsterf(d, e))) < TOL
+
+
+@pytest.mark.parametrize("family,n", [("uniform", 20000), ("toeplitz", 5000), ("clustered", 9000)])
+def test_tunings_agree(solver, family, n):
+    """Launch shapes do not change what is computed: the same deflation
+    counts at every level and the same eigenvalues to rounding, whatever
+    the subtree depth, deflation cluster and sweep parallelism."""
+    import torch
+
+    import brdc
+
+    d, e = families.generate(family, n)
+    D = torch.tensor(d, device="cuda")
+    E = torch.tensor(e, device="cuda")
+    s = brdc.Solver()
+    ref_w, ref_k = None, None
+    try:
+        for sub in (0, 1, 2, 3, 4):
+            for cl in (1, 8):
+                for lanes in (8192, 75776, 1 << 20):
+                    s.set_tuning(subtree_levels=sub, deflate_cluster=cl, sweep_lanes_target=lanes)
+                    ws = s.workspace(n)
+                    W = s.dstebr(D, E, workspace=ws).cpu().numpy()
+                    K = [lv["dd_after_sum"] for lv in s.diagnostics(n, ws)["level"]]
+                    if ref_w is None:
+                        ref_w, ref_k = W, K
+                        continue
+                    assert K == ref_k, (sub, cl, lanes)
+                    err = np.max(np.abs(W - ref_w)) / np.max(np.abs(ref_w))
+                    assert err < 1e-13, (sub, cl, lanes, err)
+    finally:
+        s.close()
+
+
+def test_tuning_validation(solver):
+    import brdc
+
+    s = brdc.Solver()
+    try:
+        for bad in ({"subtree_levels": 5}, {"deflate_cluster": 3}, {"sweep_lanes_target": 10}):
+            with pytest.raises(brdc.BrdcError):
+                s.set_tuning(**bad)
+        s.set_tuning(subtree_levels=2, deflate_cluster=4, sweep_lanes_target=50000)
+        assert s.tuning() == {"subtree_levels": 2, "deflate_cluster": 4, "sweep_lanes_target": 50000}
+    finally:
+        s.close()
