@@ -247,6 +247,9 @@ def main():
     ws = solver.workspace(N_HEAD)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
 
+    # the library's autotuner picks the launch shapes for this input
+    # (outside the timed region); the line reports its choice
+    tuning = solver.autotune(D, E, workspace=ws)
     for _ in range(args.warmup):
         solver.dstebr(D, E, W=W, workspace=ws)
     torch.cuda.synchronize()
@@ -292,6 +295,7 @@ def main():
                 "n": N_HEAD, "family": FAMILY_HEAD,
                 "l2": "flushed by a 256 MiB write before every timed solve (outside the timed interval)",
                 "parallelism": f"replicas x{world}",
+                "tuning": tuning,
             },
             "solves_per_s": world * 1000.0 / ms,
             "info": info,
@@ -314,6 +318,7 @@ def main():
 
 def collect_extras(torch, brdc, families, solver, D, E, W, ws, d, e, flush, args):
     out = {}
+    headline_tuning = solver.tuning()
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
 
@@ -351,10 +356,12 @@ def collect_extras(torch, brdc, families, solver, D, E, W, ws, d, e, flush, args
 
     # other families at the same order
     fam_ms = {}
+    fam_tuning = {}
     for fam in ("normal", "toeplitz", "clustered"):
         dd, ee = families.generate(fam, N_HEAD)
         Df = torch.tensor(dd, device="cuda")
         Ef = torch.tensor(ee, device="cuda")
+        fam_tuning[fam] = solver.autotune(Df, Ef, workspace=ws)
         solver.dstebr(Df, Ef, W=W, workspace=ws)
         torch.cuda.synchronize()
         tt = time_solves(torch, solver, Df, Ef, W, ws, 3, flush)
@@ -365,6 +372,8 @@ def collect_extras(torch, brdc, families, solver, D, E, W, ws, d, e, flush, args
             dg = solver.diagnostics(N_HEAD, ws)
             out["toeplitz_roofline"] = roofline(dg, None, N_HEAD, total_ms=fam_ms[fam])
     out["family_ms"] = fam_ms
+    out["family_tuning"] = fam_tuning
+    solver.set_tuning(**headline_tuning)
 
     # e2e through the C ABI with pinned host buffers
     hD = torch.tensor(d).pin_memory()
@@ -477,6 +486,7 @@ def bench_batched(torch, brdc, families, solver, flush):
     stream.wait_stream(torch.cuda.current_stream())
     with torch.cuda.stream(stream):
         solver.set_stream(stream)
+        tuning = solver.autotune(Dt, Et, offsets=off, workspace=ws)
         solver.dstebr_batched(off, Dt, Et, W=W, workspace=ws)  # uploads the forest tables
         stream.synchronize()
         g = torch.cuda.CUDAGraph()
@@ -492,7 +502,9 @@ def bench_batched(torch, brdc, families, solver, flush):
     Wb = W.cpu().numpy()
     del g
 
-    # the plain entry looped over the instances, one shared workspace
+    # the plain entry looped over the instances, one shared workspace, with
+    # the library's default launch shapes
+    solver.set_tuning(subtree_levels=-1, deflate_cluster=8, sweep_lanes_target=75776)
     nmax = int(np.max(orders))
     ws1 = solver.workspace(nmax)
     W1 = torch.empty_like(W)
@@ -517,6 +529,7 @@ def bench_batched(torch, brdc, families, solver, flush):
         ref = scipy.linalg.eigvalsh_tridiagonal(D[lo:hi], E[lo:hi - 1])
         errs.append(float(np.max(np.abs(Wb[lo:hi] - ref)) / np.max(np.abs(ref))))
     return {"count": count, "orders": "log-uniform [32, 8192]", "rows": int(off[-1]),
+            "tuning": tuning,
             "families": "uniform, normal, toeplitz, clustered in turn",
             "graph_ms": t_graph, "eager_batched_ms": t_eager, "looped_plain_ms": t_loop,
             "solves_per_s": count * 1e3 / t_graph,
@@ -565,6 +578,8 @@ def bench_fit(torch, brdc, families, flush, steps=200, lr=0.1):
         gE = torch.empty_like(W)
         hist = torch.zeros(steps + 1, dtype=torch.float64, device="cuda")
         ws = s.batched_workspace(off, checkpoints=True)
+        tuning = s.autotune(Dt, Et, offsets=off, workspace=ws)
+        Dt.copy_(D0)
 
         def step(i):
             s.dstebr_batched(off, Dt, Et, W=W, workspace=ws)
@@ -601,6 +616,7 @@ def bench_fit(torch, brdc, families, flush, steps=200, lr=0.1):
     del g
     s.close()
     return {"count": count, "orders": "log-uniform [64, 4096]", "rows": tot, "steps": steps,
+            "tuning": tuning,
             "lr": lr, "graph_ms_total": t_graph, "ms_per_step_graph": t_graph / steps,
             "ms_per_step_eager": t_eager, "loss_first": float(h[0]), "loss_last": float(h[steps]),
             "loss_at": {str(k): float(h[k]) for k in (1, 10, 50, 100, 199)},

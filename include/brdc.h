@@ -199,14 +199,16 @@ typedef struct brdc_timings {
  * beyond rounding: deflation decisions, roots and ordering follow the
  * same rules under every setting.  No reference counterpart (the
  * prototype's shapes are compile-time constants).
- *   subtree_levels      merge levels solved inside the per-subtree kernel,
- *                       with its leaves, in shared memory (0..4; 0 runs the
- *                       leaves alone and every level with per-level kernels)
+ *   subtree_levels      merge levels solved inside the per-subtree kernel (-1: auto),
+ *                       with its leaves, in shared memory (0..5; 0 runs the
+ *                       leaves alone and every level with per-level kernels;
+ *                       up to 4 levels a CTA holds 256 rows, 5 levels 512)
  *   deflate_cluster     largest thread-block cluster that deflates one big
  *                       merge (1, 2, 4 or 8; 1 = one CTA per merge)
  *   sweep_lanes_target  threads the per-level root sweeps aim to keep busy
  *                       (lanes per root = smallest power of two reaching it)
- * brdc_autotune (below) picks them by timing; defaults: 4, 8, 75776. */
+ * brdc_autotune picks them by timing; defaults: subtree_levels = -1 (by
+ * tree height: 3 up to n = 16384, 4 up to 32768, 5 above), 8, 75776. */
 typedef struct brdc_tuning {
     int subtree_levels;
     int deflate_cluster;
@@ -215,6 +217,18 @@ typedef struct brdc_tuning {
 
 brdc_status brdc_set_tuning(brdc_handle handle, const brdc_tuning *tuning);
 brdc_status brdc_get_tuning(brdc_handle handle, brdc_tuning *tuning);
+
+/* Autotuner: times the batched solve of this exact input (count = 1 is the
+ * plain solve) under candidate tunings on the handle's stream -- coordinate
+ * descent over subtree depth, deflation cluster and sweep lanes, median of
+ * three runs each (one for solves above 50 ms) -- then leaves the fastest
+ * on the handle and copies it to *best (may be NULL).  Uses the caller's
+ * workspace, sized as for brdc_dstebr_batched; allocates no device memory;
+ * synchronizes the stream, so it cannot be captured.  W receives the
+ * eigenvalues.  No reference counterpart. */
+brdc_status brdc_autotune(brdc_handle handle, int64_t count, const int64_t *offsets,
+                          const double *d_D, const double *d_E, double *d_W,
+                          void *workspace, size_t workspace_size, brdc_tuning *best);
 
 brdc_status brdc_set_timing(brdc_handle handle, int enable);
 brdc_status brdc_get_last_timings(brdc_handle handle, brdc_timings *out);

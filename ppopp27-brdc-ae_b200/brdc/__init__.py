@@ -67,6 +67,7 @@ EXPORTS = (
     "brdc_dstebr_batched_backward",
     "brdc_set_tuning",
     "brdc_get_tuning",
+    "brdc_autotune",
 )
 
 
@@ -189,13 +190,15 @@ def load() -> ctypes.CDLL:
     lib.brdc_get_last_timings.argtypes = [vp, ctypes.POINTER(Timings)]
     lib.brdc_set_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
     lib.brdc_get_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
+    lib.brdc_autotune.argtypes = [vp, i64, ctypes.POINTER(i64), vp, vp, vp, vp, sz,
+                                  ctypes.POINTER(Tuning)]
     for f in ("brdc_create", "brdc_destroy", "brdc_set_stream", "brdc_get_stream",
               "brdc_get_last_error", "brdc_dstebr_workspace_size", "brdc_dstebr",
               "brdc_dstebr_backward", "brdc_get_info", "brdc_get_diagnostics",
               "brdc_dstebr_batched_workspace_size", "brdc_dstebr_batched",
               "brdc_set_timing", "brdc_get_last_timings", "brdc_dstebr_noalloc",
               "brdc_dstebr_batched_checkpoint_workspace_size", "brdc_dstebr_batched_backward",
-              "brdc_set_tuning", "brdc_get_tuning"):
+              "brdc_set_tuning", "brdc_get_tuning", "brdc_autotune"):
         getattr(lib, f).restype = ctypes.c_int
     _lib = lib
     return lib
@@ -279,6 +282,29 @@ class Solver:
         cur.update(kw)
         t = Tuning(**cur)
         _check(load().brdc_set_tuning(self.h, ctypes.byref(t)), "set_tuning", self.h)
+
+    def autotune(self, D, E, offsets=None, workspace=None) -> dict:
+        """Time this input (one matrix, or a packed batch with offsets) under
+        candidate launch shapes and keep the fastest on the handle."""
+        torch = self._torch
+        n = D.shape[0]
+        off = np.ascontiguousarray(np.asarray([0, n] if offsets is None else offsets,
+                                              dtype=np.int64))
+        if offsets is None:
+            ws = self.workspace(n) if workspace is None else workspace
+            Ep = E.contiguous() if E is not None and E.numel() > 0 else D
+        else:
+            ws = self.batched_workspace(off) if workspace is None else workspace
+            Ep = E.contiguous()
+        W = torch.empty(int(off[-1]), dtype=torch.float64, device=D.device)
+        t = Tuning()
+        st = load().brdc_autotune(
+            self.h, len(off) - 1, off.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+            ctypes.c_void_p(D.contiguous().data_ptr()), ctypes.c_void_p(Ep.data_ptr()),
+            ctypes.c_void_p(W.data_ptr()), ctypes.c_void_p(ws.data_ptr()), ws.numel(),
+            ctypes.byref(t))
+        _check(st, "brdc_autotune", self.h)
+        return t.as_dict()
 
     def set_timing(self, enable: bool) -> None:
         _check(load().brdc_set_timing(self.h, 1 if enable else 0), "set_timing", self.h)

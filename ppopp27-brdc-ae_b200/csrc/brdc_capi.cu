@@ -35,8 +35,9 @@ struct brdc_handle_struct {
     const void *prep_ws;
     bool prep_ckpt = false;
     int prep_sub = -1;
-    // merge levels solved inside the subtree kernel (0: leaves alone)
-    int sub_levels = kSubMaxLevels;
+    // merge levels solved inside the subtree kernel (0: leaves alone,
+    // -1: chosen per solve from the tree height)
+    int sub_levels = -1;
     int defl_cluster = 8;         // largest deflation cluster
     int lanes_target = 75776;     // root-sweep parallelism target
     std::vector<long long> prep_off;
@@ -388,8 +389,12 @@ cudaError_t set_attrs() {
                                  (int)smem_tiles(4));
     }
     if (e == cudaSuccess) {
-        e = cudaFuncSetAttribute(k_subtree, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)sizeof(SubSmem));
+        e = cudaFuncSetAttribute(k_subtree<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(SubSmem<256>));
+    }
+    if (e == cudaSuccess) {
+        e = cudaFuncSetAttribute(k_subtree<512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(SubSmem<512>));
     }
     g_attr_done = (e == cudaSuccess);
     return e;
@@ -402,6 +407,16 @@ void mark(brdc_handle h, int slot) {
         cudaEventRecord(h->ev[slot], h->stream);
         h->ev_used = std::max(h->ev_used, slot + 1);
     }
+}
+
+// Subtree depth of a solve: the handle's setting, or by default the depth
+// measured fastest for uniform spectra on B200 for the forest's tallest
+// instance (3 up to 10 levels, i.e. n <= 16384; 4 at 11; 5 above).
+int effective_sub_levels(brdc_handle h, const HostForest &hf) {
+    if (h->sub_levels >= 0) {
+        return h->sub_levels;
+    }
+    return hf.max_levels <= 10 ? 3 : (hf.max_levels == 11 ? 4 : 5);
 }
 
 // Enqueue the whole forward solve.
@@ -427,8 +442,9 @@ brdc_status run_forest(brdc_handle h, const HostForest &hf, const Layout &L,
     a.W = W;
     a.lanes_target = h->lanes_target;
     // leaves and the lowest merge levels
-    const int fused = std::min(h->sub_levels, hf.max_levels);
-    if (h->sub_levels > 0) {
+    const int sub = effective_sub_levels(h, hf);
+    const int fused = std::min(sub, hf.max_levels);
+    if (sub > 0) {
         SubArgs A{};
         A.a = a;
         for (int k = 0; k < fused; ++k) {
@@ -440,13 +456,17 @@ brdc_status run_forest(brdc_handle h, const HostForest &hf, const Layout &L,
         A.out_d = (fused & 1) ? w.nd : w.cd;
         A.out_f = (fused & 1) ? w.nf : w.cf;
         A.out_l = (fused & 1) ? w.nl : w.cl;
-        A.levels = h->sub_levels;
+        A.levels = sub;
         A.ckpt = L.ckpt ? 1 : 0;
         long long subs = 0;
         for (int b = 0; b < hf.B; ++b) {
-            subs += subtrees_of(hf.lev[b], h->sub_levels);
+            subs += subtrees_of(hf.lev[b], sub);
         }
-        k_subtree<<<(unsigned)subs, kSubRows, sizeof(SubSmem), s>>>(A);
+        if (sub_rows_for(sub) == 256) {
+            k_subtree<256><<<(unsigned)subs, 256, sizeof(SubSmem<256>), s>>>(A);
+        } else {
+            k_subtree<512><<<(unsigned)subs, 512, sizeof(SubSmem<512>), s>>>(A);
+        }
         BRDC_CUDA(h, "brdc.subtree", cudaGetLastError());
         ++h->launches;
         mark(h, 2);
@@ -487,7 +507,7 @@ brdc_status run_forest(brdc_handle h, const HostForest &hf, const Layout &L,
     const int warp_blocks = h->sm_count * 2;
     long long elem_grid = (hf.total_n + 255) / 256;
     elem_grid = std::max<long long>(1, std::min<long long>(elem_grid, (long long)h->sm_count * 8));
-    for (int k = (h->sub_levels > 0 ? fused : 0); k < hf.max_levels; ++k) {
+    for (int k = (sub > 0 ? fused : 0); k < hf.max_levels; ++k) {
         a.k = k;
         a.nodes = hf.level_nodes[k];
         a.level_rows = hf.level_rows[k];
@@ -588,7 +608,7 @@ extern "C" brdc_status brdc_set_tuning(brdc_handle h, const brdc_tuning *t) {
         return BRDC_STATUS_INVALID_POINTER;
     }
     const int c = t->deflate_cluster;
-    if (t->subtree_levels < 0 || t->subtree_levels > kSubMaxLevels ||
+    if (t->subtree_levels < -1 || t->subtree_levels > kSubMaxLevels ||
         !(c == 1 || c == 2 || c == 4 || c == 8) || t->sweep_lanes_target < 1024 ||
         t->sweep_lanes_target > (1 << 24)) {
         return BRDC_STATUS_INVALID_VALUE;
@@ -842,7 +862,7 @@ brdc_status prepare_forest(brdc_handle h, const HostForest &hf, const Ws &w,
         return BRDC_STATUS_SUCCESS;
     }
     const bool same = h->prep_ws == workspace && h->prep_ckpt == ckpt &&
-                      h->prep_sub == h->sub_levels &&
+                      h->prep_sub == effective_sub_levels(h, hf) &&
                       h->prep_off.size() == (size_t)hf.B + 1 &&
                       std::equal(h->prep_off.begin(), h->prep_off.end(), hf.off.begin());
     if (!same) {
@@ -859,7 +879,7 @@ brdc_status prepare_forest(brdc_handle h, const HostForest &hf, const Ws &w,
         std::vector<int> sub_prefix(hf.B + 1, 0);
         for (int b = 0; b < hf.B; ++b) {
             leaf_prefix[b + 1] = leaf_prefix[b] + (1 << hf.lev[b]);
-            sub_prefix[b + 1] = sub_prefix[b] + (int)subtrees_of(hf.lev[b], h->sub_levels);
+            sub_prefix[b + 1] = sub_prefix[b] + (int)subtrees_of(hf.lev[b], effective_sub_levels(h, hf));
         }
         BRDC_CUDA(h, "brdc.batched.upload_off",
                   cudaMemcpyAsync(w.f_off, hf.off.data(), sizeof(long long) * (hf.B + 1),
@@ -882,7 +902,7 @@ brdc_status prepare_forest(brdc_handle h, const HostForest &hf, const Ws &w,
         BRDC_CUDA(h, "brdc.batched.upload_sync", cudaStreamSynchronize(h->stream));
         h->prep_ws = workspace;
         h->prep_ckpt = ckpt;
-        h->prep_sub = h->sub_levels;
+        h->prep_sub = effective_sub_levels(h, hf);
         h->prep_off = hf.off;
     }
     F->off = w.f_off;
@@ -968,6 +988,107 @@ extern "C" brdc_status brdc_dstebr_batched(brdc_handle h, int64_t count,
         return st;
     }
     return run_forest(h, hf, L, F, w, d_D, d_E, d_W);
+}
+
+// ------------------------------------------------------------- autotuner
+
+extern "C" brdc_status brdc_autotune(brdc_handle h, int64_t count, const int64_t *offsets,
+                                     const double *d_D, const double *d_E, double *d_W,
+                                     void *workspace, size_t workspace_size,
+                                     brdc_tuning *best) {
+    if (h == nullptr) {
+        return BRDC_STATUS_INVALID_HANDLE;
+    }
+    HostForest hf;
+    brdc_status st = batch_forest(count, offsets, &hf);
+    if (st != BRDC_STATUS_SUCCESS) {
+        return st;
+    }
+    cudaEvent_t e0, e1;
+    BRDC_CUDA(h, "brdc.autotune.event", cudaEventCreate(&e0));
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        set_error(h, (int)cudaErrorMemoryAllocation, BRDC_ERROR_SRC_CUDA, "brdc.autotune.event");
+        return BRDC_STATUS_CUDA_ERROR;
+    }
+    const brdc_tuning saved{h->sub_levels, h->defl_cluster, h->lanes_target};
+    brdc_tuning cur{effective_sub_levels(h, hf), h->defl_cluster, h->lanes_target};
+    int reps = 3;
+    // median device time of a few solves under tuning t (first call warms
+    // up and, for a new subtree depth, uploads the batch tables)
+    auto run = [&](const brdc_tuning &t, float *ms) -> brdc_status {
+        h->sub_levels = t.subtree_levels;
+        h->defl_cluster = t.deflate_cluster;
+        h->lanes_target = t.sweep_lanes_target;
+        brdc_status r = brdc_dstebr_batched(h, count, offsets, d_D, d_E, d_W, workspace,
+                                            workspace_size);
+        if (r != BRDC_STATUS_SUCCESS) {
+            return r;
+        }
+        float v[5];
+        for (int i = 0; i < reps; ++i) {
+            cudaEventRecord(e0, h->stream);
+            r = brdc_dstebr_batched(h, count, offsets, d_D, d_E, d_W, workspace, workspace_size);
+            cudaEventRecord(e1, h->stream);
+            if (r != BRDC_STATUS_SUCCESS) {
+                return r;
+            }
+            BRDC_CUDA(h, "brdc.autotune.sync", cudaEventSynchronize(e1));
+            cudaEventElapsedTime(&v[i], e0, e1);
+        }
+        std::sort(v, v + reps);
+        *ms = v[reps / 2];
+        return BRDC_STATUS_SUCCESS;
+    };
+    float best_ms = 0.0f;
+    st = run(cur, &best_ms);
+    if (st == BRDC_STATUS_SUCCESS && best_ms > 50.0f) {
+        reps = 1; // long solves: one timed run per candidate
+    }
+    // coordinate descent: subtree depth, deflation cluster, sweep lanes
+    const int subs[] = {0, 1, 2, 3, 4, 5};
+    const int clusters[] = {1, 2, 4, 8};
+    const int lanes[] = {18944, 37888, 75776, 151552, 303104};
+    for (int pass = 0; pass < 3 && st == BRDC_STATUS_SUCCESS; ++pass) {
+        const int *vals = pass == 0 ? subs : (pass == 1 ? clusters : lanes);
+        const int nv = pass == 0 ? 6 : (pass == 1 ? 4 : 5);
+        if (pass == 1 && *std::max_element(hf.level_mmax.begin(), hf.level_mmax.end()) <
+                             2 * kDeflEPT * 1024) {
+            continue; // no merge is large enough for a cluster
+        }
+        brdc_tuning pick = cur;
+        for (int i = 0; i < nv && st == BRDC_STATUS_SUCCESS; ++i) {
+            brdc_tuning t = cur;
+            int *field = pass == 0 ? &t.subtree_levels
+                                   : (pass == 1 ? &t.deflate_cluster : &t.sweep_lanes_target);
+            if (*field == vals[i]) {
+                continue;
+            }
+            *field = vals[i];
+            float ms = 0.0f;
+            st = run(t, &ms);
+            if (st == BRDC_STATUS_SUCCESS && ms < best_ms) {
+                best_ms = ms;
+                pick = t;
+            }
+        }
+        cur = pick;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st != BRDC_STATUS_SUCCESS) {
+        h->sub_levels = saved.subtree_levels;
+        h->defl_cluster = saved.deflate_cluster;
+        h->lanes_target = saved.sweep_lanes_target;
+        return st;
+    }
+    h->sub_levels = cur.subtree_levels;
+    h->defl_cluster = cur.deflate_cluster;
+    h->lanes_target = cur.sweep_lanes_target;
+    if (best != nullptr) {
+        *best = cur;
+    }
+    return BRDC_STATUS_SUCCESS;
 }
 
 // -------------------------------------------------------------- backward

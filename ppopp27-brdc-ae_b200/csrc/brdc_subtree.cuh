@@ -22,9 +22,11 @@
 
 namespace brdc {
 
-constexpr int kSubRows = 256;   // rows (and threads) of a subtree CTA
-constexpr int kSubMaxLevels = 4; // merge levels a subtree can hold (leaves <= 16 rows)
-constexpr int kSubWarps = kSubRows / 32;
+constexpr int kSubMaxLevels = 5; // merge levels a subtree can hold (leaves <= 16 rows)
+
+// Rows (and threads) of a subtree CTA holding `levels` merge levels: a node
+// of level k spans at most 2^(k+1) leaves of at most 16 rows.
+constexpr int sub_rows_for(int levels) { return levels <= 4 ? 256 : 512; }
 
 struct SubArgs {
     KArgs a;                  // forest, workspace, D, E, W, diagnostics
@@ -34,7 +36,9 @@ struct SubArgs {
     int ckpt;                 // write each fused level's state for the adjoint
 };
 
+template <int kSubRows>
 struct SubSmem {
+    static constexpr int kSubWarps = kSubRows / 32;
     double cd[kSubRows], cf[kSubRows], cl[kSubRows];   // children (sorted) / placed output
     double md[kSubRows], mz[kSubRows], mf[kSubRows], ml[kSubRows];
     double ad[kSubRows], az[kSubRows], af[kSubRows], al[kSubRows];
@@ -53,7 +57,8 @@ struct SubSmem {
 };
 
 // Exclusive scan of one int per thread over the CTA; ex[kSubRows] = total.
-__device__ inline void sub_scan(SubSmem &S, int v) {
+template <int kSubRows>
+__device__ inline void sub_scan(SubSmem<kSubRows> &S, int v) {
     int tot;
     const int e = block_exscan<kSubRows>(v, S.scan, &tot);
     S.ex[threadIdx.x] = e;
@@ -66,8 +71,10 @@ __device__ inline void sub_scan(SubSmem &S, int v) {
 // Per-node reduction (sum or max) of one value per row, in a fixed order:
 // warp partials per node, then the warps in order.  j = node of the row
 // (-1 for none); returns the node's result to threads j < nk via *out.
-template <bool MAX>
-__device__ inline void sub_node_reduce(SubSmem &S, double v, int j, int nk, double *out) {
+template <bool MAX, int kSubRows>
+__device__ inline void sub_node_reduce(SubSmem<kSubRows> &S, double v, int j, int nk,
+                                       double *out) {
+    constexpr int kSubWarps = kSubRows / 32;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int q = threadIdx.x; q < kSubWarps * (kSubRows / 16); q += kSubRows) {
         (&S.part[0][0])[q] = 0.0;
@@ -101,7 +108,8 @@ __device__ inline void sub_node_reduce(SubSmem &S, double v, int j, int nk, doub
     __syncthreads();
 }
 
-__device__ inline int sub_node_of(const SubSmem &S, int nk, int x) {
+template <int kSubRows>
+__device__ inline int sub_node_of(const SubSmem<kSubRows> &S, int nk, int x) {
     for (int j = 0; j < nk; ++j) {
         if (x < S.nstart[j] + S.nsize[j]) {
             return x >= S.nstart[j] ? j : -1;
@@ -110,9 +118,11 @@ __device__ inline int sub_node_of(const SubSmem &S, int nk, int x) {
     return -1;
 }
 
-__global__ void __launch_bounds__(kSubRows, 2) k_subtree(SubArgs A) {
+template <int kSubRows>
+__global__ void __launch_bounds__(kSubRows, 512 / kSubRows) k_subtree(SubArgs A) {
+    constexpr int kSubWarps = kSubRows / 32;
     extern __shared__ __align__(16) unsigned char sub_raw[];
-    SubSmem &S = *reinterpret_cast<SubSmem *>(sub_raw);
+    SubSmem<kSubRows> &S = *reinterpret_cast<SubSmem<kSubRows> *>(sub_raw);
     const KArgs &a = A.a;
     const Forest &F = a.F;
     const int x = threadIdx.x;
@@ -238,7 +248,7 @@ __global__ void __launch_bounds__(kSubRows, 2) k_subtree(SubArgs A) {
         // tolerance
         {
             double mzx = 0.0;
-            sub_node_reduce<true>(S, j >= 0 ? fabs(S.mz[x]) : 0.0, j, nk, &mzx);
+            sub_node_reduce<true, kSubRows>(S, j >= 0 ? fabs(S.mz[x]) : 0.0, j, nk, &mzx);
             if (x < nk) {
                 S.ntol[x] = kDeflTolScale * eps * fmax(S.nmaxd[x], mzx);
             }
@@ -354,7 +364,7 @@ __global__ void __launch_bounds__(kSubRows, 2) k_subtree(SubArgs A) {
         }
         {
             double zsum = 0.0;
-            sub_node_reduce<false>(S, pole ? S.az[x] * S.az[x] : 0.0, j, nk, &zsum);
+            sub_node_reduce<false, kSubRows>(S, pole ? S.az[x] * S.az[x] : 0.0, j, nk, &zsum);
             if (x < nk) {
                 S.nK[x] = S.ex[S.nstart[x] + S.nsize[x]] - S.ex[S.nstart[x]];
                 S.nzn[x] = zsum;

@@ -136,7 +136,7 @@ def test_batched_tunings_agree(solver):
     s = brdc.Solver()
     try:
         res = []
-        for sub in (0, 2, 4):
+        for sub in (0, 2, 4, 5):
             s.set_tuning(subtree_levels=sub)
             res.append(s.dstebr_batched(off, Dt, Et).cpu().numpy())
         for r in res[1:]:

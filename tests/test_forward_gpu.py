@@ -136,7 +136,7 @@ def test_tunings_agree(solver, family, n):
     s = brdc.Solver()
     ref_w, ref_k = None, None
     try:
-        for sub in (0, 1, 2, 3, 4):
+        for sub in (-1, 0, 1, 2, 3, 4, 5):
             for cl in (1, 8):
                 for lanes in (8192, 75776, 1 << 20):
                     s.set_tuning(subtree_levels=sub, deflate_cluster=cl, sweep_lanes_target=lanes)
@@ -158,10 +158,44 @@ def test_tuning_validation(solver):
 
     s = brdc.Solver()
     try:
-        for bad in ({"subtree_levels": 5}, {"deflate_cluster": 3}, {"sweep_lanes_target": 10}):
+        for bad in ({"subtree_levels": 6}, {"deflate_cluster": 3}, {"sweep_lanes_target": 10}):
             with pytest.raises(brdc.BrdcError):
                 s.set_tuning(**bad)
         s.set_tuning(subtree_levels=2, deflate_cluster=4, sweep_lanes_target=50000)
         assert s.tuning() == {"subtree_levels": 2, "deflate_cluster": 4, "sweep_lanes_target": 50000}
+    finally:
+        s.close()
+
+
+def test_autotune_single_and_batched(solver):
+    """The autotuner leaves a valid tuning on the handle, and solves under it
+    stay correct."""
+    import torch
+
+    import brdc
+
+    s = brdc.Solver()
+    try:
+        n = 20000
+        d, e = families.generate("normal", n)
+        D = torch.tensor(d, device="cuda")
+        E = torch.tensor(e, device="cuda")
+        t = s.autotune(D, E)
+        assert t == s.tuning()
+        assert -1 <= t["subtree_levels"] <= 5 and t["deflate_cluster"] in (1, 2, 4, 8)
+        W = s.dstebr(D, E).cpu().numpy()
+        ref = oracle.dstedc_dc_br(d, e)
+        assert np.max(np.abs(W - ref)) / np.max(np.abs(ref)) < 1e-12
+
+        off, Db, Eb, orders, _ = families.batch(40, 17, 2500, seed=8)
+        Dt = torch.tensor(Db, device="cuda")
+        Et = torch.tensor(Eb, device="cuda")
+        tb = s.autotune(Dt, Et, offsets=off)
+        assert tb == s.tuning()
+        Wb = s.dstebr_batched(off, Dt, Et).cpu().numpy()
+        for b in range(len(orders)):
+            lo, hi = int(off[b]), int(off[b + 1])
+            ref = oracle.dstedc_dc_br(Db[lo:hi], Eb[lo:hi - 1])
+            assert np.max(np.abs(Wb[lo:hi] - ref)) / np.max(np.abs(ref)) < 1e-12
     finally:
         s.close()
