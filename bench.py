@@ -316,17 +316,54 @@ def main():
         dist.destroy_process_group()
 
 
+def dsterf(d, e):
+    """LAPACK DSTERF eigenvalues (scipy's bundled LAPACK), ascending."""
+    import scipy.linalg.lapack as la
+
+    w, info = la.dsterf(np.array(d, dtype=np.float64), np.array(e, dtype=np.float64))
+    if info != 0:
+        raise RuntimeError(f"dsterf info {info}")
+    return np.sort(w)
+
+
+def bench_config2(torch, families, solver, flush):
+    """The plain-solve table over orders and families: median ms of 10
+    solves after 3 warm-ups (default launch shapes), eigenvalues/s, max
+    error over ||T|| against LAPACK DSTERF (Toeplitz: its closed form),
+    workspace bytes and the non-deflated pole count per level."""
+    table = []
+    for n in (8192, 16384, 32768, 49152, 65536):
+        ws = solver.workspace(n)
+        W = torch.empty(n, dtype=torch.float64, device="cuda")
+        for fam in ("uniform", "normal", "toeplitz", "clustered"):
+            d, e = families.generate(fam, n)
+            Dt = torch.tensor(d, device="cuda")
+            Et = torch.tensor(e, device="cuda")
+            for _ in range(3):
+                solver.dstebr(Dt, Et, W=W, workspace=ws)
+            torch.cuda.synchronize()
+            tt = time_solves(torch, solver, Dt, Et, W, ws, 10, flush)
+            ms = float(np.median(tt))
+            w = W.cpu().numpy()
+            ref = families.toeplitz_eigenvalues(n) if fam == "toeplitz" else dsterf(d, e)
+            err = float(np.max(np.abs(w - ref)) / np.max(np.abs(ref)))
+            dg = solver.diagnostics(n, ws)
+            table.append({"n": n, "family": fam, "ms": ms, "eigenvalues_per_s": n * 1e3 / ms,
+                          "max_err_over_normT": err, "workspace_bytes": ws.numel(),
+                          "K_per_level": [lv["dd_after_sum"] for lv in dg["level"]]})
+        solver._ws.clear()
+    return table
+
+
 def collect_extras(torch, brdc, families, solver, D, E, W, ws, d, e, flush, args):
     out = {}
     headline_tuning = solver.tuning()
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
 
-    # accuracy of the headline solve
+    # accuracy of the headline solve against LAPACK DSTERF
     solver.dstebr(D, E, W=W, workspace=ws)
     w = W.cpu().numpy()
-    ref = oracle.dstedc_dc_br(d, e)
-    out["max_err_vs_oracle"] = float(np.max(np.abs(w - ref)) / np.max(np.abs(ref)))
+    ref = dsterf(d, e)
+    out["max_err_vs_dsterf"] = float(np.max(np.abs(w - ref)) / np.max(np.abs(ref)))
 
     # per-phase timings and roofline of the dominant kernel
     solver.set_timing(True)
@@ -352,7 +389,8 @@ def collect_extras(torch, brdc, families, solver, D, E, W, ws, d, e, flush, args
     out["launches"] = launches
     out["phase_ms"] = acc
     diag = solver.diagnostics(N_HEAD, ws)
-    out["roofline"] = roofline(diag, acc, N_HEAD)
+    fused = t["fused_levels"]
+    out["roofline"] = roofline(diag, acc, N_HEAD, fused=fused)
 
     # other families at the same order
     fam_ms = {}
@@ -370,7 +408,8 @@ def collect_extras(torch, brdc, families, solver, D, E, W, ws, d, e, flush, args
             err = np.max(np.abs(W.cpu().numpy() - families.toeplitz_eigenvalues(N_HEAD))) / 4.0
             out["toeplitz_max_err_vs_closed_form"] = float(err)
             dg = solver.diagnostics(N_HEAD, ws)
-            out["toeplitz_roofline"] = roofline(dg, None, N_HEAD, total_ms=fam_ms[fam])
+            out["toeplitz_roofline"] = roofline(dg, None, N_HEAD, total_ms=fam_ms[fam],
+                                                fused=fused)
     out["family_ms"] = fam_ms
     out["family_tuning"] = fam_tuning
     solver.set_tuning(**headline_tuning)
@@ -398,11 +437,16 @@ def collect_extras(torch, brdc, families, solver, D, E, W, ws, d, e, flush, args
                   "h2d_bytes_per_step": int(hD.numel() * 8 + hE.numel() * 8),
                   "d2h_bytes_per_step": int(hW.numel() * 8)}
 
+    default = {"subtree_levels": -1, "deflate_cluster": 8, "sweep_lanes_target": 75776}
+    solver.set_tuning(**default)
+    out["config2"] = bench_config2(torch, families, solver, flush)
+    solver.set_tuning(**headline_tuning)
     out["fwd_bwd"] = bench_fwd_bwd(torch, families, solver, flush, args)
     out["batched"] = bench_batched(torch, brdc, families, solver, flush)
     out["fit"] = bench_fit(torch, brdc, families, flush)
 
     # CPU baseline: the oracle on a bounded sample of the same workload
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
     cpu_t, threads = cpu_reference_times(d, e, args.cpu_budget)
     out["cpu_baseline"] = {"value": float(np.median(cpu_t)), "unit": "ms", "cores": threads,
                            "kind": "port",
@@ -618,49 +662,91 @@ def bench_fit(torch, brdc, families, flush, steps=200, lr=0.1):
     return {"count": count, "orders": "log-uniform [64, 4096]", "rows": tot, "steps": steps,
             "tuning": tuning,
             "lr": lr, "graph_ms_total": t_graph, "ms_per_step_graph": t_graph / steps,
-            "ms_per_step_eager": t_eager, "loss_first": float(h[0]), "loss_last": float(h[steps]),
+            "ms_per_step_eager": t_eager, "steps_per_s": steps * 1e3 / t_graph,
+            "optimizer": "SGD", "loss_first": float(h[0]), "loss_last": float(h[steps]),
             "loss_at": {str(k): float(h[k]) for k in (1, 10, 50, 100, 199)},
             "checkpoint_workspace_bytes": ws.numel()}
 
 
-def roofline(diag, phase, n, total_ms=None):
-    """Roofline of the dominant phase.  FP64 phases count, per pole-root
-    pair: secular 32 flops (4 nominal sweeps x 8), Loewner 3, rows 9; the
-    merge phase moves 68 bytes per row per level."""
+def work_model(diag, fused):
+    """Algorithmic FP64 work of the solve from the solver's own counters
+    (a divide or square root counts as one flop, an FMA as two):
+      leaf Jacobi     (12 s + 15) flops per rotation, s(s-1)/2 rotations a
+                      sweep, at the largest sweep count any leaf took
+      secular         8 flops per pole-root pair and sweep; sweeps per root
+                      = its iterations + the initial midpoint sweep
+      Loewner         4 flops per pair (inner merges only)
+      boundary rows   10 flops per pair (inner merges only)
+    Returns (flops of the subtree kernel, per-level dict for the rest)."""
+    levels = diag["level"]
+    nlev = len(levels)
+    leaves = diag["leaf_count"]
+    s = 16
+    leaf = leaves * diag["leaf_sweeps_max"] * (s * (s - 1) / 2) * (12 * s + 15)
+    per = []
+    for k, lv in enumerate(levels):
+        kk = max(lv["dd_after_sum"], 1)
+        sweeps = lv["secular_iter_sum"] / kk + 1.0
+        sec = 8.0 * lv["dd_after_sq_sum"] * sweeps
+        inner = k < nlev - 1
+        low = 4.0 * lv["dd_after_sq_sum"] if inner else 0.0
+        rows = 10.0 * lv["dd_after_sq_sum"] if inner else 0.0
+        per.append((sec, low, rows))
+    sub = leaf + sum(a + b + c for a, b, c in per[:fused])
+    return sub, per
+
+
+def roofline(diag, phase, n, total_ms=None, fused=0):
+    """Roofline of the dominant kernel (by measured time): the subtree
+    kernel (leaves and the fused bottom levels) or one of the per-level
+    phases above it, each against the measured FP64 FMA peak (a flop model
+    in work_model), or the deflation against HBM copy bandwidth (68 bytes
+    per row and level: d, z, two rows read and written, an index)."""
     hbm, hbm_kind = measured_peaks()
     levels = diag["level"]
-    k2 = sum(lv["dd_after_sq_sum"] for lv in levels)
-    k2_inner = sum(lv["dd_after_sq_sum"] for lv in levels[:-1])
     fp64_peak = fp64_peak_gflops()
-    res = {"pairs_sum_k2": int(k2)}
+    sub_flops, per = work_model(diag, fused)
+    res = {"pairs_sum_k2": int(sum(lv["dd_after_sq_sum"] for lv in levels))}
     if phase is None:
-        flops = 32.0 * k2 + 12.0 * k2_inner
+        flops = sub_flops + sum(a + b + c for a, b, c in per[fused:])
         ach = flops / (total_ms * 1e-3) / 1e12
         res.update({"bound": "fp64", "kernel": "whole solve", "achieved": ach,
                     "peak": fp64_peak / 1e3, "unit": "TFLOP/s", "frac": ach / (fp64_peak / 1e3),
                     "traffic": None, "peak_kind": "measured (DFMA probe)"})
         return res
+    upper = per[fused:]
+    lv_ms = phase["level_ms"][fused:]
     cand = {
-        "secular": (phase["secular_ms"], 32.0 * k2, "fp64"),
-        "lowner": (phase["lowner_ms"], 3.0 * k2_inner, "fp64"),
-        "rows": (phase["rows_ms"], 9.0 * k2_inner, "fp64"),
-        "merge_deflate": (phase["merge_ms"], 68.0 * n * len(levels), "hbm"),
-        "leaf": (phase["leaf_ms"], 24.0 * n, "hbm"),
+        "k_subtree": (phase["leaf_ms"], sub_flops, "fp64"),
+        "k_secular": (sum(r[1] for r in lv_ms), sum(x[0] for x in upper), "fp64"),
+        "k_lowner": (sum(r[2] for r in lv_ms), sum(x[1] for x in upper), "fp64"),
+        "k_rows+k_place": (sum(r[3] for r in lv_ms), sum(x[2] for x in upper), "fp64"),
+        "k_merge+k_merge_deflate": (sum(r[0] for r in lv_ms), 68.0 * n * len(upper), "hbm"),
     }
     name = max(cand, key=lambda k: cand[k][0])
     ms, work, bound = cand[name]
     if bound == "fp64":
         ach = work / (ms * 1e-3) / 1e12
         res.update({"bound": "fp64", "kernel": name, "achieved": ach, "peak": fp64_peak / 1e3,
-                    "unit": "TFLOP/s", "frac": ach / (fp64_peak / 1e3), "traffic": None,
-                    "peak_kind": "measured (DFMA probe)"})
+                    "unit": "TFLOP/s", "frac": ach / (fp64_peak / 1e3),
+                    "traffic": KERNEL_TRAFFIC.get(name),
+                    "peak_kind": "measured (DFMA probe)", "work_per_launch": work,
+                    "kernel_ms": ms})
     else:
         ach = work / (ms * 1e-3) / 1e9
         res.update({"bound": "hbm", "kernel": name, "achieved": ach, "peak": hbm,
-                    "unit": "GB/s", "frac": ach / hbm, "traffic": None,
-                    "peak_kind": hbm_kind + " copy bandwidth"})
-    res["phase_share"] = {k: v[0] / max(sum(c[0] for c in cand.values()), 1e-9) for k, v in cand.items()}
+                    "unit": "GB/s", "frac": ach / hbm, "traffic": KERNEL_TRAFFIC.get(name),
+                    "peak_kind": hbm_kind + " copy bandwidth", "work_per_launch": work,
+                    "kernel_ms": ms})
+    tot = max(sum(c[0] for c in cand.values()), 1e-9)
+    res["phase_share"] = {k: v[0] / tot for k, v in cand.items()}
     return res
+
+
+# DRAM bytes (read + write) of one launch, from the ncu captures summarised
+# in profiles/ (uniform N=65536): the working set is L2-resident, so DRAM
+# sees little more than the first touch of the inputs.
+KERNEL_TRAFFIC = {"k_subtree": 1222144}
 
 
 _FP64 = None

@@ -185,7 +185,7 @@ brdc_status brdc_get_diagnostics(brdc_handle handle, const void *workspace,
 typedef struct brdc_timings {
     float total_ms;
     float init_ms;
-    float leaf_ms;
+    float leaf_ms;       /* leaves, with the fused_levels solved alongside them */
     float merge_ms;      /* merge + deflation, all levels */
     float secular_ms;    /* secular roots, all levels */
     float lowner_ms;     /* Loewner z, all levels */
@@ -193,6 +193,8 @@ typedef struct brdc_timings {
     int launches;        /* kernels enqueued by the solve */
     int levels;
     float level_ms[BRDC_MAX_LEVELS][4]; /* merge, secular, lowner, rows */
+    int fused_levels;    /* lowest merge levels solved by the subtree kernel
+                            (their level_ms rows are empty) */
 } brdc_timings;
 
 /* Launch-shape parameters of a handle's solves.  None changes a result

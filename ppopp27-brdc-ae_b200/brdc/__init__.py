@@ -138,6 +138,7 @@ class Timings(ctypes.Structure):
         ("launches", ctypes.c_int),
         ("levels", ctypes.c_int),
         ("level_ms", (ctypes.c_float * 4) * MAX_LEVELS),
+        ("fused_levels", ctypes.c_int),
     ]
 
     def as_dict(self) -> dict:

@@ -49,6 +49,7 @@ struct brdc_handle_struct {
     int launches;
     int timed_levels;
     int has_lowner[BRDC_MAX_LEVELS];
+    int fused_levels;
 };
 
 namespace {
@@ -471,11 +472,9 @@ brdc_status run_forest(brdc_handle h, const HostForest &hf, const Layout &L,
         ++h->launches;
         mark(h, 2);
         for (int k = 0; k < fused; ++k) {
-            for (int q = 3; q <= 6; ++q) {
-                mark(h, q + 4 * k);
-            }
             h->has_lowner[k] = 0;
         }
+        h->fused_levels = fused;
         if (L.ckpt) {
             // item tables of the fused levels, which the adjoint's sweeps use
             for (int k = 0; k < fused; ++k) {
@@ -503,6 +502,7 @@ brdc_status run_forest(brdc_handle h, const HostForest &hf, const Layout &L,
         BRDC_CUDA(h, "brdc.leaf", cudaGetLastError());
         ++h->launches;
         mark(h, 2);
+        h->fused_levels = 0;
     }
     const int warp_blocks = h->sm_count * 2;
     long long elem_grid = (hf.total_n + 255) / 256;
@@ -823,8 +823,9 @@ extern "C" brdc_status brdc_get_last_timings(brdc_handle h, brdc_timings *out) {
     out->leaf_ms = el(1, 2);
     out->levels = h->timed_levels;
     out->launches = h->launches;
+    out->fused_levels = h->fused_levels;
     int prev = 2;
-    for (int k = 0; k < h->timed_levels; ++k) {
+    for (int k = h->fused_levels; k < h->timed_levels; ++k) {
         const float m = el(prev, 3 + 4 * k);
         const float s = el(3 + 4 * k, 4 + 4 * k);
         const float l = el(4 + 4 * k, 5 + 4 * k);
