@@ -458,74 +458,95 @@ constexpr int kDeflEPT = 4; // rows per thread per deflation chunk
 // Deflation phases over a range of rows, shared by the one-CTA-per-node
 // kernel (whole node) and the cluster kernel (one slice per CTA).
 
+// Chunks of EPT*T rows: warp w of the CTA takes rows [w*128, w*128+128) of
+// the chunk, lane l rows w*128 + 32q + l (q < EPT), so every load is one
+// coalesced 256-byte row of the warp.  Order is kept by warp ballots: the
+// rank of a row among the chunk's survivors is the survivors of the warps
+// before it (one block scan of the warp totals) plus those of its own warp
+// before it (popcounts of the EPT ballots).
+
+// Exclusive prefix of this warp's count over the CTA's warps, and the total.
+template <int T>
+__device__ inline int defl_warp_prefix(int wcnt, int *iscan, int *total) {
+    const int lane = threadIdx.x & 31;
+    const int ex = block_exscan<T>(lane == 0 ? wcnt : 0, iscan, total);
+    return __shfl_sync(0xffffffffu, ex, 0);
+}
+
 // Rows [r0, r1) of the merged node that survive the small-z test.
 template <int T>
 __device__ int defl_count_active(const Ws &w, long long gs, int r0, int r1, double rho,
                                  double tol, int *iscan) {
-    int cnt = 0;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int wcnt = 0;
     for (int base = r0; base < r1; base += kDeflEPT * T) {
+        const int wbase = base + wid * (kDeflEPT * 32);
 #pragma unroll
         for (int q = 0; q < kDeflEPT; ++q) {
-            const int idx = base + kDeflEPT * threadIdx.x + q;
-            cnt += (idx < r1 && fabs(rho * w.mz[gs + idx]) > tol) ? 1 : 0;
+            const int idx = wbase + 32 * q + lane;
+            const bool f = idx < r1 && fabs(rho * w.mz[gs + idx]) > tol;
+            wcnt += __popc(__ballot_sync(0xffffffffu, f));
         }
     }
     int tot;
-    block_exscan<T>(cnt, iscan, &tot);
+    defl_warp_prefix<T>(wcnt, iscan, &tot);
     return tot;
 }
 
 // Compaction 1 of rows [r0, r1): small-z survivors to the active list from
-// position carry_a, deflated rows to the small-z list from carry_z.  Every
-// value a thread moves is loaded before the scan, so a chunk costs one
-// round trip to L2 instead of one per row.  Returns carry_a plus the
-// survivors.
+// position carry_a, deflated rows to the small-z list from carry_z, both in
+// merged order.  Every value a thread moves is loaded before the scan, so a
+// chunk costs one round trip to L2.  Returns carry_a plus the survivors.
 template <int T>
 __device__ int defl_compact_active(const Ws &w, long long gs, int r0, int r1, double rho,
                                    double tol, int carry_a, int carry_z, int *iscan) {
     constexpr int EPT = kDeflEPT;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
     for (int base = r0; base < r1; base += EPT * T) {
-        int fl[EPT];
+        const int wbase = base + wid * (EPT * 32);
+        bool fl[EPT];
+        unsigned bal[EPT];
         double vd[EPT], vz[EPT], vf[EPT], vl[EPT];
-        int cnt = 0;
+        int wcnt = 0;
 #pragma unroll
         for (int q = 0; q < EPT; ++q) {
-            const int idx = base + EPT * threadIdx.x + q;
+            const int idx = wbase + 32 * q + lane;
             const bool ok = idx < r1;
             const long long src = gs + (ok ? idx : r0);
             vd[q] = w.md[src];
             vz[q] = w.mz[src];
             vf[q] = w.mf[src];
             vl[q] = w.ml[src];
-            fl[q] = ok ? (fabs(rho * vz[q]) > tol) : 0;
-            cnt += fl[q];
+            fl[q] = ok && (fabs(rho * vz[q]) > tol);
+            bal[q] = __ballot_sync(0xffffffffu, fl[q]);
+            wcnt += __popc(bal[q]);
         }
         int tot;
-        const int ex = block_exscan<T>(cnt, iscan, &tot);
-        int ra = carry_a + ex;
-        int rz = carry_z + (EPT * threadIdx.x - ex);
+        const int wpre = defl_warp_prefix<T>(wcnt, iscan, &tot);
+        int before = wpre;
 #pragma unroll
         for (int q = 0; q < EPT; ++q) {
-            const int idx = base + EPT * threadIdx.x + q;
+            const int idx = wbase + 32 * q + lane;
             if (idx < r1) {
+                const int na = before + __popc(bal[q] & lt); // survivors before this row
                 if (fl[q]) {
-                    const long long o = gs + ra;
+                    const long long o = gs + carry_a + na;
                     w.ad[o] = vd[q];
                     w.az[o] = vz[q];
                     w.af[o] = vf[q];
                     w.al[o] = vl[q];
                     w.amap[o] = idx;
                     w.gmark[o] = 0;
-                    ++ra;
                 } else {
-                    const long long o = gs + rz;
+                    const long long o = gs + carry_z + (idx - base) - na;
                     w.zd[o] = vd[q];
                     w.zf[o] = vf[q];
                     w.zl[o] = vl[q];
                     w.zmap[o] = idx;
-                    ++rz;
                 }
             }
+            before += __popc(bal[q]);
         }
         const int valid = (r1 - base) < EPT * T ? (r1 - base) : EPT * T;
         carry_a += tot;
@@ -594,16 +615,19 @@ __device__ void defl_close_walk(const Ws &w, long long gs, int Kz, double tol, i
 // Active entries [r0, r1) that remain poles (not rotated out).
 template <int T>
 __device__ int defl_count_poles(const Ws &w, long long gs, int r0, int r1, int *iscan) {
-    int cnt = 0;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int wcnt = 0;
     for (int base = r0; base < r1; base += kDeflEPT * T) {
+        const int wbase = base + wid * (kDeflEPT * 32);
 #pragma unroll
         for (int q = 0; q < kDeflEPT; ++q) {
-            const int idx = base + kDeflEPT * threadIdx.x + q;
-            cnt += (idx < r1 && w.gmark[gs + idx] == 0) ? 1 : 0;
+            const int idx = wbase + 32 * q + lane;
+            const bool f = idx < r1 && w.gmark[gs + idx] == 0;
+            wcnt += __popc(__ballot_sync(0xffffffffu, f));
         }
     }
     int tot;
-    block_exscan<T>(cnt, iscan, &tot);
+    defl_warp_prefix<T>(wcnt, iscan, &tot);
     return tot;
 }
 
@@ -615,49 +639,53 @@ template <int T>
 __device__ double defl_compact_poles(const Ws &w, long long gs, long long po, int r0, int r1,
                                      int carry_p, int carry_g, int *iscan, int *end_p) {
     constexpr int EPT = kDeflEPT;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
     double zn = 0.0;
     for (int base = r0; base < r1; base += EPT * T) {
-        int fl[EPT];
+        const int wbase = base + wid * (EPT * 32);
+        bool fl[EPT];
+        unsigned bal[EPT];
         double vd[EPT], vz[EPT], vf[EPT], vl[EPT];
-        int cnt = 0;
+        int wcnt = 0;
 #pragma unroll
         for (int q = 0; q < EPT; ++q) {
-            const int idx = base + EPT * threadIdx.x + q;
+            const int idx = wbase + 32 * q + lane;
             const bool ok = idx < r1;
             const long long src = gs + (ok ? idx : r0);
             vd[q] = w.ad[src];
             vz[q] = w.az[src];
             vf[q] = w.af[src];
             vl[q] = w.al[src];
-            fl[q] = ok ? (w.gmark[src] == 0) : 0;
-            cnt += fl[q];
+            fl[q] = ok && (w.gmark[src] == 0);
+            bal[q] = __ballot_sync(0xffffffffu, fl[q]);
+            wcnt += __popc(bal[q]);
         }
         int tot;
-        const int ex = block_exscan<T>(cnt, iscan, &tot);
-        int rp = carry_p + ex;
-        int rg = carry_g + (EPT * threadIdx.x - ex);
+        const int wpre = defl_warp_prefix<T>(wcnt, iscan, &tot);
+        int before = wpre;
 #pragma unroll
         for (int q = 0; q < EPT; ++q) {
-            const int idx = base + EPT * threadIdx.x + q;
+            const int idx = wbase + 32 * q + lane;
             if (idx < r1) {
+                const int np = before + __popc(bal[q] & lt); // poles before this entry
                 if (fl[q]) {
-                    const long long o = po + rp;
+                    const long long o = po + carry_p + np;
                     w.pd[o] = vd[q];
                     w.pz[o] = vz[q];
                     w.pf[o] = vf[q];
                     w.pl[o] = vl[q];
                     w.pmap[o] = idx;
                     zn += vz[q] * vz[q];
-                    ++rp;
                 } else {
-                    const long long o = gs + rg;
+                    const long long o = gs + carry_g + (idx - base) - np;
                     w.gd[o] = vd[q];
                     w.gf[o] = vf[q];
                     w.gl[o] = vl[q];
                     w.gpos[o] = idx;
-                    ++rg;
                 }
             }
+            before += __popc(bal[q]);
         }
         const int valid = (r1 - base) < EPT * T ? (r1 - base) : EPT * T;
         carry_p += tot;
