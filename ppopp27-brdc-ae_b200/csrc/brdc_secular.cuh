@@ -104,9 +104,10 @@ struct SecRoot {
 
 // Set up root i (0-based) of a problem with K >= 2 poles.  d and z are the
 // pole and weight arrays (only d_p, d_{p+1}, z_p, z_{p+1} are read).
-__host__ __device__ inline void sec_init(SecRoot &r, int i, int K,
-                                         const double *d, const double *z,
-                                         double rho, double znorm2) {
+// The fields of root i that never change (a solver that parks the iteration
+// state between sweeps rebuilds them from the problem instead of storing).
+__host__ __device__ inline void sec_init_static(SecRoot &r, int i, int K, const double *d,
+                                                const double *z, double rho, double znorm2) {
     r.i = i;
     r.last = (i == K - 1) ? 1 : 0;
     r.p = r.last ? K - 2 : i;
@@ -116,6 +117,48 @@ __host__ __device__ inline void sec_init(SecRoot &r, int i, int K,
     r.zq2 = z[r.p + 1] * z[r.p + 1];
     r.rhoinv = 1.0 / rho;
     r.hi0 = rho * znorm2;
+}
+
+// The fields that a sweep and sec_after_sweep advance.
+struct SecDyn {
+    double dorg, tau, lo, hi, prevw, eorg_d, etau;
+    int stage, org, iter, swtch, failed;
+};
+
+__host__ __device__ inline void sec_park(const SecRoot &r, SecDyn &q) {
+    q.dorg = r.dorg;
+    q.tau = r.tau;
+    q.lo = r.lo;
+    q.hi = r.hi;
+    q.prevw = r.prevw;
+    q.eorg_d = r.eorg_d;
+    q.etau = r.etau;
+    q.stage = r.stage;
+    q.org = r.org;
+    q.iter = r.iter;
+    q.swtch = r.swtch;
+    q.failed = r.failed;
+}
+
+__host__ __device__ inline void sec_unpark(SecRoot &r, const SecDyn &q) {
+    r.dorg = q.dorg;
+    r.tau = q.tau;
+    r.lo = q.lo;
+    r.hi = q.hi;
+    r.prevw = q.prevw;
+    r.eorg_d = q.eorg_d;
+    r.etau = q.etau;
+    r.stage = q.stage;
+    r.org = q.org;
+    r.iter = q.iter;
+    r.swtch = q.swtch;
+    r.failed = q.failed;
+}
+
+__host__ __device__ inline void sec_init(SecRoot &r, int i, int K,
+                                         const double *d, const double *z,
+                                         double rho, double znorm2) {
+    sec_init_static(r, i, K, d, z, rho, znorm2);
     r.stage = 0;
     r.iter = 0;
     r.swtch = 0;

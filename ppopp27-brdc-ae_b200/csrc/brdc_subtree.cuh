@@ -51,9 +51,12 @@ struct SubSmem {
     int ex[kSubRows + 1];
     double part[kSubWarps][kSubRows / 16];
     int nstart[kSubRows / 16], nsize[kSubRows / 16], nK[kSubRows / 16], nKz[kSubRows / 16];
+    int kpre[kSubRows / 16 + 1]; // prefix of nK: roots of the level before node j
     double nrho[kSubRows / 16], ntol[kSubRows / 16], nzn[kSubRows / 16], nmaxd[kSubRows / 16];
+    SecDyn dyn[kSubRows];      // parked secular state of each root between rounds
+    int aq[2][kSubRows];       // unconverged roots, ping-pong
     int scan[32];
-    int it_sum, it_max, it_failed;
+    int it_sum, it_max, it_failed, qcnt;
 };
 
 // Exclusive scan of one int per thread over the CTA; ex[kSubRows] = total.
@@ -372,45 +375,134 @@ __global__ void __launch_bounds__(kSubRows, 512 / kSubRows) k_subtree(SubArgs A)
             __syncthreads();
         }
 
-        // secular roots, one thread per root
-        SecRoot st;
-        const bool root = j >= 0 && x - s < K;
-        if (root) {
-            const int r = x - s;
-            const double *pd = S.pd + s, *pz = S.pz + s;
-            if (K == 1) {
-                st.org = 0;
-                st.dorg = pd[0];
-                st.tau = rho * pz[0] * pz[0];
-                st.iter = 0;
-                st.failed = 0;
+        // Secular roots in rounds of one sweep.  After every round the
+        // unconverged roots are packed into a list and spread over the CTA
+        // with `tpr` lanes each (the largest power of two that fits), so no
+        // warp keeps iterating for one slow root while its other lanes idle,
+        // and the last few roots get whole warps.  A root's state is parked
+        // in shared memory between rounds.  Its arithmetic depends only on
+        // tpr (which lanes take which poles), not on where the root sits in
+        // the list, so the result is deterministic.  The Loewner weights and
+        // boundary rows use the same spread over the poles / roots.
+        if (x == 0) {
+            int acc = 0;
+            for (int q = 0; q < nk; ++q) {
+                S.kpre[q] = acc;
+                acc += S.nK[q];
+            }
+            S.kpre[nk] = acc;
+        }
+        __syncthreads();
+        const int nroots = S.kpre[nk];
+        auto root_node = [&](int id) {
+            int q = 0;
+            while (S.kpre[q + 1] <= id) {
+                ++q;
+            }
+            return q;
+        };
+        bool multi = false;
+        if (x < nroots) {
+            const int q = root_node(x);
+            const int rr = x - S.kpre[q], Kr = S.nK[q], sr = S.nstart[q];
+            const double *pd = S.pd + sr, *pz = S.pz + sr;
+            if (Kr == 1) {
+                S.rorg[sr] = 0;
+                S.rdo[sr] = pd[0];
+                S.rtau[sr] = S.nrho[q] * pz[0] * pz[0];
+                S.rlam[sr] = pd[0] + S.rtau[sr];
             } else {
-                sec_init(st, r, K, pd, pz, rho, S.nzn[j]);
-                const int pmin = r < K - 2 ? r : K - 2;
-                for (;;) {
-                    SecSums sum;
-                    sec_zero(sum);
-                    secular_span(sum, st, 0, K, 0, 1, pmin, r + 1,
-                                 [&](int q, double *dq, double *zq) {
-                                     *dq = pd[q];
-                                     *zq = pz[q];
-                                 });
-                    if (sec_after_sweep(st, sum, eps) == 2) {
-                        break;
-                    }
+                SecRoot st;
+                sec_init(st, rr, Kr, pd, pz, S.nrho[q], S.nzn[q]);
+                sec_park(st, S.dyn[x]);
+                multi = true;
+            }
+        }
+        sub_scan(S, multi ? 1 : 0);
+        if (multi) {
+            S.aq[0][S.ex[x]] = x;
+        }
+        int nact = S.ex[kSubRows];
+        int cur = 0;
+        __syncthreads();
+        while (nact > 0) {
+            int tp = 1;
+            while (tp < 32 && nact * tp * 2 <= kSubRows) {
+                tp <<= 1;
+            }
+            const int g2 = x / tp, l2 = x % tp;
+            const bool act = g2 < nact;
+            const int id = act ? S.aq[cur][g2] : 0;
+            const int q = act ? root_node(id) : 0;
+            const int rr = id - S.kpre[q], Kr = S.nK[q], sr = S.nstart[q];
+            const double *pd = S.pd + sr, *pz = S.pz + sr;
+            SecRoot st;
+            if (act) {
+                sec_init_static(st, rr, Kr, pd, pz, S.nrho[q], S.nzn[q]);
+                sec_unpark(st, S.dyn[id]);
+            } else {
+                st.stage = 2;
+            }
+            SecSums sum;
+            sec_zero(sum);
+            if (act) {
+                const int pmin = rr < Kr - 2 ? rr : Kr - 2;
+                secular_span(sum, st, 0, Kr, l2, tp, pmin, rr + 1,
+                             [&](int u, double *du, double *zu) {
+                                 *du = pd[u];
+                                 *zu = pz[u];
+                             });
+            }
+            sums_reduce(sum, tp);
+            if (act) {
+                sec_after_sweep(st, sum, eps);
+            }
+            if (x == 0) {
+                S.qcnt = 0;
+            }
+            __syncthreads();
+            const bool lead = act && l2 == 0;
+            if (lead) {
+                sec_park(st, S.dyn[id]);
+            }
+            const bool more = lead && st.stage != 2;
+            const unsigned mb = __ballot_sync(0xffffffffu, more);
+            int at = 0;
+            if (lane == 0 && mb != 0u) {
+                at = atomicAdd(&S.qcnt, __popc(mb));
+            }
+            at = __shfl_sync(0xffffffffu, at, 0);
+            if (more) {
+                S.aq[cur ^ 1][at + __popc(mb & ((1u << lane) - 1u))] = id;
+            }
+            __syncthreads();
+            nact = S.qcnt;
+            cur ^= 1;
+            __syncthreads();
+        }
+        // results and iteration counts, one thread per root
+        {
+            bool mine = false;
+            int it = 0, fl = 0;
+            if (x < nroots) {
+                const int q = root_node(x);
+                const int sr = S.nstart[q];
+                if (S.nK[q] >= 2) {
+                    const SecDyn &dq = S.dyn[x];
+                    const int rr = x - S.kpre[q];
+                    S.rorg[sr + rr] = dq.org;
+                    S.rdo[sr + rr] = dq.dorg;
+                    S.rtau[sr + rr] = dq.tau;
+                    S.rlam[sr + rr] = dq.dorg + dq.tau;
+                    mine = true;
+                    it = dq.iter;
+                    fl = dq.failed;
                 }
             }
-            S.rorg[s + r] = st.org;
-            S.rdo[s + r] = st.dorg;
-            S.rtau[s + r] = st.tau;
-            S.rlam[s + r] = st.dorg + st.tau;
-        }
-        {
             const unsigned full = 0xffffffffu;
-            const int it = root ? st.iter : 0;
-            const int sum = __reduce_add_sync(full, it);
-            const int mx = __reduce_max_sync(full, it);
-            const int nf = __reduce_add_sync(full, root ? st.failed : 0);
+            const int sum = __reduce_add_sync(full, mine ? it : 0);
+            const int mx = __reduce_max_sync(full, mine ? it : 0);
+            const int nf = __reduce_add_sync(full, mine ? fl : 0);
             if (lane == 0) {
                 atomicAdd(&S.it_sum, sum);
                 atomicMax(&S.it_max, mx);
@@ -419,48 +511,72 @@ __global__ void __launch_bounds__(kSubRows, 512 / kSubRows) k_subtree(SubArgs A)
         }
         __syncthreads();
 
-        if (!top) {
-            // Loewner weights (sqrt(rho) z), one thread per pole
-            if (j >= 0 && x - s < K) {
-                const int i = x - s;
-                const double di = S.pd[s + i];
+        // lanes per pole / root for the Loewner weights and the rows
+        int tpr = 1;
+        while (tpr < 32 && nroots * tpr * 2 <= kSubRows) {
+            tpr <<= 1;
+        }
+        const int grp = x / tpr, gl = x % tpr;
+        const int jr = grp < nroots ? root_node(grp) : -1;
+        const int rr = jr >= 0 ? grp - S.kpre[jr] : 0;  // pole / root index in its node
+        const int Kr = jr >= 0 ? S.nK[jr] : 0;
+        const int sr = jr >= 0 ? S.nstart[jr] : 0;
+        const double rhor = jr >= 0 ? S.nrho[jr] : 0.0;
+        const bool nodetop = top;
+
+        if (!nodetop) {
+            // Loewner weights (sqrt(rho) z), tpr lanes per pole
+            {
                 double prod = 1.0, prod2 = 1.0;
-                int q = 0;
-                for (; q + 1 < K; q += 2) {
-                    const double dl = (di - S.rdo[s + q]) - S.rtau[s + q];
-                    const double dl2 = (di - S.rdo[s + q + 1]) - S.rtau[s + q + 1];
-                    prod *= dl * brdc_rcp(q == i ? 1.0 : di - S.pd[s + q]);
-                    prod2 *= dl2 * brdc_rcp(q + 1 == i ? 1.0 : di - S.pd[s + q + 1]);
+                if (jr >= 0) {
+                    const int i = rr;
+                    const double di = S.pd[sr + i];
+                    int q = gl;
+                    for (; q + tpr < Kr; q += 2 * tpr) {
+                        const int q2 = q + tpr;
+                        const double dl = (di - S.rdo[sr + q]) - S.rtau[sr + q];
+                        const double dl2 = (di - S.rdo[sr + q2]) - S.rtau[sr + q2];
+                        prod *= dl * brdc_rcp(q == i ? 1.0 : di - S.pd[sr + q]);
+                        prod2 *= dl2 * brdc_rcp(q2 == i ? 1.0 : di - S.pd[sr + q2]);
+                    }
+                    if (q < Kr) {
+                        const double dl = (di - S.rdo[sr + q]) - S.rtau[sr + q];
+                        prod *= dl * brdc_rcp(q == i ? 1.0 : di - S.pd[sr + q]);
+                    }
                 }
-                if (q < K) {
-                    const double dl = (di - S.rdo[s + q]) - S.rtau[s + q];
-                    prod *= dl * brdc_rcp(q == i ? 1.0 : di - S.pd[s + q]);
+                prod = group_prod(prod * prod2, tpr);
+                if (jr >= 0 && gl == 0) {
+                    const double zi = S.pz[sr + rr];
+                    const double mag = sqrt(fmax(-prod, 0.0));
+                    double wi = zi < 0.0 ? -mag : mag;
+                    if (!(mag > 0.0) || !isfinite(mag)) {
+                        wi = zi * sqrt(rhor);
+                    }
+                    S.pw[sr + rr] = wi;
                 }
-                prod *= prod2;
-                const double zi = S.pz[s + i];
-                const double mag = sqrt(fmax(-prod, 0.0));
-                double wi = zi < 0.0 ? -mag : mag;
-                if (!(mag > 0.0) || !isfinite(mag)) {
-                    wi = zi * sqrt(rho);
-                }
-                S.pw[s + i] = wi;
             }
             __syncthreads();
-            // boundary rows, one thread per root
-            if (root) {
-                const int r = x - s;
-                const double dorg = S.rdo[s + r], tau = S.rtau[s + r];
+            // boundary rows, tpr lanes per root
+            {
                 double a1 = 0.0, a2 = 0.0, s2 = 0.0;
-                for (int i = 0; i < K; ++i) {
-                    const double dl = (S.pd[s + i] - dorg) - tau;
-                    const double u = (dl != 0.0) ? S.pw[s + i] * brdc_rcp(dl) : 0.0;
-                    s2 += u * u;
-                    a1 += S.pf[s + i] * u;
-                    a2 += S.pl[s + i] * u;
+                if (jr >= 0) {
+                    const double dorg = S.rdo[sr + rr], tau = S.rtau[sr + rr];
+                    for (int i = gl; i < Kr; i += tpr) {
+                        const double dl = (S.pd[sr + i] - dorg) - tau;
+                        const double u = (dl != 0.0) ? S.pw[sr + i] * brdc_rcp(dl) : 0.0;
+                        s2 += u * u;
+                        a1 += S.pf[sr + i] * u;
+                        a2 += S.pl[sr + i] * u;
+                    }
                 }
-                const double nrm = sqrt(s2);
-                S.rf[s + r] = nrm > 0.0 ? a1 / nrm : 0.0;
-                S.rl[s + r] = nrm > 0.0 ? a2 / nrm : 0.0;
+                s2 = group_sum(s2, tpr);
+                a1 = group_sum(a1, tpr);
+                a2 = group_sum(a2, tpr);
+                if (jr >= 0 && gl == 0) {
+                    const double nrm = sqrt(s2);
+                    S.rf[sr + rr] = nrm > 0.0 ? a1 / nrm : 0.0;
+                    S.rl[sr + rr] = nrm > 0.0 ? a2 / nrm : 0.0;
+                }
             }
             __syncthreads();
         }
