@@ -187,14 +187,18 @@ def run_profile_case(spec):
     parts = spec.split(":")
     fam, n = parts[0], int(parts[1])
     solves = int(parts[2]) if len(parts) > 2 else 1
+    adjoint = len(parts) > 3 and parts[3] == "bwd"
     d, e = families.generate(fam, n)
     solver = brdc.Solver()
     D = torch.tensor(d, device="cuda")
     E = torch.tensor(e, device="cuda")
     W = torch.empty(n, dtype=torch.float64, device="cuda")
-    ws = solver.workspace(n)
+    ws = solver.checkpoint_workspace(n) if adjoint else solver.workspace(n)
+    G = torch.ones(n, dtype=torch.float64, device="cuda")
     for _ in range(solves):
         solver.dstebr(D, E, W=W, workspace=ws)
+        if adjoint:
+            solver.dstebr_backward(D, E, G, workspace=ws, keep_forward=True)
     torch.cuda.synchronize()
     solver.close()
 
@@ -208,8 +212,9 @@ def main():
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--profile-case", default=None,
-                    help="family:n[:solves] -- run that many plain solves (default 1) of the "
-                         "seeded instance and exit; a fixed launch sequence for profilers")
+                    help="family:n[:solves[:bwd]] -- run that many plain solves (default 1) of "
+                         "the seeded instance, each followed by the adjoint with bwd, and exit; "
+                         "a fixed launch sequence for profilers")
     args = ap.parse_args()
     if args.profile_case:
         run_profile_case(args.profile_case)

@@ -41,6 +41,8 @@ struct BArgs {
     double *gE;
     int k;
     int nodes;
+    long long level_rows; // rows of the instances merging at this level
+    int lanes_target;     // threads the per-row sweeps aim to keep busy
 };
 
 __device__ inline double sgn(double x) { return (double)((x > 0.0) - (x < 0.0)); }
@@ -356,63 +358,138 @@ __global__ void __launch_bounds__(kSweepThreads) k_bw_poles(BArgs a) {
 //      dL/domega = z_p sum_j (1/N_j)/delta_pj^2
 //                  (gf_m f'_j + gl_m l'_j - gf_j f_m - gl_j l_m),
 //    which k_bw_undeflate turns into +-c s dL/domega on the two d's.
-// One warp per deflated slot of the level; the lanes stride over the roots.
+// `tpr` lanes per deflated row (where deflated rows are most of the level:
+// enough to reach lanes_target threads, at least ~8 roots per lane on
+// average); the lanes stride over the roots and combine by shuffles.  Every warp runs the same number of trips,
+// so the shuffles stay convergent.
 __global__ void __launch_bounds__(256) k_bw_defl(BArgs a, long long total_n) {
     const Ws &w = a.w;
-    const int lane = threadIdx.x & 31;
-    const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
-    for (long long x = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); x < total_n;
-         x += warps) {
-        int g, m, depth;
-        long long gs;
-        if (!elem_node(a.F, a.k, x, &g, &gs, &m, &depth) || depth == 0) {
-            continue;
-        }
-        const long long po = (gs + g + 1) & ~1LL;
-        const int s = (int)(x - gs);
-        const int K = w.nK[g];
-        const int Kz = w.nKz[g];
-        const int ndz = m - Kz;
-        if (s < K) {
-            continue;
-        }
-        const bool small = s < K + ndz;
-        const int q = small ? s - K : s - K - ndz;
-        double di, fi, li, gfi, gli, zp = 1.0;
-        if (small) {
-            di = w.zd[gs + q];
-            fi = w.zf[gs + q];
-            li = w.zl[gs + q];
-            gfi = w.bzf[gs + q];
-            gli = w.bzl[gs + q];
-        } else {
-            const int act = w.gpos[gs + q];
-            const int p = lower_bound_int(w.pmap + po, K, w.gbase[gs + act]);
-            di = w.pd[po + p];
-            zp = w.pw[po + p];
-            fi = w.af[gs + act];
-            li = w.al[gs + act];
-            gfi = w.bgf[gs + q];
-            gli = w.bgl[gs + q];
-        }
+    const LevelCtl *ctl = &w.hdr->lvl[a.k];
+    const long long ndefl = a.level_rows - ctl->total_k;
+    const double kavg = (double)ctl->total_k / (double)(a.nodes > 0 ? a.nodes : 1);
+    // more lanes per row only where deflated rows are most of the level:
+    // below that, every extra lane mostly classifies rows that need nothing
+    int tpr = 1;
+    while (2 * ndefl > a.level_rows && tpr < 32 &&
+           (double)tpr * (double)ndefl < (double)a.lanes_target &&
+           8.0 * (double)(2 * tpr) <= kavg) {
+        tpr <<= 1;
+    }
+    const long long slots = ((total_n * tpr + 31) / 32) * 32;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < slots; t += stride) {
+        const long long x = t / tpr;
+        const int l = (int)(t % tpr);
         double acc = 0.0;
-        for (int j = lane; j < K; j += 32) {
-            const double r = brdc_rcp((di - __ldg(w.rdo + po + j)) - __ldg(w.rtau + po + j));
-            const double t = __ldg(w.bfr + po + j) * fi + __ldg(w.blr + po + j) * li -
-                             gfi * __ldg(w.rfp + po + j) - gli * __ldg(w.rlp + po + j);
-            acc += __ldg(w.rinvn + po + j) * r * (small ? t : -t * r);
+        bool out = false, small = false;
+        long long gs = 0, dst = 0;
+        double scale = 1.0;
+        int g, m, depth;
+        if (x < total_n && elem_node(a.F, a.k, x, &g, &gs, &m, &depth) && depth != 0) {
+            const long long po = (gs + g + 1) & ~1LL;
+            const int s = (int)(x - gs);
+            const int K = w.nK[g];
+            const int Kz = w.nKz[g];
+            const int ndz = m - Kz;
+            if (s >= K) {
+                small = s < K + ndz;
+                const int q = small ? s - K : s - K - ndz;
+                double di, fi, li, gfi, gli, zp = 1.0;
+                if (small) {
+                    di = w.zd[gs + q];
+                    fi = w.zf[gs + q];
+                    li = w.zl[gs + q];
+                    gfi = w.bzf[gs + q];
+                    gli = w.bzl[gs + q];
+                } else {
+                    const int act = w.gpos[gs + q];
+                    const int p = lower_bound_int(w.pmap + po, K, w.gbase[gs + act]);
+                    di = w.pd[po + p];
+                    zp = w.pw[po + p];
+                    fi = w.af[gs + act];
+                    li = w.al[gs + act];
+                    gfi = w.bgf[gs + q];
+                    gli = w.bgl[gs + q];
+                }
+#pragma unroll 4
+                for (int j = l; j < K; j += tpr) {
+                    const double r = brdc_rcp((di - __ldg(w.rdo + po + j)) - __ldg(w.rtau + po + j));
+                    const double tt = __ldg(w.bfr + po + j) * fi + __ldg(w.blr + po + j) * li -
+                                      gfi * __ldg(w.rfp + po + j) - gli * __ldg(w.rlp + po + j);
+                    acc += __ldg(w.rinvn + po + j) * r * (small ? tt : -tt * r);
+                }
+                out = true;
+                dst = gs + q;
+                // 1/N_j is in the scale of the Loewner weights, sqrt(rho) z;
+                // the omega sum multiplies it by a weight of the same scale
+                scale = small ? sqrt(w.nrho[g]) : zp;
+            }
         }
-        acc = warp_sum(acc);
-        if (lane == 0) {
-            // 1/N_j is in the scale of the Loewner weights, sqrt(rho) z; the
-            // omega sum multiplies it by a weight of the same scale
+        acc = group_sum(acc, tpr);
+        if (out && l == 0) {
             if (small) {
-                w.bzz[gs + q] = acc * sqrt(w.nrho[g]);
+                w.bzz[dst] = acc * scale;
             } else {
-                w.bgw[gs + q] = zp * acc;
+                w.bgw[dst] = scale * acc;
             }
         }
     }
+}
+
+// Reverse the rotation chain based at active index b0 of a merge (a cluster
+// is a base with gmark 0 followed by its members, gmark 1, rotated in
+// increasing order); false if no chain starts there.
+__device__ inline bool bw_reverse_chain(const Ws &w, long long gs, int b0, int Kz) {
+    if (w.gmark[gs + b0] != 0 || b0 + 1 >= Kz || w.gmark[gs + b0 + 1] == 0) {
+        return false;
+    }
+    {
+        int c = 1;
+        while (b0 + c + 1 < Kz && w.gmark[gs + b0 + c + 1] != 0) {
+            ++c;
+        }
+        double fb = w.af[gs + b0], lb = w.al[gs + b0];       // rows after the chain
+        double gfb = w.baf[gs + b0], glb = w.bal[gs + b0], gzb = w.baz[gs + b0];
+        double gdb = w.bad[gs + b0];
+        double pic = 1.0; // product of the later rotations' c: omega_k reaches the final base scaled by it
+        for (int kk = c; kk >= 1; --kk) {
+            const long long x = gs + b0 + kk;
+            const double cc = w.gc[x], ss = w.gs[x], rr = w.gr[x];
+            const double fx2 = w.af[x], lx2 = w.al[x];          // member rows after
+            const double fb1 = cc * fb - ss * fx2, fx1 = ss * fb + cc * fx2;
+            const double lb1 = cc * lb - ss * lx2, lx1 = ss * lb + cc * lx2;
+            const double gfx2 = w.baf[x], glx2 = w.bal[x];
+            const double gfb1 = cc * gfb - ss * gfx2, gfx1 = ss * gfb + cc * gfx2;
+            const double glb1 = cc * glb - ss * glx2, glx1 = ss * glb + cc * glx2;
+            const double gcs = gfb * fb1 + gfx2 * fx1 + glb * lb1 + glx2 * lx1;
+            const double gsn = gfb * fx1 - gfx2 * fb1 + glb * lx1 - glx2 * lb1;
+            // r = hypot(zb, zx), c = zb/r, s = zx/r
+            const double gzb1 = gzb * cc + (gcs * ss * ss - gsn * cc * ss) / rr;
+            const double gzx = gzb * ss + (-gcs * cc * ss + gsn * cc * cc) / rr;
+            // d of the rotated pair: the Rayleigh quotients c^2 d_b + s^2 d_x
+            // and s^2 d_b + c^2 d_x, equal to the kept d_b, d_x up to the
+            // deflation tolerance and exact at a tie, where they are the
+            // derivative of the eigenvalues the deflation finds
+            const double c2 = cc * cc, s2 = ss * ss, gdx2 = w.bad[x];
+            const double gom = cc * ss * pic * w.baz[x];
+            w.bad[x] = s2 * gdb + c2 * gdx2 + gom;
+            gdb = c2 * gdb + s2 * gdx2 - gom;
+            pic *= cc;
+            w.baf[x] = gfx1;
+            w.bal[x] = glx1;
+            w.baz[x] = gzx;
+            fb = fb1;
+            lb = lb1;
+            gfb = gfb1;
+            glb = glb1;
+            gzb = gzb1;
+        }
+        w.baf[gs + b0] = gfb;
+        w.bal[gs + b0] = glb;
+        w.baz[gs + b0] = gzb;
+        w.bad[gs + b0] = gdb;
+    }
+    return true;
 }
 
 // ------------------------------------------------------------- undeflate
@@ -465,56 +542,9 @@ __global__ void __launch_bounds__(T) k_bw_undeflate(BArgs a) {
     }
     __syncthreads();
 
-    // reverse every rotation chain: a cluster is a base (gmark 0) followed
-    // by its members (gmark 1), rotated in increasing order
+    // reverse every rotation chain
     for (int b0 = threadIdx.x; b0 < Kz; b0 += T) {
-        if (w.gmark[gs + b0] != 0 || b0 + 1 >= Kz || w.gmark[gs + b0 + 1] == 0) {
-            continue;
-        }
-        int c = 1;
-        while (b0 + c + 1 < Kz && w.gmark[gs + b0 + c + 1] != 0) {
-            ++c;
-        }
-        double fb = w.af[gs + b0], lb = w.al[gs + b0];       // rows after the chain
-        double gfb = w.baf[gs + b0], glb = w.bal[gs + b0], gzb = w.baz[gs + b0];
-        double gdb = w.bad[gs + b0];
-        double pic = 1.0; // product of the later rotations' c: omega_k reaches the final base scaled by it
-        for (int kk = c; kk >= 1; --kk) {
-            const long long x = gs + b0 + kk;
-            const double cc = w.gc[x], ss = w.gs[x], rr = w.gr[x];
-            const double fx2 = w.af[x], lx2 = w.al[x];          // member rows after
-            const double fb1 = cc * fb - ss * fx2, fx1 = ss * fb + cc * fx2;
-            const double lb1 = cc * lb - ss * lx2, lx1 = ss * lb + cc * lx2;
-            const double gfx2 = w.baf[x], glx2 = w.bal[x];
-            const double gfb1 = cc * gfb - ss * gfx2, gfx1 = ss * gfb + cc * gfx2;
-            const double glb1 = cc * glb - ss * glx2, glx1 = ss * glb + cc * glx2;
-            const double gcs = gfb * fb1 + gfx2 * fx1 + glb * lb1 + glx2 * lx1;
-            const double gsn = gfb * fx1 - gfx2 * fb1 + glb * lx1 - glx2 * lb1;
-            // r = hypot(zb, zx), c = zb/r, s = zx/r
-            const double gzb1 = gzb * cc + (gcs * ss * ss - gsn * cc * ss) / rr;
-            const double gzx = gzb * ss + (-gcs * cc * ss + gsn * cc * cc) / rr;
-            // d of the rotated pair: the Rayleigh quotients c^2 d_b + s^2 d_x
-            // and s^2 d_b + c^2 d_x, equal to the kept d_b, d_x up to the
-            // deflation tolerance and exact at a tie, where they are the
-            // derivative of the eigenvalues the deflation finds
-            const double c2 = cc * cc, s2 = ss * ss, gdx2 = w.bad[x];
-            const double gom = cc * ss * pic * w.baz[x];
-            w.bad[x] = s2 * gdb + c2 * gdx2 + gom;
-            gdb = c2 * gdb + s2 * gdx2 - gom;
-            pic *= cc;
-            w.baf[x] = gfx1;
-            w.bal[x] = glx1;
-            w.baz[x] = gzx;
-            fb = fb1;
-            lb = lb1;
-            gfb = gfb1;
-            glb = glb1;
-            gzb = gzb1;
-        }
-        w.baf[gs + b0] = gfb;
-        w.bal[gs + b0] = glb;
-        w.baz[gs + b0] = gzb;
-        w.bad[gs + b0] = gdb;
+        bw_reverse_chain(w, gs, b0, Kz);
     }
     double kr = 0.0;
     for (int j = threadIdx.x; j < K; j += T) {
@@ -556,6 +586,140 @@ __global__ void __launch_bounds__(T) k_bw_undeflate(BArgs a) {
     if (threadIdx.x == 0) {
         const long long cut = gs + m1 - 1;
         a.gE[cut] = 2.0 * sgn(a.E[cut]) * grho;
+    }
+}
+
+// The same undeflation for the large merges near the top, where one CTA per
+// merge would stream tens of thousands of rows alone: five grid-wide passes
+// over the level's rows, each row one independent gather or scatter.  The
+// rotated-out slot q finds its active index through gpos, so no scan is
+// needed.
+
+// poles and rotated-out members -> active positions
+__global__ void __launch_bounds__(256) k_bw_ud_active(BArgs a, long long total_n) {
+    const Ws &w = a.w;
+    for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x; x < total_n;
+         x += (long long)gridDim.x * blockDim.x) {
+        int g, m, depth;
+        long long gs;
+        if (!elem_node(a.F, a.k, x, &g, &gs, &m, &depth)) {
+            continue;
+        }
+        const long long po = (gs + g + 1) & ~1LL;
+        const int s = (int)(x - gs);
+        const int K = w.nK[g], Kz = w.nKz[g];
+        if (s < K) {
+            const long long o = gs + w.pmap[po + s];
+            w.bad[o] = w.bpd[po + s];
+            w.baz[o] = w.bpz[po + s];
+            w.baf[o] = w.bpf[po + s];
+            w.bal[o] = w.bpl[po + s];
+        } else if (s < Kz) {
+            const int q = s - K;
+            const long long o = gs + w.gpos[gs + q];
+            w.bad[o] = w.bgd[gs + q];
+            // a rotated-out member's z is zero for every z, so its slot
+            // carries dL/domega to the chain reversal instead
+            w.baz[o] = depth == 0 ? 0.0 : w.bgw[gs + q];
+            w.baf[o] = w.bgf[gs + q];
+            w.bal[o] = w.bgl[gs + q];
+        }
+    }
+}
+
+// Givens chains, one thread per active index (chain bases do the work)
+__global__ void __launch_bounds__(256) k_bw_ud_chains(BArgs a, long long total_n) {
+    const Ws &w = a.w;
+    for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x; x < total_n;
+         x += (long long)gridDim.x * blockDim.x) {
+        int g, m, depth;
+        long long gs;
+        if (!elem_node(a.F, a.k, x, &g, &gs, &m, &depth)) {
+            continue;
+        }
+        const int s = (int)(x - gs);
+        const int Kz = w.nKz[g];
+        if (s < Kz) {
+            bw_reverse_chain(w, gs, s, Kz);
+        }
+    }
+}
+
+// active and small-z lists -> merged positions
+__global__ void __launch_bounds__(256) k_bw_ud_merged(BArgs a, long long total_n) {
+    const Ws &w = a.w;
+    for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x; x < total_n;
+         x += (long long)gridDim.x * blockDim.x) {
+        int g, m, depth;
+        long long gs;
+        if (!elem_node(a.F, a.k, x, &g, &gs, &m, &depth)) {
+            continue;
+        }
+        const int s = (int)(x - gs);
+        const int Kz = w.nKz[g];
+        if (s < Kz) {
+            const long long p = gs + w.amap[gs + s];
+            w.bmd[p] = w.bad[gs + s];
+            w.bmz[p] = w.baz[gs + s];
+            w.bmf[p] = w.baf[gs + s];
+            w.bml[p] = w.bal[gs + s];
+        } else {
+            const int q = s - Kz;
+            const long long p = gs + w.zmap[gs + q];
+            w.bmd[p] = w.bzd[gs + q];
+            w.bmz[p] = depth == 0 ? 0.0 : w.bzz[gs + q];
+            w.bmf[p] = w.bzf[gs + q];
+            w.bml[p] = w.bzl[gs + q];
+        }
+    }
+}
+
+// merged positions -> children (z = last row of the left child / first row
+// of the right child, over sqrt 2)
+__global__ void __launch_bounds__(256) k_bw_ud_children(BArgs a, long long total_n) {
+    const Ws &w = a.w;
+    const double isq2 = 0.70710678118654752440;
+    for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x; x < total_n;
+         x += (long long)gridDim.x * blockDim.x) {
+        int g, m, depth;
+        long long gs;
+        if (!elem_node(a.F, a.k, x, &g, &gs, &m, &depth)) {
+            continue;
+        }
+        const int p = (int)(x - gs);
+        const int m1 = m >> 1;
+        const long long xc = gs + w.morig[gs + p];
+        const int e = (int)(xc - gs);
+        w.bcd[xc] = w.bmd[x];
+        if (e < m1) {
+            w.bcf[xc] = w.bmf[x];
+            w.bcl[xc] = w.bmz[x] * isq2;
+        } else {
+            w.bcf[xc] = w.bmz[x] * isq2;
+            w.bcl[xc] = w.bml[x];
+        }
+    }
+}
+
+// dL/drho of every merge summed over its roots by one warp, in a fixed
+// order, and dL/dE at its cut
+__global__ void __launch_bounds__(256) k_bw_ud_rho(BArgs a) {
+    const Ws &w = a.w;
+    const int lane = threadIdx.x & 31;
+    const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long g = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); g < a.nodes;
+         g += warps) {
+        const NodeGeom G = node_geom(a.F, a.k, (int)g);
+        const int K = w.nK[g];
+        double kr = 0.0;
+        for (int j = lane; j < K; j += 32) {
+            kr += w.rkr[G.poff + j];
+        }
+        kr = warp_sum(kr);
+        if (lane == 0) {
+            const long long cut = G.gstart + G.m1 - 1;
+            a.gE[cut] = 2.0 * sgn(a.E[cut]) * kr;
+        }
     }
 }
 

@@ -1133,7 +1133,7 @@ brdc_status run_backward(brdc_handle h, const HostForest &hf, const Layout &L,
     double *par[3] = {w.bnd, w.bnf, w.bnl};
     double *out[3] = {w.bcd, w.bcf, w.bcl};
     const int wgrid = h->sm_count * 2;
-    long long dgrid = (nt + 7) / 8;
+    long long dgrid = (4 * nt + 255) / 256;
     dgrid = std::max<long long>(1, std::min<long long>(dgrid, (long long)h->sm_count * 16));
     for (int k = hf.max_levels - 1; k >= 0; --k) {
         Ws wl = w;
@@ -1154,13 +1154,25 @@ brdc_status run_backward(brdc_handle h, const HostForest &hf, const Layout &L,
         b.gE = gE;
         b.k = k;
         b.nodes = hf.level_nodes[k];
+        b.level_rows = hf.level_rows[k];
+        b.lanes_target = h->lanes_target;
         k_bw_unplace<<<(unsigned)eg, 256, 0, s>>>(b, nt);
         k_bw_roots<<<wgrid, kSweepThreads, 0, s>>>(b);
         k_bw_poles<<<wgrid, kSweepThreads, 0, s>>>(b);
         if (k + 1 < hf.max_levels || hf.B > 1) {
+            // up to 4 lanes per row (the kernel picks); surplus blocks exit
             k_bw_defl<<<(unsigned)dgrid, 256, 0, s>>>(b, nt);
         }
-        launch_undeflate_sized(b, hf.level_mmax[k], s);
+        if (hf.level_mmax[k] >= 2 * kDeflEPT * 1024) {
+            // large merges: grid-wide passes instead of one CTA per merge
+            k_bw_ud_active<<<(unsigned)eg, 256, 0, s>>>(b, nt);
+            k_bw_ud_chains<<<(unsigned)eg, 256, 0, s>>>(b, nt);
+            k_bw_ud_merged<<<(unsigned)eg, 256, 0, s>>>(b, nt);
+            k_bw_ud_children<<<(unsigned)eg, 256, 0, s>>>(b, nt);
+            k_bw_ud_rho<<<std::max(1, std::min(b.nodes / 8 + 1, h->sm_count * 8)), 256, 0, s>>>(b);
+        } else {
+            launch_undeflate_sized(b, hf.level_mmax[k], s);
+        }
         BRDC_CUDA(h, "brdc.bw.level", cudaGetLastError());
         std::swap(par[0], out[0]);
         std::swap(par[1], out[1]);
