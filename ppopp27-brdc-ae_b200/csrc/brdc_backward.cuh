@@ -822,18 +822,21 @@ __global__ void __launch_bounds__(kLeafWarps * 32)
         }
         double dx = 0.0, ex = 0.0, exm1 = 0.0;
         if (x < s) {
-            dx = a.D[LG.gstart + x];
+            // the scaled problem of the forward (the gradient of a
+            // homogeneous map is scale-free, so nothing else changes)
+            const double sc = inst_scale(a.w, LG.inst);
+            dx = sc * a.D[LG.gstart + x];
             if (x == 0 && LG.gstart > LG.istart) {
-                dx -= fabs(a.E[LG.gstart - 1]);
+                dx -= sc * fabs(a.E[LG.gstart - 1]);
             }
             if (x == s - 1 && LG.gstart + s < LG.iend) {
-                dx -= fabs(a.E[LG.gstart + s - 1]);
+                dx -= sc * fabs(a.E[LG.gstart + s - 1]);
             }
             if (x + 1 < s) {
-                ex = fabs(a.E[LG.gstart + x]);
+                ex = sc * fabs(a.E[LG.gstart + x]);
             }
             if (x >= 1) {
-                exm1 = fabs(a.E[LG.gstart + x - 1]);
+                exm1 = sc * fabs(a.E[LG.gstart + x - 1]);
             }
         }
         double reg[16], v[16];

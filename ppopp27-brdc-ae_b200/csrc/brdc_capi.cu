@@ -140,7 +140,7 @@ bool build_forest(int B, const long long *off, HostForest *f) {
 // Workspace descriptor: every array with its element size, its length
 // class and whether a checkpointing workspace keeps one slice per level
 // (the arrays the adjoint reads back).
-enum CountKind { CN_NT, CN_NP, CN_NN, CN_NN1, CN_ITW, CN_ITC, CN_B1, CN_B, CN_NODEPRE };
+enum CountKind { CN_NT, CN_NP, CN_NN, CN_NN1, CN_ITW, CN_ITC, CN_B1, CN_B, CN_NODEPRE, CN_INST };
 
 struct SlotDesc {
     int kind;        // 0 double*, 1 int*, 2 long long*
@@ -178,7 +178,7 @@ const SlotDesc kSlots[] = {
     SI(items_w, CN_ITW, true, false), SI(items_c, CN_ITC, true, false),
     SL(f_off, CN_B1, false, false), SI(f_lev, CN_B, false, false),
     SI(f_node_prefix, CN_NODEPRE, false, false), SI(f_leaf_prefix, CN_B1, false, false),
-    SI(f_sub_prefix, CN_B1, false, false),
+    SI(f_sub_prefix, CN_B1, false, false), SL(f_norm, CN_INST, false, false),
     // adjoint
     SD(bcd, CN_NT, false, true), SD(bcf, CN_NT, false, true), SD(bcl, CN_NT, false, true),
     SD(bnd, CN_NT, false, true), SD(bnf, CN_NT, false, true), SD(bnl, CN_NT, false, true),
@@ -207,6 +207,7 @@ long long slot_count(CountKind c, const HostForest &f, const Layout &L) {
     case CN_B1: return f.B > 1 ? f.B + 1 : 0;
     case CN_B: return f.B > 1 ? f.B : 0;
     case CN_NODEPRE: return f.B > 1 ? (long long)(f.B + 1) * std::max(f.max_levels, 1) : 0;
+    case CN_INST: return std::max(f.B, 1);
     }
     return 0;
 }
@@ -430,9 +431,15 @@ brdc_status run_forest(brdc_handle h, const HostForest &hf, const Layout &L,
     h->launches = 0;
     h->timed_levels = hf.max_levels;
     mark(h, 0);
-    k_init<<<1, 64, 0, s>>>(w.hdr, hf.max_levels, hf.B, hf.total_n, hf.leaves, 0);
+    k_init<<<1, 64, 0, s>>>(w.hdr, hf.max_levels, hf.B, hf.total_n, hf.leaves, 0, w.f_norm);
     BRDC_CUDA(h, "brdc.init", cudaGetLastError());
-    ++h->launches;
+    {
+        long long ng = hf.B > 1 ? (hf.B + 7) / 8 : (hf.total_n + 255) / 256;
+        ng = std::max<long long>(1, std::min<long long>(ng, (long long)h->sm_count * 4));
+        k_norm<<<(unsigned)ng, 256, 0, s>>>(F, D, E, w.f_norm);
+        BRDC_CUDA(h, "brdc.norm", cudaGetLastError());
+    }
+    h->launches += 2;
     mark(h, 1);
 
     KArgs a{};

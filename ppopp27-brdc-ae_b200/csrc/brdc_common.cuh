@@ -135,6 +135,7 @@ struct Ws {
     // forest tables (batched)
     long long *f_off;
     int *f_lev, *f_node_prefix, *f_leaf_prefix, *f_sub_prefix;
+    long long *f_norm;           // per instance: bits of max(|D|, |E|) (>= 0)
     // adjoint (present when the workspace keeps checkpoints)
     double *bcd, *bcf, *bcl, *bnd, *bnf, *bnl;   // cotangents, ping-pong
     double *bmd, *bmz, *bmf, *bml;               // at merged positions
@@ -244,9 +245,10 @@ __device__ inline NodeGeom node_geom(const Forest &F, int k, int g) {
 // Merge node at forest level k that contains global row x.  Returns false
 // when the row's instance has no merge at this level.
 __device__ inline bool elem_node(const Forest &F, int k, long long x, int *g,
-                                 long long *gstart, int *m, int *depth_out) {
+                                 long long *gstart, int *m, int *depth_out,
+                                 int *inst_out = nullptr) {
     long long base = 0, n = F.n0;
-    int L = F.L0, pre = 0;
+    int L = F.L0, pre = 0, inst = 0;
     if (F.B > 1) {
         int lo = 0, hi = F.B; // last b with off[b] <= x
         while (hi - lo > 1) {
@@ -261,6 +263,10 @@ __device__ inline bool elem_node(const Forest &F, int k, long long x, int *g,
         n = F.off[lo + 1] - base;
         L = F.lev[lo];
         pre = F.node_prefix[(size_t)k * (F.B + 1) + lo];
+        inst = lo;
+    }
+    if (inst_out != nullptr) {
+        *inst_out = inst;
     }
     if (L <= k) {
         return false;
@@ -289,7 +295,8 @@ __device__ inline bool elem_node(const Forest &F, int k, long long x, int *g,
 struct LeafGeom {
     long long gstart, istart, iend;
     int s;
-    int top; // instance is a single leaf
+    int top;  // instance is a single leaf
+    int inst; // instance index
 };
 
 __device__ inline LeafGeom leaf_geom(const Forest &F, long long g) {
@@ -313,7 +320,30 @@ __device__ inline LeafGeom leaf_geom(const Forest &F, long long g) {
     G.iend = base + n;
     G.s = (int)s;
     G.top = (L == 0);
+    G.inst = b;
     return G;
+}
+
+// Scale of instance b: matrices whose max-norm lies outside [2^-8, 2^8] are
+// solved as the exact power-of-two multiple with max-norm in [0.5, 1), like
+// the reference CPU path normalises before DLAED0_BR (dstedc_dc_br.f:114-128).
+// The deflation tolerance mixes the scale of d with that of z (eigenvector
+// entries, scale-free), so an unscaled tiny matrix would deflate every pole;
+// a power of two leaves every rounding unchanged.  Returns s with D_s = s D.
+__device__ inline double inst_scale(const Ws &w, int b) {
+    const double mx = __longlong_as_double(w.f_norm[b]);
+    if (!(mx > 0.0) || !isfinite(mx) || (mx >= 0x1.0p-8 && mx <= 0x1.0p8)) {
+        return 1.0;
+    }
+    return ldexp(1.0, -(ilogb(mx) + 1));
+}
+
+__device__ inline double inst_unscale(const Ws &w, int b) {
+    const double mx = __longlong_as_double(w.f_norm[b]);
+    if (!(mx > 0.0) || !isfinite(mx) || (mx >= 0x1.0p-8 && mx <= 0x1.0p8)) {
+        return 1.0;
+    }
+    return ldexp(1.0, ilogb(mx) + 1);
 }
 
 // ---------------------------------------------------------------- helpers

@@ -152,18 +152,19 @@ __device__ inline int leaf_solve(const KArgs &a, const LeafGeom &G, int s, int x
     const double eps = DBL_EPSILON;
     double dx = 0.0, ex = 0.0, exm1 = 0.0;
     if (x < s) {
-        dx = a.D[G.gstart + x];
+        const double sc = inst_scale(a.w, G.inst);
+        dx = sc * a.D[G.gstart + x];
         if (x == 0 && G.gstart > G.istart) {
-            dx -= fabs(a.E[G.gstart - 1]);
+            dx -= sc * fabs(a.E[G.gstart - 1]);
         }
         if (x == s - 1 && G.gstart + s < G.iend) {
-            dx -= fabs(a.E[G.gstart + s - 1]);
+            dx -= sc * fabs(a.E[G.gstart + s - 1]);
         }
         if (x + 1 < s) {
-            ex = fabs(a.E[G.gstart + x]);
+            ex = sc * fabs(a.E[G.gstart + x]);
         }
         if (x >= 1) {
-            exm1 = fabs(a.E[G.gstart + x - 1]);
+            exm1 = sc * fabs(a.E[G.gstart + x - 1]);
         }
     }
     double reg[16];
@@ -258,7 +259,7 @@ __global__ void __launch_bounds__(kLeafWarps * 32)
         if (x < s) {
             const long long o = G.gstart + x;
             if (G.top) {
-                a.W[o] = key;
+                a.W[o] = key * inst_unscale(a.w, G.inst);
             } else {
                 a.w.cd[o] = key;
                 a.w.cf[o] = v0;
@@ -704,7 +705,7 @@ __device__ inline void defl_node_scalars(const KArgs &a, const NodeGeom &G, doub
     const double *Ad = w.cd + gs;
     const double *Bd = w.cd + gs + G.m1;
     const int m2 = G.m - G.m1;
-    *rho = 2.0 * fabs(a.E[gs + G.m1 - 1]);
+    *rho = 2.0 * inst_scale(w, G.inst) * fabs(a.E[gs + G.m1 - 1]);
     *maxd = fmax(fmax(fabs(Ad[0]), fabs(Ad[G.m1 - 1])), fmax(fabs(Bd[0]), fabs(Bd[m2 - 1])));
 }
 
@@ -1499,9 +1500,9 @@ __global__ void __launch_bounds__(256) k_place(KArgs a, long long total_n) {
     const Ws &w = a.w;
     for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x; x < total_n;
          x += (long long)gridDim.x * blockDim.x) {
-        int g, m, depth;
+        int g, m, depth, inst;
         long long gs;
-        if (!elem_node(a.F, a.k, x, &g, &gs, &m, &depth)) {
+        if (!elem_node(a.F, a.k, x, &g, &gs, &m, &depth, &inst)) {
             continue;
         }
         const long long po = (gs + g + 1) & ~1LL;
@@ -1537,7 +1538,7 @@ __global__ void __launch_bounds__(256) k_place(KArgs a, long long total_n) {
         }
         const long long o = gs + pos;
         if (top) {
-            a.W[o] = val;
+            a.W[o] = val * inst_unscale(w, inst);
         } else {
             w.nd[o] = val;
             w.nf[o] = fo;
@@ -1546,9 +1547,53 @@ __global__ void __launch_bounds__(256) k_place(KArgs a, long long total_n) {
     }
 }
 
+// Max-norm max(|D|, |E|) of every instance, as the bits of a non-negative
+// double (which order like the integers): grid-wide with one
+// atomic per block for a single matrix, one warp per instance for a batch.
+__global__ void __launch_bounds__(256) k_norm(Forest F, const double *D, const double *E,
+                                              long long *out) {
+    const int lane = threadIdx.x & 31;
+    if (F.B == 1) {
+        const long long n = F.n0;
+        double mx = 0.0;
+        for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+             i += (long long)gridDim.x * blockDim.x) {
+            mx = fmax(mx, fabs(D[i]));
+            if (i + 1 < n) {
+                mx = fmax(mx, fabs(E[i]));
+            }
+        }
+        __shared__ double red[32];
+        mx = block_max<256>(mx, red);
+        if (threadIdx.x == 0) {
+            atomicMax(out, __double_as_longlong(mx));
+        }
+        return;
+    }
+    const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long b = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); b < F.B;
+         b += warps) {
+        const long long lo = F.off[b], hi = F.off[b + 1];
+        double mx = 0.0;
+        for (long long i = lo + lane; i < hi; i += 32) {
+            mx = fmax(mx, fabs(D[i]));
+            if (i + 1 < hi) {
+                mx = fmax(mx, fabs(E[i]));
+            }
+        }
+        mx = warp_max(mx);
+        if (lane == 0) {
+            out[b] = __double_as_longlong(mx);
+        }
+    }
+}
+
 __global__ void k_init(WsHeader *h, int levels, int B, long long total_n,
-                       long long leaves, int flags) {
+                       long long leaves, int flags, long long *norm) {
     const int t = threadIdx.x;
+    if (t == 0) {
+        norm[0] = 0;
+    }
     if (t == 0) {
         h->magic = kWsMagic;
         h->B = B;

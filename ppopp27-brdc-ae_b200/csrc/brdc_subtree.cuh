@@ -151,6 +151,8 @@ __global__ void __launch_bounds__(kSubRows, 512 / kSubRows) k_subtree(SubArgs A)
     walk_node(n, L - Ls, t, &sst, &ssz);
     const long long gsub = base + sst;
     const int R = (int)ssz;
+    const double esc = inst_scale(a.w, b);     // E (and D) of the scaled problem
+    const double wsc = inst_unscale(a.w, b);   // back to the caller's scale
 
     if (x == 0) {
         S.it_sum = 0;
@@ -175,6 +177,7 @@ __global__ void __launch_bounds__(kSubRows, 512 / kSubRows) k_subtree(SubArgs A)
                 LG.iend = base + n;
                 LG.s = (int)lsz;
                 LG.top = (L == 0);
+                LG.inst = b;
                 s = LG.s;
             }
             double key, v0, v1;
@@ -183,7 +186,7 @@ __global__ void __launch_bounds__(kSubRows, 512 / kSubRows) k_subtree(SubArgs A)
             if (xl < s) {
                 const int o = (int)(LG.gstart - gsub) + xl;
                 if (LG.top) {
-                    a.W[LG.gstart + xl] = key;
+                    a.W[LG.gstart + xl] = key * wsc;
                 } else {
                     S.cd[o] = key;
                     S.cf[o] = v0;
@@ -242,7 +245,7 @@ __global__ void __launch_bounds__(kSubRows, 512 / kSubRows) k_subtree(SubArgs A)
         }
         if (x < nk) {
             const int s0 = S.nstart[x], mm = S.nsize[x], h = mm >> 1;
-            S.nrho[x] = 2.0 * fabs(a.E[gsub + s0 + h - 1]);
+            S.nrho[x] = 2.0 * esc * fabs(a.E[gsub + s0 + h - 1]);
             S.nmaxd[x] = fmax(fmax(fabs(S.cd[s0]), fabs(S.cd[s0 + h - 1])),
                               fmax(fabs(S.cd[s0 + h]), fabs(S.cd[s0 + mm - 1])));
         }
@@ -690,7 +693,7 @@ __global__ void __launch_bounds__(kSubRows, 512 / kSubRows) k_subtree(SubArgs A)
                 lo = S.gl[s + u];
             }
             if (top) {
-                a.W[gsub + s + pos] = val;
+                a.W[gsub + s + pos] = val * wsc;
             } else {
                 S.cd[s + pos] = val;
                 S.cf[s + pos] = fo;
