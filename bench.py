@@ -270,11 +270,9 @@ def main():
     if dist is not None:
         dist.barrier()
     clocks = stop_clock_sampler(sampler, clocks_path, local_rank) if rank == 0 else None
-    ms = float(np.mean(times))
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    from brdc.sharding import max_over_ranks
+
+    ms = max_over_ranks(float(np.mean(times)), dist, device="cuda")
 
     extras = {}
     if rank == 0 and not args.no_extras:

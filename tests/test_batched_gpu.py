@@ -148,3 +148,23 @@ def test_batched_tunings_agree(solver):
         assert errs.max() < TOL
     finally:
         s.close()
+
+
+def test_sharded_batch_matches_whole(solver):
+    """A batch split by the multi-GPU partition and solved share by share
+    (here one after another on one GPU) gives the whole batch's results."""
+    import torch
+
+    from brdc.sharding import pack, partition_instances
+
+    off, D, E, orders, _ = families.batch(40, 17, 2500, seed=6)
+    whole = solver.dstebr_batched(off, torch.tensor(D, device="cuda"),
+                                  torch.tensor(E, device="cuda")).cpu().numpy()
+    for idx in partition_instances(orders, 3):
+        o2, D2, E2 = pack(off, D, E, idx)
+        part = solver.dstebr_batched(o2, torch.tensor(D2, device="cuda"),
+                                     torch.tensor(E2, device="cuda")).cpu().numpy()
+        for k, i in enumerate(idx):
+            lo, hi = int(off[i]), int(off[i + 1])
+            sc = np.max(np.abs(whole[lo:hi]))
+            assert np.max(np.abs(part[o2[k]:o2[k + 1]] - whole[lo:hi])) < 1e-13 * sc
