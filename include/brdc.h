@@ -206,15 +206,23 @@ typedef struct brdc_timings {
  *                       leaves alone and every level with per-level kernels;
  *                       up to 4 levels a CTA holds 256 rows, 5 levels 512)
  *   deflate_cluster     largest thread-block cluster that deflates one big
- *                       merge (1, 2, 4 or 8; 1 = one CTA per merge)
+ *                       merge (1, 2, 4, 8 or 16; 1 = one CTA per merge; the
+ *                       per-level deflation kernel uses at most 8)
  *   sweep_lanes_target  threads the per-level root sweeps aim to keep busy
  *                       (lanes per root = smallest power of two reaching it)
+ *   fused_level_rows    levels above the subtree whose largest merge has at
+ *                       most this many rows run as one fused kernel per level
+ *                       (merge, deflation, roots of merges with <= 1024
+ *                       poles, placement; larger merges continue in the
+ *                       sweep kernel); 0 disables it
  * brdc_autotune picks them by timing; defaults: subtree_levels = -1 (by
- * tree height: 3 up to n = 16384, 4 up to 32768, 5 above), 8, 75776. */
+ * tree height: 3 up to n = 16384, 4 up to 32768, 5 above), 16, 75776,
+ * fused_level_rows = 2^30 (every level). */
 typedef struct brdc_tuning {
     int subtree_levels;
     int deflate_cluster;
     int sweep_lanes_target;
+    int fused_level_rows;
 } brdc_tuning;
 
 brdc_status brdc_set_tuning(brdc_handle handle, const brdc_tuning *tuning);

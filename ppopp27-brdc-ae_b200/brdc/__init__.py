@@ -120,6 +120,7 @@ class Tuning(ctypes.Structure):
         ("subtree_levels", ctypes.c_int),
         ("deflate_cluster", ctypes.c_int),
         ("sweep_lanes_target", ctypes.c_int),
+        ("fused_level_rows", ctypes.c_int),
     ]
 
     def as_dict(self) -> dict:
@@ -278,7 +279,7 @@ class Solver:
 
     def set_tuning(self, **kw) -> None:
         """Change launch-shape parameters (subtree_levels, deflate_cluster,
-        sweep_lanes_target); the others keep their values."""
+        sweep_lanes_target, fused_level_rows); the others keep their values."""
         cur = self.tuning()
         cur.update(kw)
         t = Tuning(**cur)

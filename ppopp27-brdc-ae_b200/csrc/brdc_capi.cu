@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "brdc_backward.cuh"
+#include "brdc_level.cuh"
 #include "brdc_subtree.cuh"
 
 using namespace brdc;
@@ -38,8 +39,9 @@ struct brdc_handle_struct {
     // merge levels solved inside the subtree kernel (0: leaves alone,
     // -1: chosen per solve from the tree height)
     int sub_levels = -1;
-    int defl_cluster = 8;         // largest deflation cluster
+    int defl_cluster = 16;        // largest deflation cluster (8 for k_merge_deflate_cl)
     int lanes_target = 75776;     // root-sweep parallelism target
+    int lvl_rows = 1 << 30;       // largest merge of a level run by k_level (0: none)
     std::vector<long long> prep_off;
     // phase timing (off by default)
     int timing;
@@ -398,6 +400,18 @@ cudaError_t set_attrs() {
         e = cudaFuncSetAttribute(k_subtree<512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)sizeof(SubSmem<512>));
     }
+    if (e == cudaSuccess) {
+        e = cudaFuncSetAttribute(k_level<kLvlThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(LvlSmem));
+    }
+    if (e == cudaSuccess) {
+        e = cudaFuncSetAttribute(k_level<kLvlThreads>,
+                                 cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    }
+    if (e == cudaSuccess) {
+        e = cudaFuncSetAttribute(k_sweeps, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem_tiles(4));
+    }
     g_attr_done = (e == cudaSuccess);
     return e;
 }
@@ -419,6 +433,152 @@ int effective_sub_levels(brdc_handle h, const HostForest &hf) {
         return h->sub_levels;
     }
     return hf.max_levels <= 10 ? 3 : (hf.max_levels == 11 ? 4 : 5);
+}
+
+// Clusters of C = 1, 2, 4, 8, 16 k_level CTAs the device holds at once
+// (0: C not schedulable).  Asked once per device (after set_attrs, which
+// sizes its shared memory and allows the non-portable size 16).
+const int *level_clusters(int device) {
+    static int cached[64][5];
+    static bool done[64];
+    static const int none[5] = {0, 0, 0, 0, 0};
+    if (device < 0 || device >= 64) {
+        return none;
+    }
+    if (!done[device]) {
+        for (int q = 0; q < 5; ++q) {
+            const int C = 1 << q;
+            cudaLaunchAttribute at[1];
+            cudaLaunchConfig_t cfg = cluster_config((unsigned)C, C, nullptr, at);
+            cfg.blockDim = dim3(kLvlThreads);
+            cfg.dynamicSmemBytes = sizeof(LvlSmem);
+            int n = 0;
+            if (cudaOccupancyMaxActiveClusters(&n, k_level<kLvlThreads>, &cfg) != cudaSuccess) {
+                cudaGetLastError();
+                n = 0;
+            }
+            cached[device][q] = n;
+        }
+        done[device] = true;
+    }
+    return cached[device];
+}
+
+// Resident k_sweeps blocks per SM (without / with the CTA-role tiles), once
+// per device; 0 when the device has no cooperative launch.
+int sweeps_per_sm(int device, bool tiles) {
+    static int cached[64][2];
+    static bool done[64][2];
+    if (device < 0 || device >= 64) {
+        return 0;
+    }
+    if (!done[device][tiles]) {
+        int coop = 0, nb = 0;
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
+        if (coop == 0 ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_sweeps, kSweepThreads,
+                                                          tiles ? smem_tiles(4) : 0) !=
+                cudaSuccess) {
+            cudaGetLastError();
+            nb = 0;
+        }
+        cached[device][tiles] = nb;
+        done[device][tiles] = true;
+    }
+    return cached[device][tiles];
+}
+
+// Roots, Loewner weights, rows and placement of level a.k: one cooperative
+// k_sweeps (with tile memory where a merge can exceed kWarpMaxK poles), or
+// the four kernels where the device cannot launch it.
+// Returns the number of kernels launched.
+int launch_sweeps(brdc_handle h, const HostForest &hf, const KArgs &a, cudaStream_t s) {
+    const int k = a.k;
+    const bool tiles = hf.level_mmax[k] > kWarpMaxK;
+    const int rows = h->has_lowner[k];
+    const int nb = sweeps_per_sm(h->device, tiles);
+    if (nb > 0) {
+        const int grid = nb * h->sm_count;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeCooperative;
+        at[0].val.cooperative = 1;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)grid);
+        cfg.blockDim = dim3(kSweepThreads);
+        cfg.dynamicSmemBytes = tiles ? smem_tiles(4) : 0;
+        cfg.stream = s;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        cudaLaunchKernelEx(&cfg, k_sweeps, a, tiles ? 1 : 0, rows, (long long)hf.total_n);
+        mark(h, 4 + 4 * k);
+        mark(h, 5 + 4 * k);
+        mark(h, 6 + 4 * k);
+        return 1;
+    }
+    const int cta_blocks = tiles ? h->sm_count * 2 : 0;
+    const int grid = cta_blocks + h->sm_count * 2;
+    int n = 0;
+    k_secular<<<grid, kSweepThreads, cta_blocks ? smem_tiles(2) : 0, s>>>(a, cta_blocks);
+    ++n;
+    mark(h, 4 + 4 * k);
+    if (rows) {
+        k_lowner<<<grid, kSweepThreads, cta_blocks ? smem_tiles(3) : 0, s>>>(a, cta_blocks);
+        ++n;
+    }
+    mark(h, 5 + 4 * k);
+    if (rows) {
+        k_rows<<<grid, kSweepThreads, cta_blocks ? smem_tiles(4) : 0, s>>>(a, cta_blocks);
+        ++n;
+    }
+    long long elem_grid = (hf.total_n + 255) / 256;
+    elem_grid = std::max<long long>(1, std::min<long long>(elem_grid, (long long)h->sm_count * 8));
+    k_place<<<(unsigned)elem_grid, 256, 0, s>>>(a, hf.total_n);
+    ++n;
+    mark(h, 6 + 4 * k);
+    return n;
+}
+
+// One fused level (k_level), then k_sweeps for its merges with more than
+// kLvlMaxK poles (it returns at once when there are none).  Returns the
+// number of kernels launched.
+int launch_level_fused(brdc_handle h, const HostForest &hf, const KArgs &a0, bool ckpt,
+                       cudaStream_t s) {
+    const int k = a0.k;
+    const int mmax = hf.level_mmax[k];
+    // a cluster per node: at least one CTA per kLvlRowsPerCta rows, then
+    // larger while every node's cluster still runs in the first wave
+    const int *act = level_clusters(h->device);
+    int q = 0;
+    while (q < 4 && (1 << q) < h->defl_cluster && act[q + 1] > 0 &&
+           (1 << q) * kLvlRowsPerCta < mmax) {
+        ++q;
+    }
+    while (q < 4 && (2 << q) <= h->defl_cluster && act[q + 1] >= a0.nodes) {
+        ++q;
+    }
+    const int C = 1 << q;
+    KArgs a = a0;
+    a.big_k = kLvlMaxK;
+    a.plan_inline = a.nodes <= kLvlThreads ? 1 : 0;
+    cudaLaunchAttribute at[1];
+    cudaLaunchConfig_t cfg = cluster_config((unsigned)(a.nodes * C), C, s, at);
+    cfg.blockDim = dim3(kLvlThreads);
+    cfg.dynamicSmemBytes = sizeof(LvlSmem);
+    cudaLaunchKernelEx(&cfg, k_level<kLvlThreads>, a);
+    int n = 1;
+    if (!a.plan_inline) {
+        k_plan<1024><<<1, 1024, 0, s>>>(a);
+        ++n;
+    }
+    mark(h, 3 + 4 * k);
+    n += launch_sweeps(h, hf, a, s);
+    if (ckpt) {
+        // the adjoint's sweeps want the item tables of every merge
+        a.big_k = 0;
+        k_plan<1024><<<1, 1024, 0, s>>>(a);
+        ++n;
+    }
+    return n;
 }
 
 // Enqueue the whole forward solve.
@@ -511,7 +671,6 @@ brdc_status run_forest(brdc_handle h, const HostForest &hf, const Layout &L,
         mark(h, 2);
         h->fused_levels = 0;
     }
-    const int warp_blocks = h->sm_count * 2;
     long long elem_grid = (hf.total_n + 255) / 256;
     elem_grid = std::max<long long>(1, std::min<long long>(elem_grid, (long long)h->sm_count * 8));
     for (int k = (sub > 0 ? fused : 0); k < hf.max_levels; ++k) {
@@ -519,18 +678,6 @@ brdc_status run_forest(brdc_handle h, const HostForest &hf, const Layout &L,
         a.nodes = hf.level_nodes[k];
         a.level_rows = hf.level_rows[k];
         level_view(hf, L, w, k, &a.w);
-        // CTA-role blocks exist only where a merge can exceed kWarpMaxK poles
-        const int cta_blocks = hf.level_mmax[k] > kWarpMaxK ? h->sm_count * 2 : 0;
-        const int grid = cta_blocks + warp_blocks;
-        k_merge<<<(unsigned)elem_grid, 256, 0, s>>>(a, hf.total_n);
-        BRDC_CUDA(h, "brdc.merge", cudaGetLastError());
-        h->launches += 1 + launch_merge_deflate(h, a, hf.level_mmax[k], s);
-        BRDC_CUDA(h, "brdc.merge_deflate", cudaGetLastError());
-        mark(h, 3 + 4 * k);
-        k_secular<<<grid, kSweepThreads, cta_blocks ? smem_tiles(2) : 0, s>>>(a, cta_blocks);
-        BRDC_CUDA(h, "brdc.secular", cudaGetLastError());
-        ++h->launches;
-        mark(h, 4 + 4 * k);
         // rows are needed unless every merge of this level is an instance root
         bool any_inner = false;
         for (int b = 0; b < hf.B; ++b) {
@@ -540,21 +687,18 @@ brdc_status run_forest(brdc_handle h, const HostForest &hf, const Layout &L,
             }
         }
         h->has_lowner[k] = any_inner ? 1 : 0;
-        if (any_inner) {
-            k_lowner<<<grid, kSweepThreads, cta_blocks ? smem_tiles(3) : 0, s>>>(a, cta_blocks);
-            BRDC_CUDA(h, "brdc.lowner", cudaGetLastError());
-            ++h->launches;
+        if (hf.level_mmax[k] <= h->lvl_rows) {
+            h->launches += launch_level_fused(h, hf, a, L.ckpt, s);
+            BRDC_CUDA(h, "brdc.level", cudaGetLastError());
+        } else {
+            k_merge<<<(unsigned)elem_grid, 256, 0, s>>>(a, hf.total_n);
+            BRDC_CUDA(h, "brdc.merge", cudaGetLastError());
+            h->launches += 1 + launch_merge_deflate(h, a, hf.level_mmax[k], s);
+            BRDC_CUDA(h, "brdc.merge_deflate", cudaGetLastError());
+            mark(h, 3 + 4 * k);
+            h->launches += launch_sweeps(h, hf, a, s);
+            BRDC_CUDA(h, "brdc.sweeps", cudaGetLastError());
         }
-        mark(h, 5 + 4 * k);
-        if (any_inner) {
-            k_rows<<<grid, kSweepThreads, cta_blocks ? smem_tiles(4) : 0, s>>>(a, cta_blocks);
-            BRDC_CUDA(h, "brdc.rows", cudaGetLastError());
-            ++h->launches;
-        }
-        k_place<<<(unsigned)elem_grid, 256, 0, s>>>(a, hf.total_n);
-        BRDC_CUDA(h, "brdc.place", cudaGetLastError());
-        ++h->launches;
-        mark(h, 6 + 4 * k);
         std::swap(a.w.cd, a.w.nd);
         std::swap(a.w.cf, a.w.nf);
         std::swap(a.w.cl, a.w.nl);
@@ -616,13 +760,14 @@ extern "C" brdc_status brdc_set_tuning(brdc_handle h, const brdc_tuning *t) {
     }
     const int c = t->deflate_cluster;
     if (t->subtree_levels < -1 || t->subtree_levels > kSubMaxLevels ||
-        !(c == 1 || c == 2 || c == 4 || c == 8) || t->sweep_lanes_target < 1024 ||
-        t->sweep_lanes_target > (1 << 24)) {
+        !(c == 1 || c == 2 || c == 4 || c == 8 || c == 16) || t->sweep_lanes_target < 1024 ||
+        t->sweep_lanes_target > (1 << 24) || t->fused_level_rows < 0) {
         return BRDC_STATUS_INVALID_VALUE;
     }
     h->sub_levels = t->subtree_levels;
     h->defl_cluster = c;
     h->lanes_target = t->sweep_lanes_target;
+    h->lvl_rows = t->fused_level_rows;
     return BRDC_STATUS_SUCCESS;
 }
 
@@ -636,6 +781,7 @@ extern "C" brdc_status brdc_get_tuning(brdc_handle h, brdc_tuning *t) {
     t->subtree_levels = h->sub_levels;
     t->deflate_cluster = h->defl_cluster;
     t->sweep_lanes_target = h->lanes_target;
+    t->fused_level_rows = h->lvl_rows;
     return BRDC_STATUS_SUCCESS;
 }
 
@@ -1019,8 +1165,8 @@ extern "C" brdc_status brdc_autotune(brdc_handle h, int64_t count, const int64_t
         set_error(h, (int)cudaErrorMemoryAllocation, BRDC_ERROR_SRC_CUDA, "brdc.autotune.event");
         return BRDC_STATUS_CUDA_ERROR;
     }
-    const brdc_tuning saved{h->sub_levels, h->defl_cluster, h->lanes_target};
-    brdc_tuning cur{effective_sub_levels(h, hf), h->defl_cluster, h->lanes_target};
+    const brdc_tuning saved{h->sub_levels, h->defl_cluster, h->lanes_target, h->lvl_rows};
+    brdc_tuning cur{effective_sub_levels(h, hf), h->defl_cluster, h->lanes_target, h->lvl_rows};
     int reps = 3;
     // median device time of a few solves under tuning t (first call warms
     // up and, for a new subtree depth, uploads the batch tables)
@@ -1028,6 +1174,7 @@ extern "C" brdc_status brdc_autotune(brdc_handle h, int64_t count, const int64_t
         h->sub_levels = t.subtree_levels;
         h->defl_cluster = t.deflate_cluster;
         h->lanes_target = t.sweep_lanes_target;
+        h->lvl_rows = t.fused_level_rows;
         brdc_status r = brdc_dstebr_batched(h, count, offsets, d_D, d_E, d_W, workspace,
                                             workspace_size);
         if (r != BRDC_STATUS_SUCCESS) {
@@ -1053,26 +1200,36 @@ extern "C" brdc_status brdc_autotune(brdc_handle h, int64_t count, const int64_t
     if (st == BRDC_STATUS_SUCCESS && best_ms > 50.0f) {
         reps = 1; // long solves: one timed run per candidate
     }
-    // coordinate descent: subtree depth, deflation cluster, sweep lanes
+    // coordinate descent, one parameter at a time: subtree depth, fused
+    // levels, deflation cluster, sweep lanes
     const int subs[] = {0, 1, 2, 3, 4, 5};
-    const int clusters[] = {1, 2, 4, 8};
+    const int fuse[] = {0, kLvlRowsPerCta, 1 << 30};
+    const int clusters[] = {1, 2, 4, 8, 16};
     const int lanes[] = {18944, 37888, 75776, 151552, 303104};
-    for (int pass = 0; pass < 3 && st == BRDC_STATUS_SUCCESS; ++pass) {
-        const int *vals = pass == 0 ? subs : (pass == 1 ? clusters : lanes);
-        const int nv = pass == 0 ? 6 : (pass == 1 ? 4 : 5);
-        if (pass == 1 && *std::max_element(hf.level_mmax.begin(), hf.level_mmax.end()) <
-                             2 * kDeflEPT * 1024) {
+    struct Axis {
+        int brdc_tuning::*field;
+        const int *vals;
+        int nv;
+    };
+    const Axis axes[] = {{&brdc_tuning::subtree_levels, subs, 6},
+                         {&brdc_tuning::fused_level_rows, fuse, 3},
+                         {&brdc_tuning::deflate_cluster, clusters, 5},
+                         {&brdc_tuning::sweep_lanes_target, lanes, 5}};
+    const int mmax_all = *std::max_element(hf.level_mmax.begin(), hf.level_mmax.end());
+    for (const Axis &ax : axes) {
+        if (st != BRDC_STATUS_SUCCESS) {
+            break;
+        }
+        if (ax.field == &brdc_tuning::deflate_cluster && mmax_all < 2 * kDeflEPT * 1024) {
             continue; // no merge is large enough for a cluster
         }
         brdc_tuning pick = cur;
-        for (int i = 0; i < nv && st == BRDC_STATUS_SUCCESS; ++i) {
+        for (int i = 0; i < ax.nv && st == BRDC_STATUS_SUCCESS; ++i) {
             brdc_tuning t = cur;
-            int *field = pass == 0 ? &t.subtree_levels
-                                   : (pass == 1 ? &t.deflate_cluster : &t.sweep_lanes_target);
-            if (*field == vals[i]) {
+            if (t.*ax.field == ax.vals[i]) {
                 continue;
             }
-            *field = vals[i];
+            t.*ax.field = ax.vals[i];
             float ms = 0.0f;
             st = run(t, &ms);
             if (st == BRDC_STATUS_SUCCESS && ms < best_ms) {
@@ -1088,11 +1245,13 @@ extern "C" brdc_status brdc_autotune(brdc_handle h, int64_t count, const int64_t
         h->sub_levels = saved.subtree_levels;
         h->defl_cluster = saved.deflate_cluster;
         h->lanes_target = saved.sweep_lanes_target;
+        h->lvl_rows = saved.fused_level_rows;
         return st;
     }
     h->sub_levels = cur.subtree_levels;
     h->defl_cluster = cur.deflate_cluster;
     h->lanes_target = cur.sweep_lanes_target;
+    h->lvl_rows = cur.fused_level_rows;
     if (best != nullptr) {
         *best = cur;
     }

@@ -65,7 +65,9 @@ struct LevelCtl {
     int items_w;     // warp work items of the level
     int items_c;     // CTA work items of the level
     int total_k;
-    int pad;
+    int nbig;        // merges k_level left to the sweep kernels (K > kLvlMaxK)
+    unsigned bar_count; // grid barrier of k_sweeps: arrivals, generation
+    unsigned bar_gen;
 };
 
 struct WsHeader {
@@ -88,6 +90,7 @@ enum DeviceError : int {
     kErrNone = 0,
     kErrBarrierTimeout = 1,
     kErrBadGeometry = 2,
+    kErrGridBarrierTimeout = 3,
 };
 
 // Forest description passed by value to every kernel.

@@ -40,6 +40,8 @@ struct KArgs {
     long long level_rows; // rows of the instances that merge at this level
     int plan_inline;    // the last deflation CTA writes the level plan (else k_plan)
     int lanes_target;   // threads the root sweeps aim to keep busy
+    int big_k;          // > 0: the plan and the placement serve only nodes with
+                        // K > big_k (k_level finished the others)
 };
 
 // ------------------------------------------------------------------ leaves
@@ -340,18 +342,20 @@ template <int T>
 __device__ void level_plan(const KArgs &a, double *red, int *iscan) {
     const Ws &w = a.w;
     double tkw = 0.0, tkc = 0.0, cw = 0.0, cc = 0.0;
-    double skz = 0.0, sk2 = 0.0, kmax = 0.0;
+    double skz = 0.0, sk = 0.0, sk2 = 0.0, kmax = 0.0;
     for (int i = threadIdx.x; i < a.nodes; i += T) {
         const int kk = __ldcg(w.nK + i);
         const int kz = __ldcg(w.nKz + i);
-        if (kk > kWarpMaxK) {
+        // nodes with K <= big_k get no items (finished by k_level, or empty)
+        if (kk > a.big_k && kk > kWarpMaxK) {
             tkc += kk;
             cc += 1.0;
-        } else if (kk > 0) {
+        } else if (kk > a.big_k) {
             tkw += kk;
             cw += 1.0;
         }
         skz += kz;
+        sk += kk;
         sk2 += (double)kk * (double)kk;
         kmax = fmax(kmax, (double)kk);
     }
@@ -360,6 +364,7 @@ __device__ void level_plan(const KArgs &a, double *red, int *iscan) {
     cw = block_sum<T>(cw, red);
     cc = block_sum<T>(cc, red);
     skz = block_sum<T>(skz, red);
+    sk = block_sum<T>(sk, red);
     sk2 = block_sum<T>(sk2, red);
     kmax = block_max<T>(kmax, red);
     if (threadIdx.x == 0) {
@@ -369,7 +374,7 @@ __device__ void level_plan(const KArgs &a, double *red, int *iscan) {
         dg->merge_count = a.nodes;
         dg->size_sum = (int)(a.level_rows);
         dg->dd_before_sum = (int)skz;
-        dg->dd_after_sum = (int)(tkw + tkc);
+        dg->dd_after_sum = (int)(sk);
         dg->dd_after_max = (int)kmax;
         dg->dd_after_sq_sum = (long long)sk2;
     }
@@ -402,9 +407,9 @@ __device__ void level_plan(const KArgs &a, double *red, int *iscan) {
     int sw = 0, sc = 0;
     for (int i = i0; i < i1; ++i) {
         const int kk = __ldcg(w.nK + i);
-        if (kk > kWarpMaxK) {
+        if (kk > a.big_k && kk > kWarpMaxK) {
             sc += (kk + Rc - 1) / Rc;
-        } else {
+        } else if (kk > a.big_k) {
             sw += (kk + Rw - 1) / Rw;
         }
     }
@@ -415,9 +420,9 @@ __device__ void level_plan(const KArgs &a, double *red, int *iscan) {
         const int kk = __ldcg(w.nK + i);
         w.pref_w[i] = rw;
         w.pref_c[i] = rc;
-        if (kk > kWarpMaxK) {
+        if (kk > a.big_k && kk > kWarpMaxK) {
             rc += (kk + Rc - 1) / Rc;
-        } else {
+        } else if (kk > a.big_k) {
             rw += (kk + Rw - 1) / Rw;
         }
     }
@@ -1125,10 +1130,13 @@ __device__ inline int block_role_setup(uint64_t *bars) {
 // merges (8 warps per block, each on its own work item).
 constexpr int kWarpsPerBlock = kSweepThreads / 32;
 
-__global__ void __launch_bounds__(kSweepThreads)
-    k_secular(KArgs a, int cta_blocks) {
-    extern __shared__ __align__(16) double smem[];
-    __shared__ __align__(8) uint64_t bars[2];
+// The phases below are device functions over the grid's two roles, run by
+// their own kernels (k_secular, k_lowner, k_rows, k_place) or back to back
+// by k_sweeps.  CTA-role blocks set up their two mbarriers once (ph holds
+// their phase bits across phases).  Each returns false after a barrier
+// timeout (recorded in the workspace status).
+__device__ bool sweep_secular(const KArgs &a, int cta_blocks, double *smem, uint64_t *bars,
+                              unsigned *ph) {
     const Ws &w = a.w;
     const LevelCtl *ctl = &w.hdr->lvl[a.k];
     const double eps = DBL_EPSILON;
@@ -1189,11 +1197,9 @@ __global__ void __launch_bounds__(kSweepThreads)
             }
             secular_diag_warp(w, a.k, active && l == 0, st);
         }
-        return;
+        return true;
     }
 
-    block_role_setup(bars);
-    unsigned ph[2] = {0u, 0u};
     const int tpr = ctl->tpr_c;
     const int R = kSweepThreads / tpr;
     const int items = ctl->items_c;
@@ -1251,7 +1257,7 @@ __global__ void __launch_bounds__(kSweepThreads)
         ph[1] = ts.phase[1];
         if (!ok) {
             record_error(w.hdr, kErrBarrierTimeout);
-            return;
+            return false;
         }
         if (active && lane == 0) {
             secular_store(w, a, po, r, st);
@@ -1259,6 +1265,18 @@ __global__ void __launch_bounds__(kSweepThreads)
         secular_diag_warp(w, a.k, active && lane == 0, st);
         __syncthreads();
     }
+    return true;
+}
+
+__global__ void __launch_bounds__(kSweepThreads)
+    k_secular(KArgs a, int cta_blocks) {
+    extern __shared__ __align__(16) double smem[];
+    __shared__ __align__(8) uint64_t bars[2];
+    unsigned ph[2] = {0u, 0u};
+    if ((int)blockIdx.x < cta_blocks) {
+        block_role_setup(bars);
+    }
+    sweep_secular(a, cta_blocks, smem, bars, ph);
 }
 
 // ------------------------------------------------------------- Loewner z
@@ -1267,10 +1285,9 @@ __global__ void __launch_bounds__(kSweepThreads)
 // recomputation of cpu/src/dlaed9_br.f:181-266 (WPROD), one lane group per
 // pole sweeping the roots.  Instance roots are skipped (no parent reads
 // their rows).
-__global__ void __launch_bounds__(kSweepThreads)
-    k_lowner(KArgs a, int cta_blocks) {
-    extern __shared__ __align__(16) double smem[];
-    __shared__ __align__(8) uint64_t bars[2];
+// (rdo and rtau are read through L2: k_sweeps writes them in the same launch.)
+__device__ bool sweep_lowner(const KArgs &a, int cta_blocks, double *smem, uint64_t *bars,
+                             unsigned *ph) {
     const Ws &w = a.w;
     const LevelCtl *ctl = &w.hdr->lvl[a.k];
 
@@ -1303,15 +1320,15 @@ __global__ void __launch_bounds__(kSweepThreads)
 #pragma unroll 2
                 for (; j + tpr < K; j += 2 * tpr) {
                     const int j2 = j + tpr;
-                    const double dl = (di - __ldg(rdo + j)) - __ldg(rtau + j);
-                    const double dl2 = (di - __ldg(rdo + j2)) - __ldg(rtau + j2);
+                    const double dl = (di - __ldcg(rdo + j)) - __ldcg(rtau + j);
+                    const double dl2 = (di - __ldcg(rdo + j2)) - __ldcg(rtau + j2);
                     const double q = brdc_rcp(j == i ? 1.0 : di - __ldg(pd + j));
                     const double q2 = brdc_rcp(j2 == i ? 1.0 : di - __ldg(pd + j2));
                     prod *= dl * q;
                     prod2 *= dl2 * q2;
                 }
                 if (j < K) {
-                    const double dl = (di - __ldg(rdo + j)) - __ldg(rtau + j);
+                    const double dl = (di - __ldcg(rdo + j)) - __ldcg(rtau + j);
                     prod *= dl * brdc_rcp(j == i ? 1.0 : di - __ldg(pd + j));
                 }
             }
@@ -1320,11 +1337,9 @@ __global__ void __launch_bounds__(kSweepThreads)
                 w.pw[po + i] = lowner_value(w, po, i, prod, w.nrho[g]);
             }
         }
-        return;
+        return true;
     }
 
-    block_role_setup(bars);
-    unsigned ph[2] = {0u, 0u};
     const int tpr = ctl->tpr_c;
     const int R = kSweepThreads / tpr;
     const int items = ctl->items_c;
@@ -1368,7 +1383,7 @@ __global__ void __launch_bounds__(kSweepThreads)
         ph[1] = ts.phase[1];
         if (!ok) {
             record_error(w.hdr, kErrBarrierTimeout);
-            return;
+            return false;
         }
         prod = group_prod(prod * prod2, tpr);
         if (active && lane == 0) {
@@ -1376,6 +1391,18 @@ __global__ void __launch_bounds__(kSweepThreads)
         }
         __syncthreads();
     }
+    return true;
+}
+
+__global__ void __launch_bounds__(kSweepThreads)
+    k_lowner(KArgs a, int cta_blocks) {
+    extern __shared__ __align__(16) double smem[];
+    __shared__ __align__(8) uint64_t bars[2];
+    unsigned ph[2] = {0u, 0u};
+    if ((int)blockIdx.x < cta_blocks) {
+        block_role_setup(bars);
+    }
+    sweep_lowner(a, cta_blocks, smem, bars, ph);
 }
 
 // ----------------------------------------------------------- boundary rows
@@ -1383,10 +1410,10 @@ __global__ void __launch_bounds__(kSweepThreads)
 // new last row = sum_i l_i u_i: the streamed update of
 // cpu/src/dlaed9_br.f:272-334 with the compact delta.  Written to rf/rl;
 // k_place puts them in order.
-__global__ void __launch_bounds__(kSweepThreads)
-    k_rows(KArgs a, int cta_blocks) {
-    extern __shared__ __align__(16) double smem[];
-    __shared__ __align__(8) uint64_t bars[2];
+// (rdo, rtau and pw are read through L2: k_sweeps writes them in the same
+// launch.)
+__device__ bool sweep_rows(const KArgs &a, int cta_blocks, double *smem, uint64_t *bars,
+                           unsigned *ph) {
     const Ws &w = a.w;
     const LevelCtl *ctl = &w.hdr->lvl[a.k];
 
@@ -1410,8 +1437,8 @@ __global__ void __launch_bounds__(kSweepThreads)
             const bool root = s < K;
             double a1 = 0.0, a2 = 0.0, s2 = 0.0;
             if (root) {
-                const double dorg = w.rdo[po + s];
-                const double tau = w.rtau[po + s];
+                const double dorg = __ldcg(w.rdo + po + s);
+                const double tau = __ldcg(w.rtau + po + s);
                 const double *pd = w.pd + po;
                 const double *pw = w.pw + po;
                 const double *pf = w.pf + po;
@@ -1419,7 +1446,7 @@ __global__ void __launch_bounds__(kSweepThreads)
 #pragma unroll 4
                 for (int i = l; i < K; i += tpr) {
                     const double dl = (__ldg(pd + i) - dorg) - tau;
-                    const double u = (dl != 0.0) ? __ldg(pw + i) * brdc_rcp(dl) : 0.0;
+                    const double u = (dl != 0.0) ? __ldcg(pw + i) * brdc_rcp(dl) : 0.0;
                     s2 += u * u;
                     a1 += __ldg(pf + i) * u;
                     a2 += __ldg(pl + i) * u;
@@ -1434,11 +1461,9 @@ __global__ void __launch_bounds__(kSweepThreads)
                 w.rl[po + s] = nrm > 0.0 ? a2 / nrm : 0.0;
             }
         }
-        return;
+        return true;
     }
 
-    block_role_setup(bars);
-    unsigned ph[2] = {0u, 0u};
     const int tpr = ctl->tpr_c;
     const int R = kSweepThreads / tpr;
     const int items = ctl->items_c;
@@ -1453,8 +1478,8 @@ __global__ void __launch_bounds__(kSweepThreads)
         const long long po = G.poff;
         const int s = (item - w.pref_c[g]) * R + grp;
         const bool root = s < K;
-        const double dorg = root ? w.rdo[po + s] : 0.0;
-        const double tau = root ? w.rtau[po + s] : 0.0;
+        const double dorg = root ? __ldcg(w.rdo + po + s) : 0.0;
+        const double tau = root ? __ldcg(w.rtau + po + s) : 0.0;
         double a1 = 0.0, a2 = 0.0, s2 = 0.0;
         TileSet<4> ts;
         const double *srcs[4] = {w.pd, w.pw, w.pf, w.pl};
@@ -1476,7 +1501,7 @@ __global__ void __launch_bounds__(kSweepThreads)
         ph[1] = ts.phase[1];
         if (!ok) {
             record_error(w.hdr, kErrBarrierTimeout);
-            return;
+            return false;
         }
         s2 = group_sum(s2, tpr);
         a1 = group_sum(a1, tpr);
@@ -1488,6 +1513,18 @@ __global__ void __launch_bounds__(kSweepThreads)
         }
         __syncthreads();
     }
+    return true;
+}
+
+__global__ void __launch_bounds__(kSweepThreads)
+    k_rows(KArgs a, int cta_blocks) {
+    extern __shared__ __align__(16) double smem[];
+    __shared__ __align__(8) uint64_t bars[2];
+    unsigned ph[2] = {0u, 0u};
+    if ((int)blockIdx.x < cta_blocks) {
+        block_role_setup(bars);
+    }
+    sweep_rows(a, cta_blocks, smem, bars, ph);
 }
 
 // --------------------------------------------------------------- placement
@@ -1496,7 +1533,7 @@ __global__ void __launch_bounds__(kSweepThreads)
 // spectrum by rank among the three sorted lists (ties: roots, then small-z,
 // then rotated), with its first and last boundary-row entries; instance
 // roots write the final eigenvalues to W.
-__global__ void __launch_bounds__(256) k_place(KArgs a, long long total_n) {
+__device__ void place_rows(const KArgs &a, long long total_n) {
     const Ws &w = a.w;
     for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x; x < total_n;
          x += (long long)gridDim.x * blockDim.x) {
@@ -1508,6 +1545,9 @@ __global__ void __launch_bounds__(256) k_place(KArgs a, long long total_n) {
         const long long po = (gs + g + 1) & ~1LL;
         const int s = (int)(x - gs);
         const int K = w.nK[g];
+        if (K <= a.big_k && a.big_k > 0) {
+            continue; // placed by k_level
+        }
         const int Kz = w.nKz[g];
         const int ndz = m - Kz, ndg = Kz - K;
         const bool top = (depth == 0);
@@ -1517,11 +1557,11 @@ __global__ void __launch_bounds__(256) k_place(KArgs a, long long total_n) {
         double val, fo = 0.0, lo = 0.0;
         int pos;
         if (s < K) {
-            val = rl[s];
+            val = __ldcg(rl + s);
             pos = s + lower_bound_d(zdl, ndz, val) + lower_bound_d(gdl, ndg, val);
             if (!top) {
-                fo = w.rf[po + s];
-                lo = w.rl[po + s];
+                fo = __ldcg(w.rf + po + s);
+                lo = __ldcg(w.rl + po + s);
             }
         } else if (s < K + ndz) {
             const int q = s - K;
@@ -1544,6 +1584,99 @@ __global__ void __launch_bounds__(256) k_place(KArgs a, long long total_n) {
             w.nf[o] = fo;
             w.nl[o] = lo;
         }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_place(KArgs a, long long total_n) {
+    place_rows(a, total_n);
+}
+
+// ------------------------------------------------------------ k_sweeps
+// Grid-wide barrier of a cooperative launch (every block resident), on the
+// level's counter pair: arrivals, then a generation bump by the last block.
+// The wait is bounded (kGridBarrierNs); on timeout the status records it and
+// the caller leaves.
+constexpr unsigned long long kGridBarrierNs = 20ull * 1000ull * 1000ull * 1000ull;
+
+__device__ inline unsigned long long globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ inline bool grid_barrier(WsHeader *h, LevelCtl *c) {
+    __syncthreads();
+    int ok = 1;
+    if (threadIdx.x == 0) {
+        volatile unsigned *gen = &c->bar_gen;
+        const unsigned g = *gen; // before arriving: the last arrival bumps it
+        __threadfence();
+        if (atomicAdd(&c->bar_count, 1u) + 1u == gridDim.x) {
+            c->bar_count = 0u;
+            __threadfence();
+            atomicAdd(&c->bar_gen, 1u);
+        } else {
+            const unsigned long long t0 = globaltimer_ns();
+            while (*gen == g) {
+                __nanosleep(100);
+                if (globaltimer_ns() - t0 > kGridBarrierNs) {
+                    ok = 0;
+                    record_error(h, kErrGridBarrierTimeout);
+                    break;
+                }
+            }
+        }
+        __threadfence();
+    }
+    return __syncthreads_and(ok) != 0;
+}
+
+// Roots, Loewner weights, boundary rows and placement of one level in one
+// cooperative launch: the four phases above separated by grid barriers
+// instead of kernel boundaries.  After k_level (big_k > 0) it returns at
+// once when the level plan has no items: k_level finished every merge.
+// The roles split the grid by the plan: all blocks to the role that has
+// items when only one has, half each otherwise (`tiles` = 0: the launch has
+// no tile memory and every block takes the warp role).  `rows` = 0 skips the
+// Loewner and rows phases (every merge an instance root).
+__global__ void __launch_bounds__(kSweepThreads)
+    k_sweeps(KArgs a, int tiles, int rows, long long total_n) {
+    extern __shared__ __align__(16) double smem[];
+    __shared__ __align__(8) uint64_t bars[2];
+    WsHeader *h = a.w.hdr;
+    LevelCtl *ctl = &h->lvl[a.k];
+    const int iw = __ldcg(&ctl->items_w), ic = __ldcg(&ctl->items_c);
+    if (a.big_k > 0 && iw + ic == 0) {
+        return;
+    }
+    const int cta_blocks = (!tiles || ic == 0) ? 0 : (iw == 0 ? (int)gridDim.x
+                                                              : (int)gridDim.x / 2);
+    unsigned ph[2] = {0u, 0u};
+    if ((int)blockIdx.x < cta_blocks) {
+        block_role_setup(bars);
+    }
+    // a block whose tile wait timed out skips its work but keeps to the
+    // barriers, so the others do not wait for it
+    bool ok = sweep_secular(a, cta_blocks, smem, bars, ph);
+    if (!grid_barrier(h, ctl)) {
+        return;
+    }
+    if (rows) {
+        if (ok) {
+            ok = sweep_lowner(a, cta_blocks, smem, bars, ph);
+        }
+        if (!grid_barrier(h, ctl)) {
+            return;
+        }
+        if (ok) {
+            ok = sweep_rows(a, cta_blocks, smem, bars, ph);
+        }
+        if (!grid_barrier(h, ctl)) {
+            return;
+        }
+    }
+    if (ok) {
+        place_rows(a, total_n);
     }
 }
 
@@ -1612,6 +1745,9 @@ __global__ void k_init(WsHeader *h, int levels, int B, long long total_n,
         h->lvl[k].items_w = 0;
         h->lvl[k].items_c = 0;
         h->lvl[k].total_k = 0;
+        h->lvl[k].nbig = 0;
+        h->lvl[k].bar_count = 0u;
+        h->lvl[k].bar_gen = 0u;
         brdc_level_diagnostics z = {};
         z.level = k;
         h->diag[k] = z;

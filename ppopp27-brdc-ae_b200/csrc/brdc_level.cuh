@@ -1,0 +1,591 @@
+// brdc_level.cuh -- one merge level in one kernel.
+//
+// Above the subtree kernel the merges are few and large (a few thousand
+// rows to the whole matrix), but for spectra that deflate heavily they
+// leave only a few hundred poles each, and the per-level kernels spend a
+// level on launches and global round trips -- short chains of dependent
+// latencies.  k_level runs every step of a level for one merge node in a
+// cluster of C CTAs (C = 1 allowed):
+//   rank merge of the two children (sorted lists staged in shared memory),
+//   deflation (the phases of k_merge_deflate / k_merge_deflate_cl),
+//   secular roots, Loewner weights and boundary rows of the K <= kLvlMaxK
+//   poles in shared memory, the roots split over the cluster's CTAs and the
+//   results gathered through distributed shared memory,
+//   placement.
+// Every rule is the per-level kernels' own (deflation tests, compaction
+// order, rotations, the secular state machine, tie order of the placement),
+// so deflation and placement decide exactly as they do; only the lanes that
+// share a root's sweep differ, which moves the sums' rounding.  A node with
+// more than kLvlMaxK poles stops after its deflation and is counted in the
+// level's nbig; the last CTA then builds the level plan for exactly those
+// nodes (big_k = kLvlMaxK), and k_sweeps finishes them (it returns at once
+// when there are none).  Every write lands where the per-level kernels put
+// it, so the workspace slices of a checkpointed solve serve the adjoint
+// unchanged.
+#pragma once
+
+#include "brdc_kernels.cuh"
+
+namespace brdc {
+
+constexpr int kLvlThreads = 512;
+constexpr int kLvlMaxK = 1024;       // poles a node takes through the roots in shared memory
+constexpr int kLvlSamples = 4096;    // samples of a sorted list staged in shared memory
+constexpr int kLvlRowsPerCta = 4096; // merge rows per CTA the launch aims at
+constexpr int kLvlBatch = 4;         // rows a thread moves per pass (loads issued together)
+
+struct LvlSmem {
+    double pd[kLvlMaxK], pz[kLvlMaxK], pf[kLvlMaxK], pl[kLvlMaxK], pw[kLvlMaxK];
+    double rdo[kLvlMaxK], rtau[kLvlMaxK];
+    union {
+        double stage[2 * kLvlSamples];   // staged sorted lists (merge, placement)
+        SecDyn dyn[kLvlMaxK];            // parked secular state between sweeps
+    } u;
+    int wl[2][kLvlThreads / 32][kLvlMaxK / (kLvlThreads / 32)]; // live roots per warp
+    double red[32];
+    int iscan[32];
+    double s_val;                        // cluster exchange
+    int s_cnt;
+    int s_last;
+};
+
+// A sorted list in global memory with every Q-th element staged in shared
+// memory.  A bound takes a binary search of the samples, then one scan of
+// the (Q-1)-element window between two samples, so it is exact.
+struct StagedList {
+    const double *g; // the list
+    const double *s; // s[i] = g[i Q]
+    int n, Q, ns;
+};
+
+template <int T>
+__device__ inline StagedList stage_list(double *dst, const double *g, int n) {
+    StagedList L;
+    L.g = g;
+    L.s = dst;
+    L.n = n;
+    L.Q = n <= kLvlSamples ? 1 : (n + kLvlSamples - 1) / kLvlSamples;
+    L.ns = (n + L.Q - 1) / L.Q;
+    for (int i = threadIdx.x; i < L.ns; i += T) {
+        dst[i] = g[(long long)i * L.Q];
+    }
+    return L;
+}
+
+// Step 1 of a bound: samples that pass (< v, or <= v for UPPER).
+template <bool UPPER>
+__device__ inline int staged_coarse(const StagedList &L, double v) {
+    return UPPER ? upper_bound_d(L.s, L.ns, v) : lower_bound_d(L.s, L.ns, v);
+}
+
+// Step 2: elements that pass.  g[(c-1)Q] passes and g[cQ] (if any) fails,
+// so only the window between them is read.
+template <bool UPPER>
+__device__ inline int staged_fine(const StagedList &L, int c, double v) {
+    if (L.Q == 1 || c == 0) {
+        return c * L.Q < L.n ? c * L.Q : L.n;
+    }
+    const int lo = (c - 1) * L.Q + 1;
+    const int hi = c * L.Q < L.n ? c * L.Q : L.n;
+    int cnt = lo;
+    if (L.Q <= 8) {
+        double t[7];
+#pragma unroll
+        for (int q = 0; q < 7; ++q) {
+            t[q] = lo + q < hi ? L.g[lo + q] : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < 7; ++q) {
+            cnt += (lo + q < hi) && (UPPER ? t[q] <= v : t[q] < v);
+        }
+        return cnt;
+    }
+    for (int j = lo; j < hi; ++j) {
+        cnt += UPPER ? (L.g[j] <= v) : (L.g[j] < v);
+    }
+    return cnt;
+}
+
+// Roots, Loewner weights and boundary rows of one node with 1 <= K <=
+// kLvlMaxK poles, by all C CTAs of its cluster: CTA r takes the roots (and
+// poles) [r P, (r+1) P), P = ceil(K / C), and gathers the others' from their
+// shared memory.  Results go to the workspace where k_secular, k_lowner and
+// k_rows put them; on return every CTA holds all rdo/rtau.  The caller ends
+// with a cluster barrier, after which no CTA reads a peer's shared memory.
+template <int T>
+__device__ void level_roots(LvlSmem &S, cooperative_groups::cluster_group &cl, const KArgs &a,
+                            const NodeGeom &G, int K, double rho, double zn, int C, int rank) {
+    const Ws &w = a.w;
+    const long long po = G.poff;
+    const int x = threadIdx.x, lane = x & 31;
+    const double eps = DBL_EPSILON;
+    for (int i = x; i < K; i += T) {
+        S.pd[i] = w.pd[po + i];
+        S.pz[i] = w.pz[po + i];
+        S.pf[i] = w.pf[po + i];
+        S.pl[i] = w.pl[po + i];
+    }
+    __syncthreads();
+    const int P = (K + C - 1) / C;
+    const int r0 = min(K, rank * P), r1 = min(K, r0 + P);
+    if (K == 1) {
+        if (rank == 0 && x == 0) {
+            const double t = rho * S.pz[0] * S.pz[0];
+            S.rdo[0] = S.pd[0];
+            S.rtau[0] = t;
+            w.rorg[po] = 0;
+            w.rdo[po] = S.pd[0];
+            w.rtau[po] = t;
+            w.rlam[po] = S.pd[0] + t;
+        }
+    } else if (r1 > r0) {
+        // Each warp takes a contiguous share of the CTA's roots and sweeps
+        // them in rounds: after every sweep it packs its live roots into a
+        // list and spreads them over its lanes (the largest power-of-two
+        // lane count per root that fits), so converged roots free their
+        // lanes for the slow ones.  Between sweeps a root's state is parked
+        // in shared memory; a warp synchronises only with itself.
+        constexpr int NW = T / 32;
+        const int warp = x >> 5;
+        const int nmine = r1 - r0;
+        const int pw_ = (nmine + NW - 1) / NW;
+        const int q0 = min(nmine, warp * pw_), q1 = min(nmine, q0 + pw_);
+        int *la = S.wl[0][warp], *lb = S.wl[1][warp];
+        int nlive = q1 - q0;
+        for (int i = lane; i < nlive; i += 32) {
+            const int r = r0 + q0 + i;
+            SecRoot st;
+            sec_init(st, r, K, S.pd, S.pz, rho, zn);
+            sec_park(st, S.u.dyn[r]);
+            la[i] = r;
+        }
+        __syncwarp();
+        int its = 0, itm = 0, itf = 0;
+        while (nlive > 0) {
+            int tp = 1;
+            while (tp < 32 && nlive * tp * 2 <= 32) {
+                tp <<= 1;
+            }
+            const int gpw = 32 / tp, l2 = lane & (tp - 1);
+            int nn = 0;
+            for (int base = 0; base < nlive; base += gpw) {
+                const int gi = base + lane / tp;
+                const bool act = gi < nlive;
+                const int id = act ? la[gi] : 0;
+                SecRoot st;
+                if (act) {
+                    sec_init_static(st, id, K, S.pd, S.pz, rho, zn);
+                    sec_unpark(st, S.u.dyn[id]);
+                } else {
+                    st.stage = 2;
+                }
+                SecSums sum;
+                sec_zero(sum);
+                if (act) {
+                    const int pmin = id < K - 2 ? id : K - 2;
+                    secular_span(sum, st, 0, K, l2, tp, pmin, id + 1,
+                                 [&](int u, double *du, double *zu) {
+                                     *du = S.pd[u];
+                                     *zu = S.pz[u];
+                                 });
+                }
+                sums_reduce(sum, tp);
+                if (act) {
+                    sec_after_sweep(st, sum, eps);
+                }
+                const bool lead = act && l2 == 0;
+                const bool more = lead && st.stage != 2;
+                if (more) {
+                    sec_park(st, S.u.dyn[id]);
+                } else if (lead) {
+                    S.rdo[id] = st.dorg;
+                    S.rtau[id] = st.tau;
+                    w.rorg[po + id] = st.org;
+                    w.rdo[po + id] = st.dorg;
+                    w.rtau[po + id] = st.tau;
+                    w.rlam[po + id] = st.dorg + st.tau;
+                    its += st.iter;
+                    itm = max(itm, st.iter);
+                    itf += st.failed;
+                }
+                const unsigned mb = __ballot_sync(kFull, more);
+                if (more) {
+                    lb[nn + __popc(mb & ((1u << lane) - 1u))] = id;
+                }
+                nn += __popc(mb);
+            }
+            __syncwarp();
+            int *t = la;
+            la = lb;
+            lb = t;
+            nlive = nn;
+        }
+        // iteration counters, one warp at a time
+        its = __reduce_add_sync(kFull, its);
+        itm = __reduce_max_sync(kFull, itm);
+        itf = __reduce_add_sync(kFull, itf);
+        if (lane == 0 && its != 0) {
+            brdc_level_diagnostics *dg = &w.hdr->diag[a.k];
+            atomicAdd(&dg->secular_iter_sum, its);
+            atomicMax(&dg->secular_iter_max, itm);
+            if (itf != 0) {
+                atomicAdd(&dg->secular_iter_failed, itf);
+                atomicAdd(&w.hdr->nonconv, itf);
+            }
+        }
+    }
+    // every CTA: the other CTAs' roots
+    cl.sync();
+    for (int i = x; i < K; i += T) {
+        const int owner = i / P;
+        if (owner != rank) {
+            S.rdo[i] = *cl.map_shared_rank(&S.rdo[i], owner);
+            S.rtau[i] = *cl.map_shared_rank(&S.rtau[i], owner);
+        }
+    }
+    __syncthreads();
+    if (G.depth == 0) {
+        return; // an instance root: no parent reads its rows
+    }
+
+    // Loewner weights (sqrt(rho) z) of this CTA's poles, tpr lanes per pole
+    const int nmine = r1 - r0;
+    int tpr = 1;
+    while (tpr < 32 && nmine * tpr * 2 <= T) {
+        tpr <<= 1;
+    }
+    const int per = T / tpr, gl = x & (tpr - 1);
+    for (int base = 0; base < nmine; base += per) {
+        const int i = r0 + base + x / tpr;
+        double prod = 1.0, prod2 = 1.0;
+        if (i < r1) {
+            const double di = S.pd[i];
+            int q = gl;
+            for (; q + tpr < K; q += 2 * tpr) {
+                const int q2 = q + tpr;
+                const double dl = (di - S.rdo[q]) - S.rtau[q];
+                const double dl2 = (di - S.rdo[q2]) - S.rtau[q2];
+                prod *= dl * brdc_rcp(q == i ? 1.0 : di - S.pd[q]);
+                prod2 *= dl2 * brdc_rcp(q2 == i ? 1.0 : di - S.pd[q2]);
+            }
+            if (q < K) {
+                const double dl = (di - S.rdo[q]) - S.rtau[q];
+                prod *= dl * brdc_rcp(q == i ? 1.0 : di - S.pd[q]);
+            }
+        }
+        prod = group_prod(prod * prod2, tpr);
+        if (i < r1 && gl == 0) {
+            const double zi = S.pz[i];
+            const double mag = sqrt(fmax(-prod, 0.0));
+            double wi = zi < 0.0 ? -mag : mag;
+            if (!(mag > 0.0) || !isfinite(mag)) {
+                wi = zi * sqrt(rho);
+            }
+            S.pw[i] = wi;
+            w.pw[po + i] = wi;
+        }
+    }
+    cl.sync();
+    for (int i = x; i < K; i += T) {
+        const int owner = i / P;
+        if (owner != rank) {
+            S.pw[i] = *cl.map_shared_rank(&S.pw[i], owner);
+        }
+    }
+    __syncthreads();
+
+    // boundary rows of this CTA's roots, tpr lanes per root
+    for (int base = 0; base < nmine; base += per) {
+        const int r = r0 + base + x / tpr;
+        double a1 = 0.0, a2 = 0.0, s2 = 0.0;
+        if (r < r1) {
+            const double dorg = S.rdo[r], tau = S.rtau[r];
+            for (int i = gl; i < K; i += tpr) {
+                const double dl = (S.pd[i] - dorg) - tau;
+                const double u = (dl != 0.0) ? S.pw[i] * brdc_rcp(dl) : 0.0;
+                s2 += u * u;
+                a1 += S.pf[i] * u;
+                a2 += S.pl[i] * u;
+            }
+        }
+        s2 = group_sum(s2, tpr);
+        a1 = group_sum(a1, tpr);
+        a2 = group_sum(a2, tpr);
+        if (r < r1 && gl == 0) {
+            const double nrm = sqrt(s2);
+            w.rf[po + r] = nrm > 0.0 ? a1 / nrm : 0.0;
+            w.rl[po + r] = nrm > 0.0 ? a2 / nrm : 0.0;
+        }
+    }
+}
+
+// The level plan for the merges k_level leaves to k_sweeps: taken by the
+// last CTA of the launch (every node's scalars are written before its CTAs
+// take their tickets), and only when there are such merges.
+template <int T>
+__device__ void level_ticket(const KArgs &a, LvlSmem &S) {
+    if (!a.plan_inline) {
+        return; // k_plan runs after the launch
+    }
+    LevelCtl *c = &a.w.hdr->lvl[a.k];
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const int t = atomicAdd(&c->ticket, 1);
+        S.s_last = (t == (int)gridDim.x - 1) && (atomicAdd(&c->nbig, 0) > 0);
+    }
+    __syncthreads();
+    if (S.s_last) {
+        __threadfence();
+        level_plan<T>(a, S.red, S.iscan);
+    }
+}
+
+// One merge level, a cluster of C CTAs per node.  CTA r of the cluster
+// merges and places the rows [r SE, (r+1) SE) and deflates its share as
+// k_merge_deflate_cl does.
+template <int T>
+__global__ void __launch_bounds__(T, 1) k_level(KArgs a) {
+    namespace cg = cooperative_groups;
+    extern __shared__ __align__(16) unsigned char lvl_raw[];
+    LvlSmem &S = *reinterpret_cast<LvlSmem *>(lvl_raw);
+    cg::cluster_group cl = cg::this_cluster();
+    const int C = (int)cl.num_blocks();
+    const int rank = (int)cl.block_rank();
+    const int g = blockIdx.x / C;
+    const NodeGeom G = node_geom(a.F, a.k, g);
+    const Ws &w = a.w;
+    const long long gs = G.gstart;
+    const int m = G.m, m1 = G.m1, m2 = m - m1;
+    const int x = threadIdx.x;
+    constexpr int chunk = kDeflEPT * T;
+    constexpr int B = kLvlBatch;
+    const double isq2 = 0.70710678118654752440;
+    double rho, maxd;
+    defl_node_scalars(a, G, &rho, &maxd);
+
+    // ------------------------------------------------ rank merge
+    // (left wins ties), as k_merge; max|z| on the way
+    const StagedList LA = stage_list<T>(S.u.stage, w.cd + gs, m1);
+    const StagedList LB = stage_list<T>(S.u.stage + kLvlSamples, w.cd + gs + m1, m2);
+    __syncthreads();
+    const int SE = (m + C - 1) / C;
+    const int e0 = min(m, rank * SE), e1 = min(m, e0 + SE);
+    double lz = 0.0;
+    for (int e = e0 + x; e < e1; e += B * T) {
+        double v[B], z[B], f[B], l[B];
+        int c[B];
+#pragma unroll
+        for (int u = 0; u < B; ++u) {
+            const int ee = e + u * T < e1 ? e + u * T : e;
+            const bool left = ee < m1;
+            v[u] = w.cd[gs + ee];
+            const double r = left ? w.cl[gs + ee] : w.cf[gs + ee];
+            z[u] = r * isq2;
+            f[u] = left ? w.cf[gs + ee] : 0.0;
+            l[u] = left ? 0.0 : w.cl[gs + ee];
+        }
+#pragma unroll
+        for (int u = 0; u < B; ++u) {
+            const int ee = e + u * T;
+            c[u] = ee < m1 ? staged_coarse<false>(LB, v[u]) : staged_coarse<true>(LA, v[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < B; ++u) {
+            const int ee = e + u * T;
+            if (ee < e1) {
+                const int pos = ee < m1 ? ee + staged_fine<false>(LB, c[u], v[u])
+                                        : (ee - m1) + staged_fine<true>(LA, c[u], v[u]);
+                const long long o = gs + pos;
+                w.md[o] = v[u];
+                w.mz[o] = z[u];
+                w.mf[o] = f[u];
+                w.ml[o] = l[u];
+                w.morig[o] = ee;
+                lz = fmax(lz, fabs(z[u]));
+            }
+        }
+    }
+    lz = block_max<T>(lz, S.red);
+    if (x == 0) {
+        S.s_val = lz;
+    }
+    // the cluster barrier releases and acquires at cluster scope, which
+    // orders the global writes of every phase for the peer CTAs
+    cl.sync();
+    double maxz = 0.0;
+    for (int r = 0; r < C; ++r) {
+        maxz = fmax(maxz, *cl.map_shared_rank(&S.s_val, r));
+    }
+    const double tol = kDeflTolScale * DBL_EPSILON * fmax(maxd, maxz);
+
+    // ------------------------------------------------ deflation
+    int K, Kz;
+    double zn;
+    if (C == 1) {
+        Kz = defl_compact_active<T>(w, gs, 0, m, rho, tol, 0, 0, S.iscan);
+        __syncthreads();
+        defl_close_walk<T>(w, gs, Kz, tol, 0, Kz);
+        __syncthreads();
+        zn = defl_compact_poles<T>(w, gs, G.poff, 0, Kz, 0, 0, S.iscan, &K);
+        zn = block_sum<T>(zn, S.red);
+    } else {
+        const int SD = ((m + C - 1) / C + chunk - 1) / chunk * chunk;
+        const int r0 = min(m, rank * SD), r1 = min(m, r0 + SD);
+        const int na = defl_count_active<T>(w, gs, r0, r1, rho, tol, S.iscan);
+        if (x == 0) {
+            S.s_cnt = na;
+        }
+        cl.sync();
+        int off_a = 0;
+        Kz = 0;
+        for (int r = 0; r < C; ++r) {
+            const int cn = *cl.map_shared_rank(&S.s_cnt, r);
+            off_a += r < rank ? cn : 0;
+            Kz += cn;
+        }
+        defl_compact_active<T>(w, gs, r0, r1, rho, tol, off_a, r0 - off_a, S.iscan);
+        cl.sync();
+        const int A = (Kz + C - 1) / C;
+        defl_close_walk<T>(w, gs, Kz, tol, min(Kz, rank * A), min(Kz, rank * A + A));
+        cl.sync();
+        const int S2 = ((Kz + C - 1) / C + chunk - 1) / chunk * chunk;
+        const int q0 = min(Kz, rank * S2), q1 = min(Kz, q0 + S2);
+        const int np = defl_count_poles<T>(w, gs, q0, q1, S.iscan);
+        if (x == 0) {
+            S.s_cnt = np;
+        }
+        cl.sync();
+        int off_p = 0;
+        K = 0;
+        for (int r = 0; r < C; ++r) {
+            const int cn = *cl.map_shared_rank(&S.s_cnt, r);
+            off_p += r < rank ? cn : 0;
+            K += cn;
+        }
+        int end_p;
+        double zp = defl_compact_poles<T>(w, gs, G.poff, q0, q1, off_p, q0 - off_p, S.iscan,
+                                          &end_p);
+        zp = block_sum<T>(zp, S.red);
+        if (x == 0) {
+            S.s_val = zp;
+        }
+        cl.sync();
+        zn = 0.0;
+        for (int r = 0; r < C; ++r) {
+            zn += *cl.map_shared_rank(&S.s_val, r);
+        }
+    }
+    if (rank == 0 && x == 0) {
+        w.nK[g] = K;
+        w.nKz[g] = Kz;
+        w.nrho[g] = rho;
+        w.ntol[g] = tol;
+        w.nzn[g] = zn;
+        // level counters of the reference's diagnostics, one node at a time
+        brdc_level_diagnostics *dg = &w.hdr->diag[a.k];
+        atomicAdd(&dg->merge_count, 1);
+        atomicAdd(&dg->size_sum, m);
+        atomicAdd(&dg->dd_before_sum, Kz);
+        atomicAdd(&dg->dd_after_sum, K);
+        atomicMax(&dg->dd_after_max, K);
+        atomicAdd((unsigned long long *)&dg->dd_after_sq_sum,
+                  (unsigned long long)K * (unsigned long long)K);
+        if (K > kLvlMaxK) {
+            atomicAdd(&w.hdr->lvl[a.k].nbig, 1);
+        }
+    }
+    if (K > kLvlMaxK) {
+        // no CTA leaves while a peer may still read its shared memory
+        cl.sync();
+        level_ticket<T>(a, S);
+        return; // k_sweeps finishes this node
+    }
+
+    // ------------------------------------------------ roots
+    if (K > 0) {
+        level_roots<T>(S, cl, a, G, K, rho, zn, C, rank);
+    }
+    cl.sync();
+
+    // ------------------------------------------------ placement
+    // ascending order, ties: roots, small-z deflated, rotated out (k_place)
+    const int ndz = m - Kz, ndg = Kz - K;
+    const long long po = G.poff;
+    for (int i = x; i < K; i += T) {
+        S.pd[i] = S.rdo[i] + S.rtau[i]; // = rlam, bit for bit
+    }
+    const StagedList LZ = stage_list<T>(S.u.stage, w.zd + gs, ndz);
+    const StagedList LG = stage_list<T>(S.u.stage + kLvlSamples, w.gd + gs, ndg);
+    __syncthreads();
+    const bool top = (G.depth == 0);
+    const double wsc = inst_unscale(w, G.inst);
+    for (int s0 = e0 + x; s0 < e1; s0 += B * T) {
+        double val[B], fo[B], lo[B];
+        int pos[B];
+#pragma unroll
+        for (int u = 0; u < B; ++u) {
+            const int s = s0 + u * T < e1 ? s0 + u * T : s0;
+            if (s < K) {
+                val[u] = S.pd[s];
+                fo[u] = top ? 0.0 : __ldcg(w.rf + po + s);
+                lo[u] = top ? 0.0 : __ldcg(w.rl + po + s);
+            } else if (s < K + ndz) {
+                val[u] = w.zd[gs + s - K];
+                fo[u] = w.zf[gs + s - K];
+                lo[u] = w.zl[gs + s - K];
+            } else {
+                val[u] = w.gd[gs + s - K - ndz];
+                fo[u] = w.gf[gs + s - K - ndz];
+                lo[u] = w.gl[gs + s - K - ndz];
+            }
+        }
+        // each row searches the two lists it is not in (rows of one warp
+        // are consecutive, so the branches split few warps)
+        int cz[B], cgr[B];
+#pragma unroll
+        for (int u = 0; u < B; ++u) {
+            const int s = s0 + u * T;
+            cz[u] = 0;
+            cgr[u] = 0;
+            if (s < K) {
+                cz[u] = staged_coarse<false>(LZ, val[u]);
+                cgr[u] = staged_coarse<false>(LG, val[u]);
+            } else if (s < K + ndz) {
+                cgr[u] = staged_coarse<false>(LG, val[u]);
+            } else {
+                cz[u] = staged_coarse<true>(LZ, val[u]); // rotated out: ties after small-z
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < B; ++u) {
+            const int s = s0 + u * T;
+            if (s < K) {
+                pos[u] = s + staged_fine<false>(LZ, cz[u], val[u]) +
+                         staged_fine<false>(LG, cgr[u], val[u]);
+            } else if (s < K + ndz) {
+                pos[u] = (s - K) + upper_bound_d(S.pd, K, val[u]) +
+                         staged_fine<false>(LG, cgr[u], val[u]);
+            } else {
+                pos[u] = (s - K - ndz) + upper_bound_d(S.pd, K, val[u]) +
+                         staged_fine<true>(LZ, cz[u], val[u]);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < B; ++u) {
+            const int s = s0 + u * T;
+            if (s < e1) {
+                const long long o = gs + pos[u];
+                if (top) {
+                    a.W[o] = val[u] * wsc;
+                } else {
+                    w.nd[o] = val[u];
+                    w.nf[o] = fo[u];
+                    w.nl[o] = lo[u];
+                }
+            }
+        }
+    }
+    level_ticket<T>(a, S);
+}
+
+} // namespace brdc

@@ -256,3 +256,24 @@ def test_batched_backward_keep_forward(solver):
     assert torch.equal(a1, a2) and torch.equal(b1, b2)
     W2 = solver.dstebr_batched(off, Dt, Et)
     assert torch.equal(W, W2)
+
+
+@pytest.mark.parametrize("family,n", [("uniform", 20000), ("toeplitz", 6000), ("normal", 12000)])
+def test_fused_levels_same_gradient(solver, family, n):
+    """The checkpoint a fused-level solve leaves (merges finished by k_level,
+    big ones by the sweep kernel) serves the adjoint like the per-level one."""
+    import brdc
+
+    d, e = families.generate(family, n)
+    g = np.random.default_rng(11).standard_normal(n)
+    s = brdc.Solver()
+    try:
+        out = []
+        for fuse in (0, 1 << 30):
+            s.set_tuning(fused_level_rows=fuse)
+            out.append(grads(s, d, e, g))
+        sc = max(np.max(np.abs(out[0][0])), np.max(np.abs(out[0][1])))
+        assert np.max(np.abs(out[1][0] - out[0][0])) < 1e-11 * sc
+        assert np.max(np.abs(out[1][1] - out[0][1])) < 1e-11 * sc
+    finally:
+        s.close()

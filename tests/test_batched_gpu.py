@@ -125,7 +125,7 @@ def test_graph_capture_batched(solver):
 def test_batched_tunings_agree(solver):
     """A batch of mixed orders (tiny ones solved wholly inside the subtree
     kernel, large ones continuing with per-level kernels) gives the same
-    eigenvalues whatever the subtree depth."""
+    eigenvalues whatever the subtree depth and level fusion."""
     import torch
 
     import brdc
@@ -136,8 +136,8 @@ def test_batched_tunings_agree(solver):
     s = brdc.Solver()
     try:
         res = []
-        for sub in (0, 2, 4, 5):
-            s.set_tuning(subtree_levels=sub)
+        for sub, fuse in ((0, 0), (0, 1 << 30), (2, 1 << 30), (4, 0), (4, 1 << 30), (5, 4096)):
+            s.set_tuning(subtree_levels=sub, fused_level_rows=fuse)
             res.append(s.dstebr_batched(off, Dt, Et).cpu().numpy())
         for r in res[1:]:
             for b in range(len(orders)):

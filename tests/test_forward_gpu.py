@@ -125,7 +125,8 @@ def test_lapack_style_host_entry(built_lib):
 def test_tunings_agree(solver, family, n):
     """Launch shapes do not change what is computed: the same deflation
     counts at every level and the same eigenvalues to rounding, whatever
-    the subtree depth, deflation cluster and sweep parallelism."""
+    the subtree depth, deflation cluster, sweep parallelism and level
+    fusion."""
     import torch
 
     import brdc
@@ -136,19 +137,22 @@ def test_tunings_agree(solver, family, n):
     s = brdc.Solver()
     ref_w, ref_k = None, None
     try:
+        ws = s.workspace(n)
         for sub in (-1, 0, 1, 2, 3, 4, 5):
-            for cl in (1, 8):
+            for cl in (1, 16):
                 for lanes in (8192, 75776, 1 << 20):
-                    s.set_tuning(subtree_levels=sub, deflate_cluster=cl, sweep_lanes_target=lanes)
-                    ws = s.workspace(n)
-                    W = s.dstebr(D, E, workspace=ws).cpu().numpy()
-                    K = [lv["dd_after_sum"] for lv in s.diagnostics(n, ws)["level"]]
-                    if ref_w is None:
-                        ref_w, ref_k = W, K
-                        continue
-                    assert K == ref_k, (sub, cl, lanes)
-                    err = np.max(np.abs(W - ref_w)) / np.max(np.abs(ref_w))
-                    assert err < 1e-13, (sub, cl, lanes, err)
+                    for fuse in (0, 4096, 1 << 30):
+                        s.set_tuning(subtree_levels=sub, deflate_cluster=cl,
+                                     sweep_lanes_target=lanes, fused_level_rows=fuse)
+                        W = s.dstebr(D, E, workspace=ws).cpu().numpy()
+                        K = [lv["dd_after_sum"] for lv in s.diagnostics(n, ws)["level"]]
+                        if ref_w is None:
+                            ref_w, ref_k = W, K
+                            continue
+                        key = (sub, cl, lanes, fuse)
+                        assert K == ref_k, key
+                        err = np.max(np.abs(W - ref_w)) / np.max(np.abs(ref_w))
+                        assert err < 1e-13, (key, err)
     finally:
         s.close()
 
@@ -158,11 +162,14 @@ def test_tuning_validation(solver):
 
     s = brdc.Solver()
     try:
-        for bad in ({"subtree_levels": 6}, {"deflate_cluster": 3}, {"sweep_lanes_target": 10}):
+        for bad in ({"subtree_levels": 6}, {"deflate_cluster": 3}, {"sweep_lanes_target": 10},
+                    {"fused_level_rows": -1}):
             with pytest.raises(brdc.BrdcError):
                 s.set_tuning(**bad)
-        s.set_tuning(subtree_levels=2, deflate_cluster=4, sweep_lanes_target=50000)
-        assert s.tuning() == {"subtree_levels": 2, "deflate_cluster": 4, "sweep_lanes_target": 50000}
+        s.set_tuning(subtree_levels=2, deflate_cluster=4, sweep_lanes_target=50000,
+                     fused_level_rows=8192)
+        assert s.tuning() == {"subtree_levels": 2, "deflate_cluster": 4,
+                              "sweep_lanes_target": 50000, "fused_level_rows": 8192}
     finally:
         s.close()
 
@@ -182,7 +189,7 @@ def test_autotune_single_and_batched(solver):
         E = torch.tensor(e, device="cuda")
         t = s.autotune(D, E)
         assert t == s.tuning()
-        assert -1 <= t["subtree_levels"] <= 5 and t["deflate_cluster"] in (1, 2, 4, 8)
+        assert -1 <= t["subtree_levels"] <= 5 and t["deflate_cluster"] in (1, 2, 4, 8, 16)
         W = s.dstebr(D, E).cpu().numpy()
         ref = oracle.dstedc_dc_br(d, e)
         assert np.max(np.abs(W - ref)) / np.max(np.abs(ref)) < 1e-12
