@@ -37,11 +37,7 @@ constexpr int kLvlBatch = 4;         // rows a thread moves per pass (loads issu
 struct LvlSmem {
     double pd[kLvlMaxK], pz[kLvlMaxK], pf[kLvlMaxK], pl[kLvlMaxK], pw[kLvlMaxK];
     double rdo[kLvlMaxK], rtau[kLvlMaxK];
-    union {
-        double stage[2 * kLvlSamples];   // staged sorted lists (merge, placement)
-        SecDyn dyn[kLvlMaxK];            // parked secular state between sweeps
-    } u;
-    int wl[2][kLvlThreads / 32][kLvlMaxK / (kLvlThreads / 32)]; // live roots per warp
+    double stage[2 * kLvlSamples];       // staged sorted lists (merge, placement)
     double red[32];
     int iscan[32];
     double s_val;                        // cluster exchange
@@ -139,86 +135,56 @@ __device__ void level_roots(LvlSmem &S, cooperative_groups::cluster_group &cl, c
             w.rlam[po] = S.pd[0] + t;
         }
     } else if (r1 > r0) {
-        // Each warp takes a contiguous share of the CTA's roots and sweeps
-        // them in rounds: after every sweep it packs its live roots into a
-        // list and spreads them over its lanes (the largest power-of-two
-        // lane count per root that fits), so converged roots free their
-        // lanes for the slow ones.  Between sweeps a root's state is parked
-        // in shared memory; a warp synchronises only with itself.
-        constexpr int NW = T / 32;
-        const int warp = x >> 5;
+        // tp lanes per root (the largest power of two that covers the CTA's
+        // roots in one pass), each group iterating its root to convergence:
+        // no barrier between sweeps
         const int nmine = r1 - r0;
-        const int pw_ = (nmine + NW - 1) / NW;
-        const int q0 = min(nmine, warp * pw_), q1 = min(nmine, q0 + pw_);
-        int *la = S.wl[0][warp], *lb = S.wl[1][warp];
-        int nlive = q1 - q0;
-        for (int i = lane; i < nlive; i += 32) {
-            const int r = r0 + q0 + i;
-            SecRoot st;
-            sec_init(st, r, K, S.pd, S.pz, rho, zn);
-            sec_park(st, S.u.dyn[r]);
-            la[i] = r;
+        int tp = 1;
+        while (tp < 32 && nmine * tp * 2 <= T) {
+            tp <<= 1;
         }
-        __syncwarp();
+        const int per = T / tp, l2 = x & (tp - 1);
         int its = 0, itm = 0, itf = 0;
-        while (nlive > 0) {
-            int tp = 1;
-            while (tp < 32 && nlive * tp * 2 <= 32) {
-                tp <<= 1;
+        for (int base = 0; base < nmine; base += per) {
+            const int r = r0 + base + x / tp;
+            const bool act = r < r1;
+            SecRoot st;
+            if (act) {
+                sec_init(st, r, K, S.pd, S.pz, rho, zn);
+            } else {
+                st.stage = 2;
             }
-            const int gpw = 32 / tp, l2 = lane & (tp - 1);
-            int nn = 0;
-            for (int base = 0; base < nlive; base += gpw) {
-                const int gi = base + lane / tp;
-                const bool act = gi < nlive;
-                const int id = act ? la[gi] : 0;
-                SecRoot st;
-                if (act) {
-                    sec_init_static(st, id, K, S.pd, S.pz, rho, zn);
-                    sec_unpark(st, S.u.dyn[id]);
-                } else {
-                    st.stage = 2;
-                }
+            const int pmin = r < K - 2 ? r : K - 2;
+            for (;;) {
                 SecSums sum;
                 sec_zero(sum);
-                if (act) {
-                    const int pmin = id < K - 2 ? id : K - 2;
-                    secular_span(sum, st, 0, K, l2, tp, pmin, id + 1,
+                const bool live = act && st.stage != 2;
+                if (live) {
+                    secular_span(sum, st, 0, K, l2, tp, pmin, r + 1,
                                  [&](int u, double *du, double *zu) {
                                      *du = S.pd[u];
                                      *zu = S.pz[u];
                                  });
                 }
                 sums_reduce(sum, tp);
-                if (act) {
+                if (live) {
                     sec_after_sweep(st, sum, eps);
                 }
-                const bool lead = act && l2 == 0;
-                const bool more = lead && st.stage != 2;
-                if (more) {
-                    sec_park(st, S.u.dyn[id]);
-                } else if (lead) {
-                    S.rdo[id] = st.dorg;
-                    S.rtau[id] = st.tau;
-                    w.rorg[po + id] = st.org;
-                    w.rdo[po + id] = st.dorg;
-                    w.rtau[po + id] = st.tau;
-                    w.rlam[po + id] = st.dorg + st.tau;
-                    its += st.iter;
-                    itm = max(itm, st.iter);
-                    itf += st.failed;
+                if (__all_sync(kFull, !act || st.stage == 2)) {
+                    break;
                 }
-                const unsigned mb = __ballot_sync(kFull, more);
-                if (more) {
-                    lb[nn + __popc(mb & ((1u << lane) - 1u))] = id;
-                }
-                nn += __popc(mb);
             }
-            __syncwarp();
-            int *t = la;
-            la = lb;
-            lb = t;
-            nlive = nn;
+            if (act && l2 == 0) {
+                S.rdo[r] = st.dorg;
+                S.rtau[r] = st.tau;
+                w.rorg[po + r] = st.org;
+                w.rdo[po + r] = st.dorg;
+                w.rtau[po + r] = st.tau;
+                w.rlam[po + r] = st.dorg + st.tau;
+                its += st.iter;
+                itm = max(itm, st.iter);
+                itf += st.failed;
+            }
         }
         // iteration counters, one warp at a time
         its = __reduce_add_sync(kFull, its);
@@ -365,8 +331,8 @@ __global__ void __launch_bounds__(T, 1) k_level(KArgs a) {
 
     // ------------------------------------------------ rank merge
     // (left wins ties), as k_merge; max|z| on the way
-    const StagedList LA = stage_list<T>(S.u.stage, w.cd + gs, m1);
-    const StagedList LB = stage_list<T>(S.u.stage + kLvlSamples, w.cd + gs + m1, m2);
+    const StagedList LA = stage_list<T>(S.stage, w.cd + gs, m1);
+    const StagedList LB = stage_list<T>(S.stage + kLvlSamples, w.cd + gs + m1, m2);
     __syncthreads();
     const int SE = (m + C - 1) / C;
     const int e0 = min(m, rank * SE), e1 = min(m, e0 + SE);
@@ -514,8 +480,8 @@ __global__ void __launch_bounds__(T, 1) k_level(KArgs a) {
     for (int i = x; i < K; i += T) {
         S.pd[i] = S.rdo[i] + S.rtau[i]; // = rlam, bit for bit
     }
-    const StagedList LZ = stage_list<T>(S.u.stage, w.zd + gs, ndz);
-    const StagedList LG = stage_list<T>(S.u.stage + kLvlSamples, w.gd + gs, ndg);
+    const StagedList LZ = stage_list<T>(S.stage, w.zd + gs, ndz);
+    const StagedList LG = stage_list<T>(S.stage + kLvlSamples, w.gd + gs, ndg);
     __syncthreads();
     const bool top = (G.depth == 0);
     const double wsc = inst_unscale(w, G.inst);

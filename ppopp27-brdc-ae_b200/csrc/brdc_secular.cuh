@@ -314,15 +314,21 @@ __host__ __device__ inline int sec_after_sweep(SecRoot &r, const SecSums &s,
         return 1;
     }
 
-    // stage 1: sums at (dorg, tau)
+    // stage 1: sums at (dorg, tau).  This update is the serial part of every
+    // iteration, so its quotients are reciprocals (brdc_rcp, no special-case
+    // branch) times the numerator: deltas are nonzero (tau stays strictly
+    // inside its bracket), and the model denominators are nonzero on the
+    // branches that take them.
     r.iter += 1;
     const double tau = r.tau;
     const double dlp = (r.dp - r.dorg) - tau; // delta_p
     const double dlq = (r.dq - r.dorg) - tau; // delta_{p+1}
-    const double tp = r.zp2 / dlp;
-    const double tq = r.zq2 / dlq;
-    const double dtp = tp / dlp;
-    const double dtq = tq / dlq;
+    const double rp = brdc_rcp(dlp);
+    const double rq = brdc_rcp(dlq);
+    const double tp = r.zp2 * rp;  // z_p^2 / delta_p
+    const double tq = r.zq2 * rq;
+    const double dtp = tp * rp;    // z_p^2 / delta_p^2
+    const double dtq = tq * rq;
     const double psi_f = s.psi + tp;
     const double phi_f = s.phi + tq;
     const double dpsi_f = s.dpsi + dtp;
@@ -371,10 +377,10 @@ __host__ __device__ inline int sec_after_sweep(SecRoot &r, const SecSums &s,
     // switching rule between fixed-weight and middle-way models
     if (!r.last) {
         if (r.iter == 2) {
-            r.swtch = (r.org == r.p) ? (-w > fabs(r.prevw) / 10.0)
-                                     : (w > fabs(r.prevw) / 10.0);
+            r.swtch = (r.org == r.p) ? (-w > fabs(r.prevw) * 0.1)
+                                     : (w > fabs(r.prevw) * 0.1);
         } else if (r.iter > 2) {
-            if (w * r.prevw > 0.0 && fabs(w) > fabs(r.prevw) / 10.0) {
+            if (w * r.prevw > 0.0 && fabs(w) > fabs(r.prevw) * 0.1) {
                 r.swtch = !r.swtch;
             }
         }
@@ -388,9 +394,9 @@ __host__ __device__ inline int sec_after_sweep(SecRoot &r, const SecSums &s,
             c = w - dlp * dpsi_f - dlq * dphi_f;
         } else if (r.org == r.p) {
             // fixed weight: (d_p - d_q) * (z_p / delta_p)^2
-            c = w - dlq * dw - (r.dp - r.dq) * (r.zp2 / (dlp * dlp));
+            c = w - dlq * dw - (r.dp - r.dq) * dtp;
         } else {
-            c = w - dlp * dw - (r.dq - r.dp) * (r.zq2 / (dlq * dlq));
+            c = w - dlp * dw - (r.dq - r.dp) * dtq;
         }
         const double a = (dlp + dlq) * w - dlp * dlq * dw;
         const double b = dlp * dlq * w;
@@ -405,14 +411,14 @@ __host__ __device__ inline int sec_after_sweep(SecRoot &r, const SecSums &s,
                     aa = r.zq2 + dlp * dlp * dw;
                 }
             }
-            eta = b / aa;
+            eta = b * brdc_rcp(aa);
         } else if (a <= 0.0) {
-            eta = (a - sqrt(fabs(a * a - 4.0 * b * c))) / (2.0 * c);
+            eta = (a - sqrt(fabs(a * a - 4.0 * b * c))) * brdc_rcp(2.0 * c);
         } else {
-            eta = 2.0 * b / (a + sqrt(fabs(a * a - 4.0 * b * c)));
+            eta = 2.0 * b * brdc_rcp(a + sqrt(fabs(a * a - 4.0 * b * c)));
         }
         if (w * eta >= 0.0) {
-            eta = -w / dw;
+            eta = -w * brdc_rcp(dw);
         }
     } else {
         const double c0 = w - dlp * dpsi_f - dlq * dphi_f;
@@ -422,12 +428,12 @@ __host__ __device__ inline int sec_after_sweep(SecRoot &r, const SecSums &s,
         if (c == 0.0) {
             eta = r.hi - tau;
         } else if (a >= 0.0) {
-            eta = (a + sqrt(fabs(a * a - 4.0 * b * c))) / (2.0 * c);
+            eta = (a + sqrt(fabs(a * a - 4.0 * b * c))) * brdc_rcp(2.0 * c);
         } else {
-            eta = 2.0 * b / (a - sqrt(fabs(a * a - 4.0 * b * c)));
+            eta = 2.0 * b * brdc_rcp(a - sqrt(fabs(a * a - 4.0 * b * c)));
         }
         if (w * eta > 0.0) {
-            eta = -w / dw;
+            eta = -w * brdc_rcp(dw);
         }
     }
     double tnew = tau + eta;
