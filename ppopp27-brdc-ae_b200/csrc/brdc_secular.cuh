@@ -106,8 +106,11 @@ struct SecRoot {
 // pole and weight arrays (only d_p, d_{p+1}, z_p, z_{p+1} are read).
 // The fields of root i that never change (a solver that parks the iteration
 // state between sweeps rebuilds them from the problem instead of storing).
+// rhoinv = 1 / rho, which a caller that rebuilds the fields every sweep
+// computes once per node.
 __host__ __device__ inline void sec_init_static(SecRoot &r, int i, int K, const double *d,
-                                                const double *z, double rho, double znorm2) {
+                                                const double *z, double rho, double rhoinv,
+                                                double znorm2) {
     r.i = i;
     r.last = (i == K - 1) ? 1 : 0;
     r.p = r.last ? K - 2 : i;
@@ -115,8 +118,13 @@ __host__ __device__ inline void sec_init_static(SecRoot &r, int i, int K, const 
     r.dq = d[r.p + 1];
     r.zp2 = z[r.p] * z[r.p];
     r.zq2 = z[r.p + 1] * z[r.p + 1];
-    r.rhoinv = 1.0 / rho;
+    r.rhoinv = rhoinv;
     r.hi0 = rho * znorm2;
+}
+
+__host__ __device__ inline void sec_init_static(SecRoot &r, int i, int K, const double *d,
+                                                const double *z, double rho, double znorm2) {
+    sec_init_static(r, i, K, d, z, rho, 1.0 / rho, znorm2);
 }
 
 // The fields that a sweep and sec_after_sweep advance.

@@ -53,10 +53,12 @@ struct SubSmem {
     int nstart[kSubRows / 16], nsize[kSubRows / 16], nK[kSubRows / 16], nKz[kSubRows / 16];
     int kpre[kSubRows / 16 + 1]; // prefix of nK: roots of the level before node j
     double nrho[kSubRows / 16], ntol[kSubRows / 16], nzn[kSubRows / 16], nmaxd[kSubRows / 16];
+    double nrinv[kSubRows / 16]; // 1 / rho of node j
     SecDyn dyn[kSubRows];      // parked secular state of each root between rounds
-    int aq[2][kSubRows];       // unconverged roots, ping-pong
+    int aq[2][kSubRows];       // unconverged roots (root | node << 16), ping-pong
     int scan[32];
-    int it_sum, it_max, it_failed, qcnt;
+    int qc[3];                 // list counters, rotating
+    int it_sum, it_max, it_failed;
 };
 
 // Exclusive scan of one int per thread over the CTA; ex[kSubRows] = total.
@@ -394,6 +396,12 @@ __global__ void __launch_bounds__(kSubRows, 512 / kSubRows) k_subtree(SubArgs A)
                 acc += S.nK[q];
             }
             S.kpre[nk] = acc;
+            S.qc[0] = 0;
+            S.qc[1] = 0;
+            S.qc[2] = 0;
+        }
+        if (x < nk) {
+            S.nrinv[x] = 1.0 / S.nrho[x];
         }
         __syncthreads();
         const int nroots = S.kpre[nk];
@@ -405,8 +413,10 @@ __global__ void __launch_bounds__(kSubRows, 512 / kSubRows) k_subtree(SubArgs A)
             return q;
         };
         bool multi = false;
+        int myq = 0;
         if (x < nroots) {
             const int q = root_node(x);
+            myq = q;
             const int rr = x - S.kpre[q], Kr = S.nK[q], sr = S.nstart[q];
             const double *pd = S.pd + sr, *pz = S.pz + sr;
             if (Kr == 1) {
@@ -423,10 +433,10 @@ __global__ void __launch_bounds__(kSubRows, 512 / kSubRows) k_subtree(SubArgs A)
         }
         sub_scan(S, multi ? 1 : 0);
         if (multi) {
-            S.aq[0][S.ex[x]] = x;
+            S.aq[0][S.ex[x]] = x | (myq << 16);
         }
         int nact = S.ex[kSubRows];
-        int cur = 0;
+        int cur = 0, round = 0;
         __syncthreads();
         while (nact > 0) {
             int tp = 1;
@@ -435,13 +445,13 @@ __global__ void __launch_bounds__(kSubRows, 512 / kSubRows) k_subtree(SubArgs A)
             }
             const int g2 = x / tp, l2 = x % tp;
             const bool act = g2 < nact;
-            const int id = act ? S.aq[cur][g2] : 0;
-            const int q = act ? root_node(id) : 0;
+            const int code = act ? S.aq[cur][g2] : 0;
+            const int id = code & 0xffff, q = code >> 16;
             const int rr = id - S.kpre[q], Kr = S.nK[q], sr = S.nstart[q];
             const double *pd = S.pd + sr, *pz = S.pz + sr;
             SecRoot st;
             if (act) {
-                sec_init_static(st, rr, Kr, pd, pz, S.nrho[q], S.nzn[q]);
+                sec_init_static(st, rr, Kr, pd, pz, S.nrho[q], S.nrinv[q], S.nzn[q]);
                 sec_unpark(st, S.dyn[id]);
             } else {
                 st.stage = 2;
@@ -460,10 +470,10 @@ __global__ void __launch_bounds__(kSubRows, 512 / kSubRows) k_subtree(SubArgs A)
             if (act) {
                 sec_after_sweep(st, sum, eps);
             }
-            if (x == 0) {
-                S.qcnt = 0;
-            }
-            __syncthreads();
+            // one barrier per round: round r appends to qc[r % 3], and
+            // qc[(r+2) % 3], last read in round r-1, is cleared after this
+            // round's barrier, a barrier before its next appends
+            int *cnt = &S.qc[round % 3];
             const bool lead = act && l2 == 0;
             if (lead) {
                 sec_park(st, S.dyn[id]);
@@ -472,16 +482,19 @@ __global__ void __launch_bounds__(kSubRows, 512 / kSubRows) k_subtree(SubArgs A)
             const unsigned mb = __ballot_sync(0xffffffffu, more);
             int at = 0;
             if (lane == 0 && mb != 0u) {
-                at = atomicAdd(&S.qcnt, __popc(mb));
+                at = atomicAdd(cnt, __popc(mb));
             }
             at = __shfl_sync(0xffffffffu, at, 0);
             if (more) {
-                S.aq[cur ^ 1][at + __popc(mb & ((1u << lane) - 1u))] = id;
+                S.aq[cur ^ 1][at + __popc(mb & ((1u << lane) - 1u))] = code;
             }
             __syncthreads();
-            nact = S.qcnt;
+            nact = *cnt;
+            if (x == 0) {
+                S.qc[(round + 2) % 3] = 0;
+            }
             cur ^= 1;
-            __syncthreads();
+            ++round;
         }
         // results and iteration counts, one thread per root
         {
