@@ -175,10 +175,10 @@ def run_reference_arm(args, rank):
 
 
 def run_profile_case(spec):
-    """One or more plain solves of a seeded instance, nothing else on the
-    GPU: solve i launches k_init, k_leaf, then per level k_merge,
-    k_merge_deflate, k_secular, k_lowner and k_rows (below the top level)
-    and k_place, so a kernel's launch index is known in advance."""
+    """One or more plain solves of a seeded instance with the library's
+    default launch shapes, nothing else on the GPU: solve i launches k_init,
+    k_norm, k_subtree, then per level above the subtree k_level and k_sweeps,
+    so a kernel's launch index is known in advance."""
     import torch
 
     import brdc
@@ -420,7 +420,8 @@ def collect_extras(torch, brdc, families, solver, D, E, W, ws, d, e, flush, args
     out["phase_ms"] = acc
     diag = solver.diagnostics(N_HEAD, ws)
     fused = t["fused_levels"]
-    out["roofline"] = roofline(diag, acc, N_HEAD, fused=fused)
+    out["roofline"] = roofline(diag, acc, N_HEAD, fused=fused,
+                               level_rows=headline_tuning["fused_level_rows"])
 
     # other families at the same order
     fam_ms = {}
@@ -439,7 +440,7 @@ def collect_extras(torch, brdc, families, solver, D, E, W, ws, d, e, flush, args
             out["toeplitz_max_err_vs_closed_form"] = float(err)
             dg = solver.diagnostics(N_HEAD, ws)
             out["toeplitz_roofline"] = roofline(dg, None, N_HEAD, total_ms=fam_ms[fam],
-                                                fused=fused)
+                                                fused=fused, level_rows=0)
     out["family_ms"] = fam_ms
     out["family_tuning"] = fam_tuning
     solver.set_tuning(**headline_tuning)
@@ -467,8 +468,7 @@ def collect_extras(torch, brdc, families, solver, D, E, W, ws, d, e, flush, args
                   "h2d_bytes_per_step": int(hD.numel() * 8 + hE.numel() * 8),
                   "d2h_bytes_per_step": int(hW.numel() * 8)}
 
-    default = {"subtree_levels": -1, "deflate_cluster": 8, "sweep_lanes_target": 75776}
-    solver.set_tuning(**default)
+    solver.set_tuning(**DEFAULT_TUNING)
     out["config2"] = bench_config2(torch, families, solver, flush)
     solver.set_tuning(**headline_tuning)
     out["fwd_bwd"] = bench_fwd_bwd(torch, families, solver, flush, args)
@@ -586,7 +586,7 @@ def bench_batched(torch, brdc, families, solver, flush):
 
     # the plain entry looped over the instances, one shared workspace, with
     # the library's default launch shapes
-    solver.set_tuning(subtree_levels=-1, deflate_cluster=8, sweep_lanes_target=75776)
+    solver.set_tuning(**DEFAULT_TUNING)
     nmax = int(np.max(orders))
     ws1 = solver.workspace(nmax)
     W1 = torch.empty_like(W)
@@ -734,12 +734,16 @@ def work_model(diag, fused):
     return sub, per
 
 
-def roofline(diag, phase, n, total_ms=None, fused=0):
-    """Roofline of the dominant kernel (by measured time): the subtree
-    kernel (leaves and the fused bottom levels) or one of the per-level
-    phases above it, each against the measured FP64 FMA peak (a flop model
-    in work_model), or the deflation against HBM copy bandwidth (68 bytes
-    per row and level: d, z, two rows read and written, an index)."""
+def roofline(diag, phase, n, total_ms=None, fused=0, level_rows=0):
+    """Roofline of the dominant kernel (by measured time) against the
+    measured FP64 FMA peak (flop model in work_model), or, for the
+    per-level deflation, against HBM copy bandwidth (68 bytes per row and
+    level: d, z, two rows read and written, an index).  Candidates: the
+    subtree kernel (leaves and the lowest levels), k_level (the levels whose
+    largest merge has at most `level_rows` rows: its phase column holds the
+    whole level), k_sweeps (roots, Loewner, rows and placement of the other
+    levels, and of the merges k_level hands on), and the per-level merge and
+    deflation."""
     hbm, hbm_kind = measured_peaks()
     levels = diag["level"]
     fp64_peak = fp64_peak_gflops()
@@ -752,14 +756,27 @@ def roofline(diag, phase, n, total_ms=None, fused=0):
                     "peak": fp64_peak / 1e3, "unit": "TFLOP/s", "frac": ach / (fp64_peak / 1e3),
                     "traffic": None, "peak_kind": "measured (DFMA probe)"})
         return res
-    upper = per[fused:]
-    lv_ms = phase["level_ms"][fused:]
+    lvl_ms = [0.0, 0.0]       # k_level, per-level merge + deflation
+    lvl_work = [0.0, 0.0]
+    sw_ms, sw_work = 0.0, 0.0
+    for k in range(fused, len(levels)):
+        lv = levels[k]
+        mmax = lv["size_sum"] // max(lv["merge_count"], 1)
+        row = phase["level_ms"][k]
+        flops = sum(per[k])
+        if mmax <= level_rows:
+            lvl_ms[0] += row[0]
+            lvl_work[0] += flops
+        else:
+            lvl_ms[1] += row[0]
+            lvl_work[1] += 68.0 * n
+            sw_work += flops
+        sw_ms += row[1] + row[2] + row[3]
     cand = {
         "k_subtree": (phase["leaf_ms"], sub_flops, "fp64"),
-        "k_secular": (sum(r[1] for r in lv_ms), sum(x[0] for x in upper), "fp64"),
-        "k_lowner": (sum(r[2] for r in lv_ms), sum(x[1] for x in upper), "fp64"),
-        "k_rows+k_place": (sum(r[3] for r in lv_ms), sum(x[2] for x in upper), "fp64"),
-        "k_merge+k_merge_deflate": (sum(r[0] for r in lv_ms), 68.0 * n * len(upper), "hbm"),
+        "k_level": (lvl_ms[0], lvl_work[0], "fp64"),
+        "k_sweeps": (sw_ms, sw_work, "fp64"),
+        "k_merge+k_merge_deflate": (lvl_ms[1], lvl_work[1], "hbm"),
     }
     name = max(cand, key=lambda k: cand[k][0])
     ms, work, bound = cand[name]
@@ -785,6 +802,10 @@ def roofline(diag, phase, n, total_ms=None, fused=0):
 # in profiles/ (uniform N=65536): the working set is L2-resident, so DRAM
 # sees little more than the first touch of the inputs.
 KERNEL_TRAFFIC = {"k_subtree": 1222144}
+
+# the library's default launch shapes (brdc_tuning defaults)
+DEFAULT_TUNING = {"subtree_levels": -1, "deflate_cluster": 16, "sweep_lanes_target": 75776,
+                  "fused_level_rows": 1 << 30}
 
 
 _FP64 = None

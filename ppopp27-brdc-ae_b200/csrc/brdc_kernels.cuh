@@ -341,7 +341,7 @@ __global__ void __launch_bounds__(256) k_merge(KArgs a, long long total_n) {
 template <int T>
 __device__ void level_plan(const KArgs &a, double *red, int *iscan) {
     const Ws &w = a.w;
-    double tkw = 0.0, tkc = 0.0, cw = 0.0, cc = 0.0;
+    double tkw = 0.0, tkc = 0.0, cw = 0.0, cc = 0.0, qw = 0.0, qc = 0.0;
     double skz = 0.0, sk = 0.0, sk2 = 0.0, kmax = 0.0;
     for (int i = threadIdx.x; i < a.nodes; i += T) {
         const int kk = __ldcg(w.nK + i);
@@ -350,9 +350,11 @@ __device__ void level_plan(const KArgs &a, double *red, int *iscan) {
         if (kk > a.big_k && kk > kWarpMaxK) {
             tkc += kk;
             cc += 1.0;
+            qc += (double)kk * (double)kk;
         } else if (kk > a.big_k) {
             tkw += kk;
             cw += 1.0;
+            qw += (double)kk * (double)kk;
         }
         skz += kz;
         sk += kk;
@@ -363,6 +365,8 @@ __device__ void level_plan(const KArgs &a, double *red, int *iscan) {
     tkc = block_sum<T>(tkc, red);
     cw = block_sum<T>(cw, red);
     cc = block_sum<T>(cc, red);
+    qw = block_sum<T>(qw, red);
+    qc = block_sum<T>(qc, red);
     skz = block_sum<T>(skz, red);
     sk = block_sum<T>(sk, red);
     sk2 = block_sum<T>(sk2, red);
@@ -448,6 +452,8 @@ __device__ void level_plan(const KArgs &a, double *red, int *iscan) {
         c->items_w = carry_w;
         c->items_c = carry_c;
         c->total_k = (int)(tkw + tkc);
+        c->work_w = qw;
+        c->work_c = qc;
         w.hdr->diag[a.k].threads_per_root = carry_c > 0 ? tpr_c : tpr_w;
     }
 }
@@ -1635,9 +1641,9 @@ __device__ inline bool grid_barrier(WsHeader *h, LevelCtl *c) {
 // cooperative launch: the four phases above separated by grid barriers
 // instead of kernel boundaries.  After k_level (big_k > 0) it returns at
 // once when the level plan has no items: k_level finished every merge.
-// The roles split the grid by the plan: all blocks to the role that has
-// items when only one has, half each otherwise (`tiles` = 0: the launch has
-// no tile memory and every block takes the warp role).  `rows` = 0 skips the
+// The roles split the grid in proportion to their pole-root pairs in the
+// plan (all blocks to the role that has items when only one has; `tiles` =
+// 0: the launch has no tile memory and every block takes the warp role).  `rows` = 0 skips the
 // Loewner and rows phases (every merge an instance root).
 __global__ void __launch_bounds__(kSweepThreads)
     k_sweeps(KArgs a, int tiles, int rows, long long total_n) {
@@ -1649,8 +1655,15 @@ __global__ void __launch_bounds__(kSweepThreads)
     if (a.big_k > 0 && iw + ic == 0) {
         return;
     }
-    const int cta_blocks = (!tiles || ic == 0) ? 0 : (iw == 0 ? (int)gridDim.x
-                                                              : (int)gridDim.x / 2);
+    int cta_blocks = 0;
+    if (tiles && ic > 0) {
+        cta_blocks = (int)gridDim.x;
+        if (iw > 0) {
+            const double wc = __ldcg(&ctl->work_c), ww = __ldcg(&ctl->work_w);
+            const int share = (int)((double)gridDim.x * wc / fmax(wc + ww, 1.0) + 0.5);
+            cta_blocks = max(1, min((int)gridDim.x - 1, min(share, ic)));
+        }
+    }
     unsigned ph[2] = {0u, 0u};
     if ((int)blockIdx.x < cta_blocks) {
         block_role_setup(bars);
@@ -1748,6 +1761,8 @@ __global__ void k_init(WsHeader *h, int levels, int B, long long total_n,
         h->lvl[k].nbig = 0;
         h->lvl[k].bar_count = 0u;
         h->lvl[k].bar_gen = 0u;
+        h->lvl[k].work_w = 0.0;
+        h->lvl[k].work_c = 0.0;
         brdc_level_diagnostics z = {};
         z.level = k;
         h->diag[k] = z;
