@@ -439,11 +439,46 @@ __global__ void __launch_bounds__(kSubRows, 512 / kSubRows) k_subtree(SubArgs A)
         int cur = 0, round = 0;
         __syncthreads();
         while (nact > 0) {
-            int tp = 1;
-            while (tp < 32 && nact * tp * 2 <= kSubRows) {
-                tp <<= 1;
+            if (nact <= kSubRows / 32) {
+                // The last few roots (the slow tail of the iteration): one
+                // warp each, iterated to convergence with no barrier,
+                // parking or list between sweeps.  All 32 lanes hold the
+                // same state (the butterfly sums are bit-identical), so the
+                // loop is warp-uniform; the iteration cap ends it.
+                const int wq = x >> 5;
+                if (wq < nact) {
+                    const int code = S.aq[cur][wq];
+                    const int id = code & 0xffff, q = code >> 16;
+                    const int rr = id - S.kpre[q], Kr = S.nK[q], sr = S.nstart[q];
+                    const double *pd = S.pd + sr, *pz = S.pz + sr;
+                    SecRoot st;
+                    sec_init_static(st, rr, Kr, pd, pz, S.nrho[q], S.nrinv[q], S.nzn[q]);
+                    sec_unpark(st, S.dyn[id]);
+                    const int pmin = rr < Kr - 2 ? rr : Kr - 2;
+                    while (st.stage != 2) {
+                        SecSums sum;
+                        sec_zero(sum);
+                        secular_span(sum, st, 0, Kr, lane, 32, pmin, rr + 1,
+                                     [&](int u, double *du, double *zu) {
+                                         *du = pd[u];
+                                         *zu = pz[u];
+                                     });
+                        sums_reduce(sum, 32);
+                        sec_after_sweep(st, sum, eps);
+                    }
+                    if (lane == 0) {
+                        sec_park(st, S.dyn[id]);
+                    }
+                }
+                __syncthreads();
+                break;
             }
-            const int g2 = x / tp, l2 = x % tp;
+            int lg = 0;
+            while (lg < 5 && nact << (lg + 1) <= kSubRows) {
+                ++lg;
+            }
+            const int tp = 1 << lg;
+            const int g2 = x >> lg, l2 = x & (tp - 1);
             const bool act = g2 < nact;
             const int code = act ? S.aq[cur][g2] : 0;
             const int id = code & 0xffff, q = code >> 16;
