@@ -539,8 +539,9 @@ int launch_sweeps(brdc_handle h, const HostForest &hf, const KArgs &a, cudaStrea
 }
 
 // One fused level (k_level), then k_sweeps for its merges with more than
-// kLvlMaxK poles (it returns at once when there are none).  Returns the
-// number of kernels launched.
+// kLvlMaxK poles (it returns at once when there are none; it is not launched
+// where no merge has more rows than that).  Returns the number of kernels
+// launched.
 int launch_level_fused(brdc_handle h, const HostForest &hf, const KArgs &a0, bool ckpt,
                        cudaStream_t s) {
     const int k = a0.k;
@@ -571,7 +572,14 @@ int launch_level_fused(brdc_handle h, const HostForest &hf, const KArgs &a0, boo
         ++n;
     }
     mark(h, 3 + 4 * k);
-    n += launch_sweeps(h, hf, a, s);
+    if (mmax > kLvlMaxK) {
+        n += launch_sweeps(h, hf, a, s);
+    } else {
+        // no merge of this level can keep more than kLvlMaxK poles
+        mark(h, 4 + 4 * k);
+        mark(h, 5 + 4 * k);
+        mark(h, 6 + 4 * k);
+    }
     if (ckpt) {
         // the adjoint's sweeps want the item tables of every merge
         a.big_k = 0;
