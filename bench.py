@@ -804,7 +804,7 @@ def roofline(diag, phase, n, total_ms=None, fused=0, level_rows=0):
 KERNEL_TRAFFIC = {"k_subtree": 1222144}
 
 # the library's default launch shapes (brdc_tuning defaults)
-DEFAULT_TUNING = {"subtree_levels": -1, "deflate_cluster": 16, "sweep_lanes_target": 75776,
+DEFAULT_TUNING = {"subtree_levels": -1, "deflate_cluster": 16, "sweep_lanes_target": 303104,
                   "fused_level_rows": 1 << 30}
 
 

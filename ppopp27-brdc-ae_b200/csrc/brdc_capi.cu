@@ -40,7 +40,7 @@ struct brdc_handle_struct {
     // -1: chosen per solve from the tree height)
     int sub_levels = -1;
     int defl_cluster = 16;        // largest deflation cluster (8 for k_merge_deflate_cl)
-    int lanes_target = 75776;     // root-sweep parallelism target
+    int lanes_target = 303104;    // root-sweep parallelism target
     int lvl_rows = 1 << 30;       // largest merge of a level run by k_level (0: none)
     std::vector<long long> prep_off;
     // phase timing (off by default)
@@ -426,11 +426,15 @@ void mark(brdc_handle h, int slot) {
 }
 
 // Subtree depth of a solve: the handle's setting, or by default the depth
-// measured fastest for uniform spectra on B200 for the forest's tallest
-// instance (3 up to 10 levels, i.e. n <= 16384; 4 at 11; 5 above).
+// measured fastest on B200: 5 for a batch with at least two 512-row
+// subtrees per SM (the subtrees fill the GPU), otherwise by the forest's
+// tallest instance (3 up to 10 levels, i.e. n <= 16384; 4 at 11; 5 above).
 int effective_sub_levels(brdc_handle h, const HostForest &hf) {
     if (h->sub_levels >= 0) {
         return h->sub_levels;
+    }
+    if (hf.B > 1 && hf.total_n >= 512LL * 2 * h->sm_count) {
+        return 5;
     }
     return hf.max_levels <= 10 ? 3 : (hf.max_levels == 11 ? 4 : 5);
 }
@@ -1213,7 +1217,7 @@ extern "C" brdc_status brdc_autotune(brdc_handle h, int64_t count, const int64_t
     const int subs[] = {0, 1, 2, 3, 4, 5};
     const int fuse[] = {0, kLvlRowsPerCta, 1 << 30};
     const int clusters[] = {1, 2, 4, 8, 16};
-    const int lanes[] = {18944, 37888, 75776, 151552, 303104};
+    const int lanes[] = {37888, 75776, 151552, 303104, 606208};
     struct Axis {
         int brdc_tuning::*field;
         const int *vals;
