@@ -584,12 +584,7 @@ int launch_level_fused(brdc_handle h, const HostForest &hf, const KArgs &a0, boo
         mark(h, 5 + 4 * k);
         mark(h, 6 + 4 * k);
     }
-    if (ckpt) {
-        // the adjoint's sweeps want the item tables of every merge
-        a.big_k = 0;
-        k_plan<1024><<<1, 1024, 0, s>>>(a);
-        ++n;
-    }
+    (void)ckpt; // the adjoint's full plan of this level comes with run_forest's last launch
     return n;
 }
 
@@ -654,19 +649,6 @@ brdc_status run_forest(brdc_handle h, const HostForest &hf, const Layout &L,
             h->has_lowner[k] = 0;
         }
         h->fused_levels = fused;
-        if (L.ckpt) {
-            // item tables of the fused levels, which the adjoint's sweeps use
-            for (int k = 0; k < fused; ++k) {
-                KArgs ak = a;
-                ak.k = k;
-                ak.nodes = hf.level_nodes[k];
-                ak.level_rows = hf.level_rows[k];
-                level_view(hf, L, w, k, &ak.w);
-                k_plan<1024><<<1, 1024, 0, s>>>(ak);
-                ++h->launches;
-            }
-            BRDC_CUDA(h, "brdc.subtree_plan", cudaGetLastError());
-        }
         if (fused & 1) {
             std::swap(a.w.cd, a.w.nd);
             std::swap(a.w.cf, a.w.nf);
@@ -714,6 +696,39 @@ brdc_status run_forest(brdc_handle h, const HostForest &hf, const Layout &L,
         std::swap(a.w.cd, a.w.nd);
         std::swap(a.w.cf, a.w.nf);
         std::swap(a.w.cl, a.w.nl);
+    }
+    if (L.ckpt) {
+        // the item tables of every merge on the levels the forward solved
+        // without them (subtree and fused levels), which the adjoint's
+        // sweeps read: one launch, one CTA per level
+        static_assert(sizeof(PlanAllArgs) <= 4096, "kernel parameters of k_plan_all");
+        PlanAllArgs P{};
+        P.base = a;
+        int cnt = 0;
+        for (int k = 0; k < hf.max_levels && cnt < kPlanMaxLevels; ++k) {
+            const bool sub_level = sub > 0 && k < fused;
+            const bool fused_level = !sub_level && hf.level_mmax[k] <= h->lvl_rows;
+            if (!sub_level && !fused_level) {
+                continue;
+            }
+            Ws v = w;
+            level_view(hf, L, w, k, &v);
+            PlanLevel &pl = P.lv[cnt++];
+            pl.nK = v.nK;
+            pl.nKz = v.nKz;
+            pl.pref_w = v.pref_w;
+            pl.pref_c = v.pref_c;
+            pl.items_w = v.items_w;
+            pl.items_c = v.items_c;
+            pl.nodes = hf.level_nodes[k];
+            pl.k = k;
+            pl.rows = hf.level_rows[k];
+        }
+        if (cnt > 0) {
+            k_plan_all<1024><<<cnt, 1024, 0, s>>>(P);
+            BRDC_CUDA(h, "brdc.plans", cudaGetLastError());
+            ++h->launches;
+        }
     }
     return BRDC_STATUS_SUCCESS;
 }

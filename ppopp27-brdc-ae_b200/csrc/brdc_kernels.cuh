@@ -465,6 +465,40 @@ __global__ void __launch_bounds__(T) k_plan(KArgs a) {
     level_plan<T>(a, red, iscan);
 }
 
+// The full plans (every merge) of many levels in one launch, one CTA per
+// level: what a checkpointed forward leaves for the adjoint's sweeps on the
+// levels it solved without them (subtree and fused levels).  A level's plan
+// reads and writes only these arrays of its workspace slice.
+struct PlanLevel {
+    int *nK, *nKz, *pref_w, *pref_c, *items_w, *items_c;
+    int nodes, k;
+    long long rows;
+};
+constexpr int kPlanMaxLevels = 40;
+struct PlanAllArgs {
+    KArgs base;
+    PlanLevel lv[kPlanMaxLevels];
+};
+
+template <int T>
+__global__ void __launch_bounds__(T) k_plan_all(PlanAllArgs P) {
+    __shared__ double red[32];
+    __shared__ int iscan[32];
+    const PlanLevel &L = P.lv[blockIdx.x];
+    KArgs a = P.base;
+    a.w.nK = L.nK;
+    a.w.nKz = L.nKz;
+    a.w.pref_w = L.pref_w;
+    a.w.pref_c = L.pref_c;
+    a.w.items_w = L.items_w;
+    a.w.items_c = L.items_c;
+    a.nodes = L.nodes;
+    a.level_rows = L.rows;
+    a.k = L.k;
+    a.big_k = 0;
+    level_plan<T>(a, red, iscan);
+}
+
 constexpr int kDeflEPT = 4; // rows per thread per deflation chunk
 
 // Deflation phases over a range of rows, shared by the one-CTA-per-node
