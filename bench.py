@@ -801,7 +801,7 @@ def roofline(diag, phase, n, total_ms=None, fused=0, level_rows=0):
 # DRAM bytes (read + write) of one launch, from the ncu captures summarised
 # in profiles/ (uniform N=65536): the working set is L2-resident, so DRAM
 # sees little more than the first touch of the inputs.
-KERNEL_TRAFFIC = {"k_subtree": 1222144}
+KERNEL_TRAFFIC = {"k_subtree": 1240320}
 
 # the library's default launch shapes (brdc_tuning defaults)
 DEFAULT_TUNING = {"subtree_levels": -1, "deflate_cluster": 16, "sweep_lanes_target": 303104,

@@ -564,19 +564,21 @@ int launch_level_fused(brdc_handle h, const HostForest &hf, const KArgs &a0, boo
     const int C = 1 << q;
     KArgs a = a0;
     a.big_k = kLvlMaxK;
-    a.plan_inline = a.nodes <= kLvlThreads ? 1 : 0;
+    // a plan is needed only where a merge can keep more than kLvlMaxK poles
+    const bool big = mmax > kLvlMaxK;
+    a.plan_inline = big && a.nodes <= kLvlThreads ? 1 : 0;
     cudaLaunchAttribute at[1];
     cudaLaunchConfig_t cfg = cluster_config((unsigned)(a.nodes * C), C, s, at);
     cfg.blockDim = dim3(kLvlThreads);
     cfg.dynamicSmemBytes = sizeof(LvlSmem);
     cudaLaunchKernelEx(&cfg, k_level<kLvlThreads>, a);
     int n = 1;
-    if (!a.plan_inline) {
+    if (big && !a.plan_inline) {
         k_plan<1024><<<1, 1024, 0, s>>>(a);
         ++n;
     }
     mark(h, 3 + 4 * k);
-    if (mmax > kLvlMaxK) {
+    if (big) {
         n += launch_sweeps(h, hf, a, s);
     } else {
         // no merge of this level can keep more than kLvlMaxK poles

@@ -174,6 +174,18 @@ def test_tuning_validation(solver):
         s.close()
 
 
+def test_default_tuning(solver):
+    """A new handle carries the documented default launch shapes."""
+    import brdc
+
+    s = brdc.Solver()
+    try:
+        assert s.tuning() == {"subtree_levels": -1, "deflate_cluster": 16,
+                              "sweep_lanes_target": 303104, "fused_level_rows": 1 << 30}
+    finally:
+        s.close()
+
+
 def test_autotune_single_and_batched(solver):
     """The autotuner leaves a valid tuning on the handle, and solves under it
     stay correct."""
