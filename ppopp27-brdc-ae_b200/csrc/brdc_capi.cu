@@ -1,11 +1,11 @@
 // brdc_capi.cu -- host driver and C ABI (include/brdc.h).
 //
 // The driver plans a forest (one or many tridiagonals), carves the caller's
-// workspace, and enqueues per level: k_merge, k_merge_deflate, k_secular,
-// k_lowner, k_rows, k_place.  All launch shapes depend only on the orders,
-// never on data,
-// and no call synchronises the stream, so a solve can be captured in a CUDA
-// graph.  Data-dependent sizes (deflation counts K) travel from kernel to
+// workspace, and enqueues the leaves and lowest levels (k_subtree), then per
+// level either the fused k_level (with k_sweeps for merges that keep many
+// poles) or k_merge, the deflation and k_sweeps.  All launch shapes depend
+// only on the orders, never on data, and no call synchronises the stream,
+// so a solve can be captured in a CUDA graph.  Data-dependent sizes (deflation counts K) travel from kernel to
 // kernel through the workspace header; that replaces the per-level device
 // to host copy of the reference (gpu/src/tridiag_solver.cu:624-630).
 #include <cuda_runtime.h>
@@ -381,17 +381,7 @@ cudaError_t set_attrs() {
     if (g_attr_done) {
         return cudaSuccess;
     }
-    cudaError_t e = cudaFuncSetAttribute(
-        k_secular, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_tiles(2));
-    if (e == cudaSuccess) {
-        e = cudaFuncSetAttribute(k_lowner, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem_tiles(3));
-    }
-    if (e == cudaSuccess) {
-        e = cudaFuncSetAttribute(k_rows,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem_tiles(4));
-    }
+    cudaError_t e = cudaSuccess;
     if (e == cudaSuccess) {
         e = cudaFuncSetAttribute(k_subtree<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)sizeof(SubSmem<256>));
@@ -493,53 +483,33 @@ int sweeps_per_sm(int device, bool tiles) {
 }
 
 // Roots, Loewner weights, rows and placement of level a.k: one cooperative
-// k_sweeps (with tile memory where a merge can exceed kWarpMaxK poles), or
-// the four kernels where the device cannot launch it.
-// Returns the number of kernels launched.
+// k_sweeps (with tile memory where a merge can exceed kWarpMaxK poles).
+// Returns the number of kernels launched, or -1 where the device cannot
+// launch a cooperative grid (every sm_100 device can).
 int launch_sweeps(brdc_handle h, const HostForest &hf, const KArgs &a, cudaStream_t s) {
     const int k = a.k;
     const bool tiles = hf.level_mmax[k] > kWarpMaxK;
     const int rows = h->has_lowner[k];
     const int nb = sweeps_per_sm(h->device, tiles);
-    if (nb > 0) {
-        const int grid = nb * h->sm_count;
-        cudaLaunchAttribute at[1];
-        at[0].id = cudaLaunchAttributeCooperative;
-        at[0].val.cooperative = 1;
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3((unsigned)grid);
-        cfg.blockDim = dim3(kSweepThreads);
-        cfg.dynamicSmemBytes = tiles ? smem_tiles(4) : 0;
-        cfg.stream = s;
-        cfg.attrs = at;
-        cfg.numAttrs = 1;
-        cudaLaunchKernelEx(&cfg, k_sweeps, a, tiles ? 1 : 0, rows, (long long)hf.total_n);
-        mark(h, 4 + 4 * k);
-        mark(h, 5 + 4 * k);
-        mark(h, 6 + 4 * k);
-        return 1;
+    if (nb <= 0) {
+        return -1;
     }
-    const int cta_blocks = tiles ? h->sm_count * 2 : 0;
-    const int grid = cta_blocks + h->sm_count * 2;
-    int n = 0;
-    k_secular<<<grid, kSweepThreads, cta_blocks ? smem_tiles(2) : 0, s>>>(a, cta_blocks);
-    ++n;
+    const int grid = nb * h->sm_count;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(kSweepThreads);
+    cfg.dynamicSmemBytes = tiles ? smem_tiles(4) : 0;
+    cfg.stream = s;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k_sweeps, a, tiles ? 1 : 0, rows, (long long)hf.total_n);
     mark(h, 4 + 4 * k);
-    if (rows) {
-        k_lowner<<<grid, kSweepThreads, cta_blocks ? smem_tiles(3) : 0, s>>>(a, cta_blocks);
-        ++n;
-    }
     mark(h, 5 + 4 * k);
-    if (rows) {
-        k_rows<<<grid, kSweepThreads, cta_blocks ? smem_tiles(4) : 0, s>>>(a, cta_blocks);
-        ++n;
-    }
-    long long elem_grid = (hf.total_n + 255) / 256;
-    elem_grid = std::max<long long>(1, std::min<long long>(elem_grid, (long long)h->sm_count * 8));
-    k_place<<<(unsigned)elem_grid, 256, 0, s>>>(a, hf.total_n);
-    ++n;
     mark(h, 6 + 4 * k);
-    return n;
+    return 1;
 }
 
 // One fused level (k_level), then k_sweeps for its merges with more than
@@ -579,7 +549,11 @@ int launch_level_fused(brdc_handle h, const HostForest &hf, const KArgs &a0, boo
     }
     mark(h, 3 + 4 * k);
     if (big) {
-        n += launch_sweeps(h, hf, a, s);
+        const int ns = launch_sweeps(h, hf, a, s);
+        if (ns < 0) {
+            return -1;
+        }
+        n += ns;
     } else {
         // no merge of this level can keep more than kLvlMaxK poles
         mark(h, 4 + 4 * k);
@@ -683,8 +657,9 @@ brdc_status run_forest(brdc_handle h, const HostForest &hf, const Layout &L,
             }
         }
         h->has_lowner[k] = any_inner ? 1 : 0;
+        int nl;
         if (hf.level_mmax[k] <= h->lvl_rows) {
-            h->launches += launch_level_fused(h, hf, a, L.ckpt, s);
+            nl = launch_level_fused(h, hf, a, L.ckpt, s);
             BRDC_CUDA(h, "brdc.level", cudaGetLastError());
         } else {
             k_merge<<<(unsigned)elem_grid, 256, 0, s>>>(a, hf.total_n);
@@ -692,9 +667,15 @@ brdc_status run_forest(brdc_handle h, const HostForest &hf, const Layout &L,
             h->launches += 1 + launch_merge_deflate(h, a, hf.level_mmax[k], s);
             BRDC_CUDA(h, "brdc.merge_deflate", cudaGetLastError());
             mark(h, 3 + 4 * k);
-            h->launches += launch_sweeps(h, hf, a, s);
+            nl = launch_sweeps(h, hf, a, s);
             BRDC_CUDA(h, "brdc.sweeps", cudaGetLastError());
         }
+        if (nl < 0) {
+            set_error(h, (int)cudaErrorNotSupported, BRDC_ERROR_SRC_CUDA,
+                      "brdc.sweeps: no cooperative launch on this device");
+            return BRDC_STATUS_NOT_IMPLEMENTED;
+        }
+        h->launches += nl;
         std::swap(a.w.cd, a.w.nd);
         std::swap(a.w.cf, a.w.nf);
         std::swap(a.w.cl, a.w.nl);

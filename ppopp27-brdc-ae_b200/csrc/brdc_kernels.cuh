@@ -1,22 +1,25 @@
 // brdc_kernels.cuh -- sm_100a kernels of the forward BR solve.
 //
-// One forest level runs six kernels:
+// A forest level solved by per-level kernels (the levels the fused level
+// kernel of brdc_level.cuh does not take) runs:
 //   k_merge          one thread per row: rank merge of the two sorted child
 //                    spectra, z from the children's boundary rows
-//   k_merge_deflate  one CTA per merge: small-z and close-pole deflation
-//                    with Givens rotations of z and of both boundary rows,
-//                    compaction, work plan of the level
-//   k_secular        secular roots, TPR lanes per root; merges with K <=
+//   k_merge_deflate  one CTA (or a cluster of CTAs) per merge: small-z and
+//                    close-pole deflation with Givens rotations of z and of
+//                    both boundary rows, compaction, work plan of the level
+//   k_sweeps         one cooperative launch, its phases separated by grid
+//                    barriers:
+//     secular        secular roots, TPR lanes per root; merges with K <=
 //                    kWarpMaxK one warp per work item (poles through L1),
 //                    larger ones one CTA per item with pole tiles staged in
 //                    shared memory by cp.async.bulk
-//   k_lowner         Loewner / Gu-Eisenstat recomputation of z (same roles)
-//   k_rows           first/last rows of the merged eigenvector matrix for
+//     Loewner        Loewner / Gu-Eisenstat recomputation of z (same roles)
+//     rows           first/last rows of the merged eigenvector matrix for
 //                    every root (same roles)
-//   k_place          one thread per row: every eigenvalue of a node to its
+//     placement      one thread per row: every eigenvalue of a node to its
 //                    place in the node's ascending spectrum
-// The leaves are solved first by k_leaf (one warp per leaf, parallel
-// cyclic Jacobi).
+// The leaves are solved first by k_leaf (one warp per two leaves, parallel
+// cyclic Jacobi) or inside k_subtree.
 #pragma once
 
 #include <cooperative_groups.h>
@@ -1170,10 +1173,9 @@ __device__ inline int block_role_setup(uint64_t *bars) {
 // merges (8 warps per block, each on its own work item).
 constexpr int kWarpsPerBlock = kSweepThreads / 32;
 
-// The phases below are device functions over the grid's two roles, run by
-// their own kernels (k_secular, k_lowner, k_rows, k_place) or back to back
-// by k_sweeps.  CTA-role blocks set up their two mbarriers once (ph holds
-// their phase bits across phases).  Each returns false after a barrier
+// The phases below are device functions over the grid's two roles, run back
+// to back by k_sweeps.  CTA-role blocks set up their two mbarriers once (ph
+// holds their phase bits across phases).  Each returns false after a barrier
 // timeout (recorded in the workspace status).
 __device__ bool sweep_secular(const KArgs &a, int cta_blocks, double *smem, uint64_t *bars,
                               unsigned *ph) {
@@ -1308,16 +1310,6 @@ __device__ bool sweep_secular(const KArgs &a, int cta_blocks, double *smem, uint
     return true;
 }
 
-__global__ void __launch_bounds__(kSweepThreads)
-    k_secular(KArgs a, int cta_blocks) {
-    extern __shared__ __align__(16) double smem[];
-    __shared__ __align__(8) uint64_t bars[2];
-    unsigned ph[2] = {0u, 0u};
-    if ((int)blockIdx.x < cta_blocks) {
-        block_role_setup(bars);
-    }
-    sweep_secular(a, cta_blocks, smem, bars, ph);
-}
 
 // ------------------------------------------------------------- Loewner z
 // For every pole i:  w_i = sign(z_i) * sqrt(-prod_j delta_i(j) /
@@ -1434,16 +1426,6 @@ __device__ bool sweep_lowner(const KArgs &a, int cta_blocks, double *smem, uint6
     return true;
 }
 
-__global__ void __launch_bounds__(kSweepThreads)
-    k_lowner(KArgs a, int cta_blocks) {
-    extern __shared__ __align__(16) double smem[];
-    __shared__ __align__(8) uint64_t bars[2];
-    unsigned ph[2] = {0u, 0u};
-    if ((int)blockIdx.x < cta_blocks) {
-        block_role_setup(bars);
-    }
-    sweep_lowner(a, cta_blocks, smem, bars, ph);
-}
 
 // ----------------------------------------------------------- boundary rows
 // Root s: u_i = w_i / delta_i(s), normalised; new first row = sum_i f_i u_i,
@@ -1556,16 +1538,6 @@ __device__ bool sweep_rows(const KArgs &a, int cta_blocks, double *smem, uint64_
     return true;
 }
 
-__global__ void __launch_bounds__(kSweepThreads)
-    k_rows(KArgs a, int cta_blocks) {
-    extern __shared__ __align__(16) double smem[];
-    __shared__ __align__(8) uint64_t bars[2];
-    unsigned ph[2] = {0u, 0u};
-    if ((int)blockIdx.x < cta_blocks) {
-        block_role_setup(bars);
-    }
-    sweep_rows(a, cta_blocks, smem, bars, ph);
-}
 
 // --------------------------------------------------------------- placement
 // One thread per row of the level: every eigenvalue of a merged node (root,
@@ -1627,9 +1599,6 @@ __device__ void place_rows(const KArgs &a, long long total_n) {
     }
 }
 
-__global__ void __launch_bounds__(256) k_place(KArgs a, long long total_n) {
-    place_rows(a, total_n);
-}
 
 // ------------------------------------------------------------ k_sweeps
 // Grid-wide barrier of a cooperative launch (every block resident), on the
