@@ -724,79 +724,12 @@ __global__ void __launch_bounds__(256) k_bw_ud_rho(BArgs a) {
 }
 
 // ------------------------------------------------------------------ leaves
-// The leaf solve re-run with the full eigenvector matrix V (column x of V in
-// lane x), then
+// The leaf's whole eigenvector matrix V, kept by the checkpointing forward
+// (k_leaf_full, column x of V in lane x), then
 //   Abar = V sym(diag(glam) + F o (V^T Vbar)) V^T,  F_kl = 1/(lambda_l -
 //   lambda_k), Vbar nonzero only in rows 0 and s-1 (the boundary rows),
 // gD = diag(Abar), gE = 2 sign(E) Abar_{j,j+1}, and the corner corrections
 // of the cuts.
-template <int M>
-__device__ __forceinline__ void leaf_round_v(double (&a)[16], double (&v)[16],
-                                             int x, double th) {
-    const bool isp = x < (x ^ M);
-    const double mydiag = a[0];
-    const double odiag = __shfl_xor_sync(kFull, mydiag, M);
-    const double apq_mine = a[M];
-    const double app = isp ? mydiag : odiag;
-    const double aqq = isp ? odiag : mydiag;
-    double c = 1.0, sn = 0.0, t = 0.0;
-    int rot = 0;
-    if (fabs(apq_mine) > th) {
-        const double theta = (aqq - app) / (2.0 * apq_mine);
-        if (fabs(theta) > 1.0e150) {
-            t = 0.5 / theta;
-        } else {
-            t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
-        }
-        c = 1.0 / sqrt(t * t + 1.0);
-        sn = t * c;
-        rot = 1;
-    }
-    {
-        const double co = __shfl_xor_sync(kFull, c, M);
-        const double so = __shfl_xor_sync(kFull, sn, M);
-        const double to = __shfl_xor_sync(kFull, t, M);
-        const int ro = __shfl_xor_sync(kFull, rot, M);
-        if (!isp) {
-            c = co;
-            sn = so;
-            t = to;
-            rot = ro;
-        }
-    }
-    const double apq_o = __shfl_xor_sync(kFull, apq_mine, M);
-    const double apq = isp ? apq_mine : apq_o;
-    const double sgx = isp ? -1.0 : 1.0;
-    double b[16];
-#pragma unroll
-    for (int j = 0; j < 16; ++j) {
-        const double other = __shfl_xor_sync(kFull, a[j ^ M], M);
-        b[j] = c * a[j] + sgx * sn * other;
-    }
-#pragma unroll
-    for (int j = 0; j < 16; ++j) {
-        const double other = __shfl_xor_sync(kFull, v[j], M);
-        v[j] = c * v[j] + sgx * sn * other;
-    }
-#pragma unroll
-    for (int j = 0; j < 16; ++j) {
-        if (j < (j ^ M)) {
-            const int jj = j ^ M;
-            const double cr = __shfl_xor_sync(kFull, c, j);
-            const double sr = __shfl_xor_sync(kFull, sn, j);
-            const int r = x ^ j;
-            const double sgr = (r < (r ^ M)) ? -1.0 : 1.0;
-            const double bj = b[j], bjj = b[jj];
-            a[j] = cr * bj + sgr * sr * bjj;
-            a[jj] = cr * bjj - sgr * sr * bj;
-        }
-    }
-    if (rot) {
-        a[0] = isp ? app - t * apq : aqq + t * apq;
-        a[M] = 0.0;
-    }
-}
-
 __global__ void __launch_bounds__(kLeafWarps * 32)
     k_bw_leaf(BArgs a, long long total_leaves) {
     __shared__ double sV[kLeafWarps * 2][16][17];
@@ -807,7 +740,6 @@ __global__ void __launch_bounds__(kLeafWarps * 32)
     const int x = lane & 15;
     const int half = lane >> 4;
     const int slot = (threadIdx.x >> 5) * 2 + half;
-    const double eps = DBL_EPSILON;
     const Ws &w = a.w;
     const long long pairs = (total_leaves + 1) / 2;
     for (long long pr = (long long)blockIdx.x * kLeafWarps + (threadIdx.x >> 5); pr < pairs;
@@ -820,69 +752,25 @@ __global__ void __launch_bounds__(kLeafWarps * 32)
             LG = leaf_geom(a.F, leaf);
             s = LG.s;
         }
-        double dx = 0.0, ex = 0.0, exm1 = 0.0;
+        // the forward's leaf (k_leaf_full): eigenvalue of rank x and its
+        // eigenvector, in the scaled problem of the forward (the gradient
+        // of a homogeneous map is scale-free, so nothing else changes)
+        double v[16];
+        double lamx = 0.0;
         if (x < s) {
-            // the scaled problem of the forward (the gradient of a
-            // homogeneous map is scale-free, so nothing else changes)
-            const double sc = inst_scale(a.w, LG.inst);
-            dx = sc * a.D[LG.gstart + x];
-            if (x == 0 && LG.gstart > LG.istart) {
-                dx -= sc * fabs(a.E[LG.gstart - 1]);
-            }
-            if (x == s - 1 && LG.gstart + s < LG.iend) {
-                dx -= sc * fabs(a.E[LG.gstart + s - 1]);
-            }
-            if (x + 1 < s) {
-                ex = sc * fabs(a.E[LG.gstart + x]);
-            }
-            if (x >= 1) {
-                exm1 = sc * fabs(a.E[LG.gstart + x - 1]);
-            }
-        }
-        double reg[16], v[16];
-        const int jup = x ^ (x + 1);
-        const int jdn = x ^ (x - 1);
+            const long long o = LG.gstart + x;
+            lamx = w.leafl[o];
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-            reg[j] = (j == 0) ? dx : ((j == jup) ? ex : ((j == jdn) ? exm1 : 0.0));
-            v[j] = (j == x) ? 1.0 : 0.0;
-        }
-        const double amax = half_max(fmax(fabs(dx), fmax(ex, exm1)));
-        const double th = 1.0e-3 * eps * amax;
-        for (int sweep = 0; sweep < 40; ++sweep) {
-            double off = 0.0;
-#pragma unroll
-            for (int j = 1; j < 16; ++j) {
-                off = fmax(off, fabs(reg[j]));
+            for (int j = 0; j < 16; ++j) {
+                v[j] = w.leafv[o * 16 + j];
             }
-            off = half_max(off);
-            if (!__any_sync(kFull, off > th)) {
-                break;
-            }
-            leaf_round_v<1>(reg, v, x, th);
-            leaf_round_v<2>(reg, v, x, th);
-            leaf_round_v<3>(reg, v, x, th);
-            leaf_round_v<4>(reg, v, x, th);
-            leaf_round_v<5>(reg, v, x, th);
-            leaf_round_v<6>(reg, v, x, th);
-            leaf_round_v<7>(reg, v, x, th);
-            leaf_round_v<8>(reg, v, x, th);
-            leaf_round_v<9>(reg, v, x, th);
-            leaf_round_v<10>(reg, v, x, th);
-            leaf_round_v<11>(reg, v, x, th);
-            leaf_round_v<12>(reg, v, x, th);
-            leaf_round_v<13>(reg, v, x, th);
-            leaf_round_v<14>(reg, v, x, th);
-            leaf_round_v<15>(reg, v, x, th);
-        }
-        // rank of my eigenvalue in the ascending order of the forward sort
-        const double lam = (x < s) ? reg[0] : INFINITY;
-        int rank = 0;
+        } else {
 #pragma unroll
-        for (int y = 0; y < 16; ++y) {
-            const double ly = __shfl_sync(kFull, lam, (lane & 16) | y);
-            rank += (ly < lam || (ly == lam && y < x)) ? 1 : 0;
+            for (int j = 0; j < 16; ++j) {
+                v[j] = 0.0;
+            }
         }
+        const int rank = x; // stored in ascending order
         double gmu = 0.0, gf = 0.0, gl = 0.0;
         if (x < s) {
             const long long o = LG.gstart + rank;
@@ -900,7 +788,7 @@ __global__ void __launch_bounds__(kLeafWarps * 32)
         for (int j = 0; j < 16; ++j) {
             vlast = (j == s - 1) ? v[j] : vlast;
         }
-        sLam[slot][x] = (x < s) ? reg[0] : 0.0;
+        sLam[slot][x] = lamx;
         sV0[slot][x] = v0;
         sV1[slot][x] = vlast;
         sGf[slot][x] = gf;

@@ -142,7 +142,8 @@ bool build_forest(int B, const long long *off, HostForest *f) {
 // Workspace descriptor: every array with its element size, its length
 // class and whether a checkpointing workspace keeps one slice per level
 // (the arrays the adjoint reads back).
-enum CountKind { CN_NT, CN_NP, CN_NN, CN_NN1, CN_ITW, CN_ITC, CN_B1, CN_B, CN_NODEPRE, CN_INST };
+enum CountKind { CN_NT, CN_NT16, CN_NP, CN_NN, CN_NN1, CN_ITW, CN_ITC, CN_B1, CN_B, CN_NODEPRE,
+                 CN_INST };
 
 struct SlotDesc {
     int kind;        // 0 double*, 1 int*, 2 long long*
@@ -196,11 +197,13 @@ const SlotDesc kSlots[] = {
     SD(bzz, CN_NT, false, true), SD(bgw, CN_NT, false, true),
     SD(bpd, CN_NP, false, true), SD(bpz, CN_NP, false, true), SD(bpf, CN_NP, false, true),
     SD(bpl, CN_NP, false, true), SD(rkr, CN_NP, false, true), SD(wtmp, CN_NT, false, true),
+    SD(leafv, CN_NT16, false, true), SD(leafl, CN_NT, false, true),
 };
 
 long long slot_count(CountKind c, const HostForest &f, const Layout &L) {
     switch (c) {
     case CN_NT: return L.nt;
+    case CN_NT16: return 16 * L.nt;
     case CN_NP: return L.np;
     case CN_NN: return L.nn0;
     case CN_NN1: return L.nn0 + 1;
@@ -592,9 +595,18 @@ brdc_status run_forest(brdc_handle h, const HostForest &hf, const Layout &L,
     a.E = E;
     a.W = W;
     a.lanes_target = h->lanes_target;
-    // leaves and the lowest merge levels
+    // leaves and the lowest merge levels; a checkpointing forward solves the
+    // leaves first, keeping their whole eigenvector matrices for the adjoint
     const int sub = effective_sub_levels(h, hf);
     const int fused = std::min(sub, hf.max_levels);
+    const long long leaf_per = 2LL * kLeafWarps; // leaves per block
+    long long leaf_grid = (hf.leaves + leaf_per - 1) / leaf_per;
+    leaf_grid = std::max<long long>(1, std::min<long long>(leaf_grid, (long long)h->sm_count * 16));
+    if (L.ckpt) {
+        k_leaf_full<<<(unsigned)leaf_grid, kLeafWarps * 32, 0, s>>>(a, hf.leaves);
+        BRDC_CUDA(h, "brdc.leaf_full", cudaGetLastError());
+        ++h->launches;
+    }
     if (sub > 0) {
         SubArgs A{};
         A.a = a;
@@ -609,6 +621,7 @@ brdc_status run_forest(brdc_handle h, const HostForest &hf, const Layout &L,
         A.out_l = (fused & 1) ? w.nl : w.cl;
         A.levels = sub;
         A.ckpt = L.ckpt ? 1 : 0;
+        A.leaves_done = L.ckpt ? 1 : 0;
         long long subs = 0;
         for (int b = 0; b < hf.B; ++b) {
             subs += subtrees_of(hf.lev[b], sub);
@@ -631,13 +644,11 @@ brdc_status run_forest(brdc_handle h, const HostForest &hf, const Layout &L,
             std::swap(a.w.cl, a.w.nl);
         }
     } else {
-        const long long per = 2LL * kLeafWarps; // leaves per block
-        long long grid = (hf.leaves + per - 1) / per;
-        grid = std::min<long long>(grid, (long long)h->sm_count * 16);
-        grid = std::max<long long>(grid, 1);
-        k_leaf<<<(unsigned)grid, kLeafWarps * 32, 0, s>>>(a, hf.leaves);
-        BRDC_CUDA(h, "brdc.leaf", cudaGetLastError());
-        ++h->launches;
+        if (!L.ckpt) {
+            k_leaf<<<(unsigned)leaf_grid, kLeafWarps * 32, 0, s>>>(a, hf.leaves);
+            BRDC_CUDA(h, "brdc.leaf", cudaGetLastError());
+            ++h->launches;
+        }
         mark(h, 2);
         h->fused_levels = 0;
     }

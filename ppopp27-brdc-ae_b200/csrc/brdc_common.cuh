@@ -153,6 +153,8 @@ struct Ws {
     double *bpd, *bpz, *bpf, *bpl;               // per pole (padded)
     double *rkr;                                 // per root: its drho term
     double *wtmp;                                // eigenvalues of the re-run
+    double *leafv, *leafl;                       // checkpointed leaves: eigenvectors
+                                                 // (16 per row), eigenvalues
 };
 
 struct Layout {

@@ -67,6 +67,13 @@ struct KArgs {
 constexpr int kLeafWarps = 4;
 constexpr unsigned kFull = 0xffffffffu;
 
+// The arithmetic of a leaf rotation, spelled out (explicit FMAs and rounded
+// products, nothing left for the compiler to contract), so that leaf_round
+// and leaf_round_v produce bit for bit the same matrix and rows.
+__device__ __forceinline__ double leaf_rot(double c, double x, double sgs, double y) {
+    return fma(c, x, __dmul_rn(sgs, y)); // c x + (sg s) y
+}
+
 template <int M>
 __device__ __forceinline__ void leaf_round(double (&a)[16], double &v0,
                                            double &v1, int x, double th) {
@@ -83,10 +90,10 @@ __device__ __forceinline__ void leaf_round(double (&a)[16], double &v0,
         if (fabs(theta) > 1.0e150) {
             t = 0.5 / theta;
         } else {
-            t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+            t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(fma(theta, theta, 1.0)));
         }
-        c = 1.0 / sqrt(t * t + 1.0);
-        sn = t * c;
+        c = 1.0 / sqrt(fma(t, t, 1.0));
+        sn = __dmul_rn(t, c);
         rot = 1;
     }
     // the lane holding the larger index adopts its partner's rotation, so
@@ -111,13 +118,13 @@ __device__ __forceinline__ void leaf_round(double (&a)[16], double &v0,
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
         const double other = __shfl_xor_sync(kFull, a[j ^ M], M);
-        b[j] = c * a[j] + sgx * sn * other;
+        b[j] = leaf_rot(c, a[j], __dmul_rn(sgx, sn), other);
     }
     {
         const double o0 = __shfl_xor_sync(kFull, v0, M);
         const double o1 = __shfl_xor_sync(kFull, v1, M);
-        v0 = c * v0 + sgx * sn * o0;
-        v1 = c * v1 + sgx * sn * o1;
+        v0 = leaf_rot(c, v0, __dmul_rn(sgx, sn), o0);
+        v1 = leaf_rot(c, v1, __dmul_rn(sgx, sn), o1);
     }
     // rows: A' = J^T B; rows x^j and x^j^M use the rotation of lane x^j
 #pragma unroll
@@ -129,12 +136,12 @@ __device__ __forceinline__ void leaf_round(double (&a)[16], double &v0,
             const int r = x ^ j;
             const double sgr = (r < (r ^ M)) ? -1.0 : 1.0;
             const double bj = b[j], bjj = b[jj];
-            a[j] = cr * bj + sgr * sr * bjj;
-            a[jj] = cr * bjj - sgr * sr * bj;
+            a[j] = leaf_rot(cr, bj, __dmul_rn(sgr, sr), bjj);
+            a[jj] = leaf_rot(cr, bjj, -__dmul_rn(sgr, sr), bj);
         }
     }
     if (rot) {
-        a[0] = isp ? app - t * apq : aqq + t * apq;
+        a[0] = isp ? fma(-t, apq, app) : fma(t, apq, aqq);
         a[M] = 0.0;
     }
 }
@@ -239,6 +246,216 @@ __device__ inline int leaf_solve(const KArgs &a, const LeafGeom &G, int s, int x
     *v0_out = v0;
     *v1_out = v1;
     return sweep;
+}
+
+// leaf_round on the whole eigenvector matrix (lane x holds column x in v):
+// the same rotation, applied to every row with leaf_round's arithmetic.
+template <int M>
+__device__ __forceinline__ void leaf_round_v(double (&a)[16], double (&v)[16],
+                                             int x, double th) {
+    const bool isp = x < (x ^ M);
+    const double mydiag = a[0];
+    const double odiag = __shfl_xor_sync(kFull, mydiag, M);
+    const double apq_mine = a[M];
+    const double app = isp ? mydiag : odiag;
+    const double aqq = isp ? odiag : mydiag;
+    double c = 1.0, sn = 0.0, t = 0.0;
+    int rot = 0;
+    if (fabs(apq_mine) > th) {
+        const double theta = (aqq - app) / (2.0 * apq_mine);
+        if (fabs(theta) > 1.0e150) {
+            t = 0.5 / theta;
+        } else {
+            t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(fma(theta, theta, 1.0)));
+        }
+        c = 1.0 / sqrt(fma(t, t, 1.0));
+        sn = __dmul_rn(t, c);
+        rot = 1;
+    }
+    {
+        const double co = __shfl_xor_sync(kFull, c, M);
+        const double so = __shfl_xor_sync(kFull, sn, M);
+        const double to = __shfl_xor_sync(kFull, t, M);
+        const int ro = __shfl_xor_sync(kFull, rot, M);
+        if (!isp) {
+            c = co;
+            sn = so;
+            t = to;
+            rot = ro;
+        }
+    }
+    const double apq_o = __shfl_xor_sync(kFull, apq_mine, M);
+    const double apq = isp ? apq_mine : apq_o;
+    const double sgx = isp ? -1.0 : 1.0;
+    double b[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        const double other = __shfl_xor_sync(kFull, a[j ^ M], M);
+        b[j] = leaf_rot(c, a[j], __dmul_rn(sgx, sn), other);
+    }
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        const double other = __shfl_xor_sync(kFull, v[j], M);
+        v[j] = leaf_rot(c, v[j], __dmul_rn(sgx, sn), other);
+    }
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        if (j < (j ^ M)) {
+            const int jj = j ^ M;
+            const double cr = __shfl_xor_sync(kFull, c, j);
+            const double sr = __shfl_xor_sync(kFull, sn, j);
+            const int r = x ^ j;
+            const double sgr = (r < (r ^ M)) ? -1.0 : 1.0;
+            const double bj = b[j], bjj = b[jj];
+            a[j] = leaf_rot(cr, bj, __dmul_rn(sgr, sr), bjj);
+            a[jj] = leaf_rot(cr, bjj, -__dmul_rn(sgr, sr), bj);
+        }
+    }
+    if (rot) {
+        a[0] = isp ? fma(-t, apq, app) : fma(t, apq, aqq);
+        a[M] = 0.0;
+    }
+}
+
+// leaf_solve with the whole eigenvector matrix, for a checkpointing
+// forward (the adjoint of a leaf needs all of it): the same sweeps and
+// rotations, so rows 0 and s-1 of v are bit for bit leaf_solve's v0 and v1,
+// and the same sort.  Lane x returns the eigenvalue of rank x and its
+// eigenvector (rows 0..15, zero past s).
+__device__ inline int leaf_solve_full(const KArgs &a, const LeafGeom &G, int s, int x,
+                                      double *key_out, double (&v)[16]) {
+    const double eps = DBL_EPSILON;
+    double dx = 0.0, ex = 0.0, exm1 = 0.0;
+    if (x < s) {
+        const double sc = inst_scale(a.w, G.inst);
+        dx = sc * a.D[G.gstart + x];
+        if (x == 0 && G.gstart > G.istart) {
+            dx -= sc * fabs(a.E[G.gstart - 1]);
+        }
+        if (x == s - 1 && G.gstart + s < G.iend) {
+            dx -= sc * fabs(a.E[G.gstart + s - 1]);
+        }
+        if (x + 1 < s) {
+            ex = sc * fabs(a.E[G.gstart + x]);
+        }
+        if (x >= 1) {
+            exm1 = sc * fabs(a.E[G.gstart + x - 1]);
+        }
+    }
+    double reg[16];
+    const int jup = x ^ (x + 1);
+    const int jdn = x ^ (x - 1);
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        reg[j] = (j == 0) ? dx : ((j == jup) ? ex : ((j == jdn) ? exm1 : 0.0));
+        v[j] = (j == x) ? 1.0 : 0.0;
+    }
+    const double amax = half_max(fmax(fabs(dx), fmax(ex, exm1)));
+    const double th = 1.0e-3 * eps * amax;
+    int sweep = 0;
+    for (; sweep < 40; ++sweep) {
+        double off = 0.0;
+#pragma unroll
+        for (int j = 1; j < 16; ++j) {
+            off = fmax(off, fabs(reg[j]));
+        }
+        off = half_max(off);
+        if (!__any_sync(kFull, off > th)) {
+            break;
+        }
+        leaf_round_v<1>(reg, v, x, th);
+        leaf_round_v<2>(reg, v, x, th);
+        leaf_round_v<3>(reg, v, x, th);
+        leaf_round_v<4>(reg, v, x, th);
+        leaf_round_v<5>(reg, v, x, th);
+        leaf_round_v<6>(reg, v, x, th);
+        leaf_round_v<7>(reg, v, x, th);
+        leaf_round_v<8>(reg, v, x, th);
+        leaf_round_v<9>(reg, v, x, th);
+        leaf_round_v<10>(reg, v, x, th);
+        leaf_round_v<11>(reg, v, x, th);
+        leaf_round_v<12>(reg, v, x, th);
+        leaf_round_v<13>(reg, v, x, th);
+        leaf_round_v<14>(reg, v, x, th);
+        leaf_round_v<15>(reg, v, x, th);
+    }
+    // bitonic sort of (eigenvalue, column) within the half-warp, as leaf_solve
+    double key = (x < s) ? reg[0] : INFINITY;
+    int col = x;
+#pragma unroll
+    for (int size = 2; size <= 16; size <<= 1) {
+#pragma unroll
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            const double ok = __shfl_xor_sync(kFull, key, stride);
+            const int oc = __shfl_xor_sync(kFull, col, stride);
+            double ov[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                ov[j] = __shfl_xor_sync(kFull, v[j], stride);
+            }
+            const bool up = (size == 16) || ((x & size) == 0);
+            const bool lower = ((x & stride) == 0);
+            const bool take_min = (up == lower);
+            const bool swap = take_min ? (ok < key || (ok == key && oc < col))
+                                       : (ok > key || (ok == key && oc > col));
+            if (swap) {
+                key = ok;
+                col = oc;
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    v[j] = ov[j];
+                }
+            }
+        }
+    }
+    *key_out = key;
+    return sweep;
+}
+
+// The leaves of a checkpointing forward: leaf_solve_full, then the leaf
+// outputs as k_leaf writes them plus, for the adjoint, every eigenvalue
+// (leafl) and eigenvector (leafv, 16 entries per column) in sorted order.
+__global__ void __launch_bounds__(kLeafWarps * 32)
+    k_leaf_full(KArgs a, long long total_leaves) {
+    const int lane = threadIdx.x & 31;
+    const int x = lane & 15;
+    const int half = lane >> 4;
+    int sweeps_max = 0;
+    const long long pairs = (total_leaves + 1) / 2;
+    for (long long pr = (long long)blockIdx.x * kLeafWarps + (threadIdx.x >> 5); pr < pairs;
+         pr += (long long)gridDim.x * kLeafWarps) {
+        const long long leaf = 2 * pr + half;
+        const bool has = leaf < total_leaves;
+        LeafGeom G{};
+        int s = 0;
+        if (has) {
+            G = leaf_geom(a.F, leaf);
+            s = G.s;
+        }
+        double key, v[16];
+        const int sweep = leaf_solve_full(a, G, s, x, &key, v);
+        sweeps_max = sweeps_max > sweep ? sweeps_max : sweep;
+        if (x < s) {
+            const long long o = G.gstart + x;
+            double vlast = 0.0;
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                vlast = (j == s - 1) ? v[j] : vlast;
+                a.w.leafv[o * 16 + j] = (j < s) ? v[j] : 0.0;
+            }
+            a.w.leafl[o] = key;
+            if (G.top) {
+                a.W[o] = key * inst_unscale(a.w, G.inst);
+            } else {
+                a.w.cd[o] = key;
+                a.w.cf[o] = v[0];
+                a.w.cl[o] = vlast;
+            }
+        }
+    }
+    if (lane == 0 && sweeps_max > 0) {
+        atomicMax(&a.w.hdr->leaf_sweeps_max, sweeps_max);
+    }
 }
 
 __global__ void __launch_bounds__(kLeafWarps * 32)

@@ -34,6 +34,7 @@ struct SubArgs {
     double *out_d, *out_f, *out_l; // inputs of the first per-level merge
     int levels;               // fused merge levels (1..kSubMaxLevels)
     int ckpt;                 // write each fused level's state for the adjoint
+    int leaves_done;          // the leaves were solved by k_leaf_full: read them
 };
 
 template <int kSubRows>
@@ -163,7 +164,16 @@ __global__ void __launch_bounds__(kSubRows, 512 / kSubRows) k_subtree(SubArgs A)
     }
 
     // ---------------------------------------------------------- leaves
-    {
+    if (A.leaves_done) {
+        // solved by k_leaf_full (checkpointing forward): this subtree's
+        // rows, sorted per leaf with their first and last rows (a one-leaf
+        // instance is already in W)
+        for (int r = x; r < R; r += kSubRows) {
+            S.cd[r] = a.w.cd[gsub + r];
+            S.cf[r] = a.w.cf[gsub + r];
+            S.cl[r] = a.w.cl[gsub + r];
+        }
+    } else {
         int sweeps_max = 0;
         const int nleaves = 1 << Ls;
         const int xl = lane & 15, half = lane >> 4;
