@@ -1319,7 +1319,8 @@ brdc_status run_backward(brdc_handle h, const HostForest &hf, const Layout &L,
     }
     double *par[3] = {w.bnd, w.bnf, w.bnl};
     double *out[3] = {w.bcd, w.bcf, w.bcl};
-    const int wgrid = h->sm_count * 2;
+    // k_bw_roots and k_bw_poles: 64 registers or fewer, four blocks per SM
+    const int wgrid = h->sm_count * 4;
     long long dgrid = (4 * nt + 255) / 256;
     dgrid = std::max<long long>(1, std::min<long long>(dgrid, (long long)h->sm_count * 16));
     for (int k = hf.max_levels - 1; k >= 0; --k) {
