@@ -474,7 +474,8 @@ __global__ void __launch_bounds__(T, 1) k_level(KArgs a) {
     cl.sync();
 
     // ------------------------------------------------ placement
-    // ascending order, ties: roots, small-z deflated, rotated out (k_place)
+    // ascending order, ties: roots, small-z deflated, rotated out (as
+    // place_rows)
     const int ndz = m - Kz, ndg = Kz - K;
     const long long po = G.poff;
     for (int i = x; i < K; i += T) {

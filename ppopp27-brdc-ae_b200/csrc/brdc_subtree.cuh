@@ -9,13 +9,15 @@
 //   rank merge of the two children; tolerance tol = 8 eps max(max|d|,
 //   max|z|); small-z compaction (merged order kept); close-pole Givens
 //   chains; pole compaction; secular roots by the state machine of
-//   brdc_secular.cuh (one thread per root); Loewner weights; first/last
-//   boundary rows; placement in ascending order.
-// Only the order of a few floating-point sums differs (sum z^2 and the
-// secular sweeps are accumulated by one thread per root), so deflation is
-// decided exactly as the per-level path decides it.  In checkpoint mode
-// every fused level's state is also written to its workspace slice, in the
-// layout the per-level kernels use, for the adjoint.
+//   brdc_secular.cuh (rounds over the live roots, then one warp per root
+//   for the slow tail); Loewner weights; first/last boundary rows;
+//   placement in ascending order.
+// Only the order of a few floating-point sums differs (sum z^2 by warp
+// partials, the secular sweeps by the lanes a round gives each root), so
+// deflation is decided exactly as the per-level path decides it.  In
+// checkpoint mode the leaves come from k_leaf_full, and every fused level's
+// state is also written to its workspace slice, in the layout the per-level
+// kernels use, for the adjoint.
 #pragma once
 
 #include "brdc_kernels.cuh"
