@@ -17,6 +17,12 @@ bytes, clocks sampled during the timed loop, and the CPU baseline: the
 oracle (C restatement of the reference's DSTEDC_DC_BR, OpenMP on all host
 threads) timed on a bounded sample of the same workload.
 
+--input PATH.de.bin or --data MODE[:N] replace the headline input with a
+file in the reference's .de.bin format or one of the reference's own
+generators (its GPU bench's data modes, or the paper's DLATMS
+spectrum-prescribed matrices as spectrum-MODE); the default line also carries
+those inputs at N = 8,192 under "paper_inputs".
+
 --impl reference times the reference's CPU implementation of this path
 (the oracle port; no Fortran compiler exists in the image) on the same
 workload and prints the same metric with "impl": "reference".
@@ -131,11 +137,9 @@ def cpu_reference_times(d, e, budget_s, min_solves=1, max_solves=50):
 
 
 def run_reference_arm(args, rank):
-    from brdc import families
-
     if rank != 0:
         return
-    d, e = families.generate(FAMILY_HEAD, N_HEAD)
+    d, e, name, data, _ = load_workload(args.input, args.data)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
 
@@ -151,7 +155,7 @@ def run_reference_arm(args, rank):
     v = float(np.mean(times))
     line = {
         "impl": "reference",
-        "metric": METRIC,
+        "metric": f"ms/solve FP64, {name}" if (args.input or args.data) else METRIC,
         "value": v,
         "unit": "ms",
         "n_gpus": args.gpus,
@@ -162,11 +166,10 @@ def run_reference_arm(args, rank):
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64",
-        "data": "synthetic (seeded uniform U(0,1) family)",
-        "config": {"workload": f"plain values-only BR solve, {FAMILY_HEAD} family, N={N_HEAD}",
-                   "n": N_HEAD, "family": FAMILY_HEAD},
+        "data": data,
+        "config": {"workload": name, "n": len(d)},
         "cpu_baseline": {"value": v, "unit": "ms", "cores": threads, "kind": "port",
-                         "sample": f"{args.steps} full solves of the headline input"},
+                         "sample": f"{args.steps} full solves of the workload"},
         "e2e": {"value": v, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "reference CPU path DSTEDC_DC_BR restated in C (oracle/brdc_oracle.c); "
                 "no Fortran compiler in the image",
@@ -215,6 +218,12 @@ def main():
                     help="family:n[:solves[:bwd]] -- run that many plain solves (default 1) of "
                          "the seeded instance, each followed by the adjoint with bwd, and exit; "
                          "a fixed launch sequence for profilers")
+    ap.add_argument("--input", default=None,
+                    help="solve the tridiagonal of a .de.bin file instead of the headline input")
+    ap.add_argument("--data", default=None,
+                    help="MODE[:N] -- solve one of the reference's inputs instead: bench, test, "
+                         "normal, uniform, toeplitz, clustered (its GPU bench's generators) or "
+                         "spectrum-{uniform,normal,clustered,toeplitz} (the paper's DLATMS cache)")
     args = ap.parse_args()
     if args.profile_case:
         run_profile_case(args.profile_case)
@@ -227,6 +236,10 @@ def main():
 
     if args.impl == "reference":
         run_reference_arm(args, rank)
+        return
+    if args.input or args.data:
+        if rank == 0:
+            run_input_workload(args)
         return
 
     import torch
@@ -385,6 +398,143 @@ def bench_config2(torch, families, solver, flush):
     return table
 
 
+def measure_e2e(torch, solver, D, E, W, ws, d, e, flush, warmup, steps):
+    """The solve end to end through the C ABI: pinned host D and E copied in,
+    the solve, W copied back, all inside the timed interval."""
+    hD = torch.tensor(d).pin_memory()
+    hE = torch.tensor(e).pin_memory()
+    hW = torch.empty(len(d), dtype=torch.float64).pin_memory()
+    stream = torch.cuda.current_stream()
+    e2e = []
+    for i in range(warmup + steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        D.copy_(hD, non_blocking=True)
+        E.copy_(hE, non_blocking=True)
+        solver.dstebr(D, E, W=W, workspace=ws)
+        hW.copy_(W, non_blocking=True)
+        e1.record(stream)
+        e1.synchronize()
+        if i >= warmup:
+            e2e.append(e0.elapsed_time(e1))
+    return {"value": float(np.mean(e2e)), "unit": "ms",
+            "h2d_bytes_per_step": int(hD.numel() * 8 + hE.numel() * 8),
+            "d2h_bytes_per_step": int(hW.numel() * 8)}
+
+
+def load_workload(input_path, data_spec):
+    """(d, e, workload name, data description, exact spectrum or None).
+
+    --input PATH reads a .de.bin file (compact or dense payload);
+    --data MODE[:N] generates one of the reference's inputs: the GPU bench's
+    modes (bench, test, normal, uniform, toeplitz, clustered) or the paper's
+    spectrum-prescribed cache (spectrum-uniform, spectrum-normal,
+    spectrum-clustered through LAPACK DLATMS, spectrum-toeplitz); N defaults
+    to 65,536.  Without either, the headline uniform family."""
+    from brdc import families, inputs
+
+    if input_path:
+        d, e = inputs.read_de(input_path)
+        return d, e, f"file {os.path.basename(input_path)}, N={len(d)}", "file (.de.bin)", None
+    if data_spec:
+        mode, _, n = data_spec.partition(":")
+        n = int(n) if n else N_HEAD
+        if mode.startswith("spectrum-"):
+            m = mode[len("spectrum-"):]
+            d, e, info, eig = inputs.spectrum_case(m, n)
+            if info != 0:
+                raise RuntimeError(f"DLATMS info {info} for {mode}:{n}")
+            exact = np.sort(eig) if eig is not None else families.toeplitz_eigenvalues(n, 2.0, 0.25)
+            return (d, e, f"spectrum-prescribed {m} (paper cache), N={n}",
+                    "LAPACK DLATMS spectrum-prescribed tridiagonal" if eig is not None
+                    else "Toeplitz D=2, E=1/4", exact)
+        d, e = inputs.generate(mode, n)
+        exact = families.toeplitz_eigenvalues(n, 2.0, 0.25) if mode == "toeplitz" else None
+        return d, e, f"reference GPU-bench data mode {mode}, N={n}", f"reference generator ({mode})", exact
+    d, e = families.generate(FAMILY_HEAD, N_HEAD)
+    return (d, e, f"plain values-only BR solve, {FAMILY_HEAD} family, N={N_HEAD}",
+            "synthetic (seeded uniform U(0,1) family)", None)
+
+
+def input_error(d, e, w, exact):
+    """max |w - lambda| / ||T||: against the exact spectrum where the input
+    prescribes one, else against LAPACK bisection on sampled eigenvalues."""
+    if exact is not None:
+        return float(np.max(np.abs(w - exact)) / max(np.max(np.abs(exact)), 1e-300))
+    return lapack_sample_error(d, e, w)
+
+
+def run_input_workload(args):
+    """One plain solve per step of the workload --input or --data names, on
+    one GPU; the line carries the same timing keys as the headline's."""
+    import torch
+
+    import brdc
+
+    d, e, name, data, exact = load_workload(args.input, args.data)
+    n = len(d)
+    solver = brdc.Solver()
+    D = torch.tensor(d, device="cuda")
+    E = torch.tensor(e if len(e) else np.zeros(1), device="cuda")
+    W = torch.empty(n, dtype=torch.float64, device="cuda")
+    ws = solver.workspace(n)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    tuning = solver.autotune(D, E, workspace=ws)
+    for _ in range(args.warmup):
+        solver.dstebr(D, E, W=W, workspace=ws)
+    torch.cuda.synchronize()
+    clocks_path = os.path.join("/tmp", f"brdc_clocks_{os.getpid()}.csv")
+    sampler = start_clock_sampler(clocks_path)
+    times = time_solves(torch, solver, D, E, W, ws, args.steps, flush)
+    torch.cuda.synchronize()
+    clocks = stop_clock_sampler(sampler, clocks_path, torch.cuda.current_device())
+    ms = float(np.mean(times))
+    err = input_error(d, e, W.cpu().numpy(), exact)
+    solver.set_timing(True)
+    solver.dstebr(D, E, W=W, workspace=ws)
+    launches = solver.last_timings()["launches"]
+    solver.set_timing(False)
+    line = {
+        "metric": f"ms/solve FP64, {name}", "value": ms, "unit": "ms", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": data,
+        "config": {"workload": name, "n": n, "tuning": tuning,
+                   "l2": "flushed by a 256 MiB write before every timed solve (outside the timed interval)"},
+        "info": solver.info(n, ws), "max_err_over_normT": err,
+        "e2e": measure_e2e(torch, solver, D, E, W, ws, d, e, flush, args.warmup, args.steps),
+        "gpu_launches": launches, "ms_median": float(np.median(times)), "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    solver.close()
+
+
+def bench_paper_inputs(torch, solver, flush, n=8192):
+    """The reference's own inputs at one order: its GPU bench's data modes
+    and the paper's spectrum-prescribed matrices (DLATMS), each solved with
+    the default launch shapes -- median ms of 5 solves and the max error over
+    ||T|| (against the prescribed spectrum where there is one)."""
+    from brdc import inputs
+
+    out = {"n": n}
+    ws = solver.workspace(n)
+    W = torch.empty(n, dtype=torch.float64, device="cuda")
+    specs = [m for m in inputs.GPU_BENCH_MODES] + ["spectrum-" + m for m in ("uniform", "normal", "clustered")]
+    for spec in specs:
+        d, e, _, _, exact = load_workload(None, f"{spec}:{n}")
+        Dt = torch.tensor(d, device="cuda")
+        Et = torch.tensor(e, device="cuda")
+        for _ in range(3):
+            solver.dstebr(Dt, Et, W=W, workspace=ws)
+        torch.cuda.synchronize()
+        tt = time_solves(torch, solver, Dt, Et, W, ws, 5, flush)
+        out[spec] = {"ms": float(np.median(tt)),
+                     "max_err_over_normT": input_error(d, e, W.cpu().numpy(), exact)}
+    solver._ws.clear()
+    return out
+
+
 def collect_extras(torch, brdc, families, solver, D, E, W, ws, d, e, flush, args):
     out = {}
     headline_tuning = solver.tuning()
@@ -445,31 +595,11 @@ def collect_extras(torch, brdc, families, solver, D, E, W, ws, d, e, flush, args
     out["family_tuning"] = fam_tuning
     solver.set_tuning(**headline_tuning)
 
-    # e2e through the C ABI with pinned host buffers
-    hD = torch.tensor(d).pin_memory()
-    hE = torch.tensor(e).pin_memory()
-    hW = torch.empty(N_HEAD, dtype=torch.float64).pin_memory()
-    stream = torch.cuda.current_stream()
-    e2e = []
-    for i in range(args.warmup + args.steps):
-        flush.zero_()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        D.copy_(hD, non_blocking=True)
-        E.copy_(hE, non_blocking=True)
-        solver.dstebr(D, E, W=W, workspace=ws)
-        hW.copy_(W, non_blocking=True)
-        e1.record(stream)
-        e1.synchronize()
-        if i >= args.warmup:
-            e2e.append(e0.elapsed_time(e1))
-    out["e2e"] = {"value": float(np.mean(e2e)), "unit": "ms",
-                  "h2d_bytes_per_step": int(hD.numel() * 8 + hE.numel() * 8),
-                  "d2h_bytes_per_step": int(hW.numel() * 8)}
+    out["e2e"] = measure_e2e(torch, solver, D, E, W, ws, d, e, flush, args.warmup, args.steps)
 
     solver.set_tuning(**DEFAULT_TUNING)
     out["config2"] = bench_config2(torch, families, solver, flush)
+    out["paper_inputs"] = bench_paper_inputs(torch, solver, flush)
     solver.set_tuning(**headline_tuning)
     out["fwd_bwd"] = bench_fwd_bwd(torch, families, solver, flush, args)
     out["batched"] = bench_batched(torch, brdc, families, solver, flush)

@@ -1,9 +1,11 @@
 """Build the sm_100a solver library in-tree.
 
 ``python build.py`` (or ``brdc.build.build()``) compiles
-``csrc/brdc_capi.cu`` with nvcc into ``brdc/libbrdc_b200.so`` and the host
+``csrc/brdc_capi.cu`` with nvcc into ``brdc/libbrdc_b200.so``, the host
 copy of the secular state machine into ``brdc/libbrdc_hostcheck.so`` (used by
-the CPU tests only).  nvcc cross-compiles without a GPU.
+the CPU tests only) and the reference bench's input generators
+(``csrc/brdc_inputs.cpp``) into ``brdc/libbrdc_inputs.so``.  nvcc
+cross-compiles without a GPU.
 """
 from __future__ import annotations
 
@@ -18,6 +20,7 @@ OUT = os.path.join(HERE, "brdc")
 LIB = os.path.join(OUT, "libbrdc_b200.so")
 HOSTLIB = os.path.join(OUT, "libbrdc_hostcheck.so")
 PROBELIB = os.path.join(OUT, "libbrdc_probe.so")
+INPUTLIB = os.path.join(OUT, "libbrdc_inputs.so")
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -46,7 +49,7 @@ def _stale(target: str, deps) -> bool:
 
 def build(force: bool = False, verbose: bool = False) -> str:
     deps = _sources() + [os.path.join(HERE, "..", "include", "brdc.h"), __file__]
-    deps = [d for d in deps if not d.endswith(("probe_fp64.cu", "host_check.cpp"))]
+    deps = [d for d in deps if not d.endswith(("probe_fp64.cu", "host_check.cpp", "brdc_inputs.cpp"))]
     if force or _stale(LIB, deps):
         cmd = [_nvcc(), *NVCC_FLAGS, "-o", LIB, os.path.join(CSRC, "brdc_capi.cu")]
         if verbose:
@@ -55,12 +58,18 @@ def build(force: bool = False, verbose: bool = False) -> str:
     pdeps = [os.path.join(CSRC, "probe_fp64.cu"), os.path.join(CSRC, "brdc_secular.cuh")]
     if force or _stale(PROBELIB, pdeps):
         subprocess.run([_nvcc(), *NVCC_FLAGS, "-o", PROBELIB, pdeps[0]], check=True)
+    cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
     hdeps = [os.path.join(CSRC, "host_check.cpp"), os.path.join(CSRC, "brdc_secular.cuh")]
     if force or _stale(HOSTLIB, hdeps):
-        cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
         subprocess.run(
             [cxx, "-O2", "-fPIC", "-shared", "-std=c++17", "-o", HOSTLIB,
              os.path.join(CSRC, "host_check.cpp")],
+            check=True,
+        )
+    ideps = [os.path.join(CSRC, "brdc_inputs.cpp"), os.path.join(HERE, "..", "include", "brdc_inputs.h")]
+    if force or _stale(INPUTLIB, ideps):
+        subprocess.run(
+            [cxx, "-O2", "-fPIC", "-shared", "-std=c++17", "-o", INPUTLIB, ideps[0]],
             check=True,
         )
     return LIB
