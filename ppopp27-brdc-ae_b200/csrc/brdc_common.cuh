@@ -68,6 +68,8 @@ struct LevelCtl {
     int nbig;        // merges k_level left to the sweep kernels (K > kLvlMaxK)
     unsigned bar_count; // grid barrier of k_sweeps: arrivals, generation
     unsigned bar_gen;
+    int citem;       // next CTA-role item of the secular phase (taken by atomicAdd)
+    int pad_ctl;
     double work_w;   // pole-root pairs (sum K^2) of the warp-role merges
     double work_c;   // and of the CTA-role merges
 };

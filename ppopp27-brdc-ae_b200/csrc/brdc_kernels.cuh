@@ -1459,37 +1459,112 @@ __device__ bool sweep_secular(const KArgs &a, int cta_blocks, double *smem, uint
         return true;
     }
 
+    // CTA role.  A block serves one merge at a time from shared-memory pole
+    // tiles; each warp iterates a run of Rw consecutive roots (lane group grp
+    // on root run + grp) and, once every root of its run has converged,
+    // takes the next run at the following sweep boundary.  Runs come from the
+    // block's current item (R consecutive roots), items from the level's
+    // counter, so lanes stay busy until the level's pool is empty instead of
+    // each item sweeping as long as its slowest root, and the blocks balance
+    // themselves.  A root's arithmetic does not depend on when or where it
+    // runs: its window [pmin, r1] is fixed by its run.
     const int tpr = ctl->tpr_c;
     const int R = kSweepThreads / tpr;
+    const int Rw = 32 / tpr;
+    const int runs = R / Rw; // runs per item (= warps per block)
     const int items = ctl->items_c;
-    const int grp = threadIdx.x / tpr, lane = threadIdx.x % tpr;
-    for (int item = blockIdx.x; item < items; item += cta_blocks) {
-        const int g = item_node(w.items_c, item);
+    const int warp = threadIdx.x >> 5;
+    const int grp = (threadIdx.x & 31) / tpr, lane = threadIdx.x % tpr;
+    __shared__ int s_item;            // item the runs come from (-1: none)
+    __shared__ int s_next;            // next run of s_item
+    __shared__ int s_pending;         // fetched item of the next merge (-1: none yet)
+    __shared__ int s_run[kWarpsPerBlock];
+    if (threadIdx.x == 0) {
+        s_pending = atomicAdd(&w.hdr->lvl[a.k].citem, 1);
+    }
+    __syncthreads();
+    for (;;) {
+        const int first = s_pending;
+        if (first >= items) {
+            break;
+        }
+        const int g = w.items_c[first];
         const NodeGeom G = node_geom(a.F, a.k, g);
         const int K = w.nK[g];
         const double rho = w.nrho[g];
         const long long po = G.poff;
-        const int r0 = (item - w.pref_c[g]) * R;
-        const int r1 = (r0 + R < K) ? r0 + R : K;
-        const int pmin = (r0 < K - 2) ? r0 : K - 2;
-        const int r = r0 + grp;
-        const bool active = r < K;
-        SecRoot st;
-        if (active) {
-            sec_init(st, r, K, w.pd + po, w.pz + po, rho, w.nzn[g]);
-        } else {
-            st.stage = 2;
+        const int item0 = w.pref_c[g], item1 = w.pref_c[g + 1];
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            s_item = first;
+            s_next = 0;
+            s_pending = -1;
         }
         TileSet<2> ts;
         const double *srcs[2] = {w.pd, w.pz};
         tiles_setup<2>(ts, smem, bars, srcs, po, K);
         ts.phase[0] = ph[0];
         ts.phase[1] = ph[1];
+        SecRoot st;
+        st.stage = 2;
+        bool wlive = false; // this warp has a run (warp-uniform)
+        bool active = false;
+        int r = 0, pmin = 0, r1 = 0;
         bool ok = true;
         for (;;) {
+            // sweep boundary: runs for the warps without one (-1 asks, -2
+            // keeps the current run)
+            if ((threadIdx.x & 31) == 0) {
+                s_run[warp] = wlive ? -2 : -1;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                for (int q = 0; q < kWarpsPerBlock; ++q) {
+                    if (s_run[q] != -1) {
+                        continue;
+                    }
+                    while (s_item >= 0) {
+                        if (s_next < runs) {
+                            const int root0 = (s_item - item0) * R + s_next * Rw;
+                            ++s_next;
+                            if (root0 < K) {
+                                s_run[q] = root0;
+                                break;
+                            }
+                            s_next = runs; // the merge's last, partial item
+                            continue;
+                        }
+                        const int it = atomicAdd(&w.hdr->lvl[a.k].citem, 1);
+                        if (it >= item0 && it < item1) {
+                            s_item = it;
+                            s_next = 0;
+                        } else {
+                            s_pending = it;
+                            s_item = -1;
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+            const int run = s_run[warp];
+            if (!wlive && run >= 0) {
+                r = run + grp;
+                active = r < K;
+                pmin = (run < K - 2) ? run : K - 2;
+                r1 = (run + Rw < K) ? run + Rw : K;
+                if (active) {
+                    sec_init(st, r, K, w.pd + po, w.pz + po, rho, w.nzn[g]);
+                } else {
+                    st.stage = 2;
+                }
+                wlive = true;
+            }
+            if (!__syncthreads_or(wlive)) {
+                break; // the merge is done
+            }
             SecSums sum;
             sec_zero(sum);
-            const bool live = active && st.stage != 2;
+            const bool live = wlive && active && st.stage != 2;
             ok = tiles_sweep<2>(ts, [&](int j0, int cnt, double *const *b) {
                 if (live) {
                     const double *bd = b[0];
@@ -1504,12 +1579,19 @@ __device__ bool sweep_secular(const KArgs &a, int cta_blocks, double *smem, uint
             if (!ok) {
                 break;
             }
-            sums_reduce(sum, tpr);
-            if (live) {
-                sec_after_sweep(st, sum, eps);
-            }
-            if (__syncthreads_and((!active) || st.stage == 2)) {
-                break;
+            if (wlive) {
+                sums_reduce(sum, tpr);
+                if (live) {
+                    sec_after_sweep(st, sum, eps);
+                }
+                if (__all_sync(0xffffffffu, (!active) || st.stage == 2)) {
+                    if (active && lane == 0) {
+                        secular_store(w, a, po, r, st);
+                    }
+                    secular_diag_warp(w, a.k, active && lane == 0, st);
+                    wlive = false;
+                    active = false;
+                }
             }
         }
         ph[0] = ts.phase[0];
@@ -1518,10 +1600,10 @@ __device__ bool sweep_secular(const KArgs &a, int cta_blocks, double *smem, uint
             record_error(w.hdr, kErrBarrierTimeout);
             return false;
         }
-        if (active && lane == 0) {
-            secular_store(w, a, po, r, st);
+        __syncthreads();
+        if (threadIdx.x == 0 && s_pending < 0) {
+            s_pending = atomicAdd(&w.hdr->lvl[a.k].citem, 1);
         }
-        secular_diag_warp(w, a.k, active && lane == 0, st);
         __syncthreads();
     }
     return true;
@@ -1981,6 +2063,7 @@ __global__ void k_init(WsHeader *h, int levels, int B, long long total_n,
         h->lvl[k].nbig = 0;
         h->lvl[k].bar_count = 0u;
         h->lvl[k].bar_gen = 0u;
+        h->lvl[k].citem = 0;
         h->lvl[k].work_w = 0.0;
         h->lvl[k].work_c = 0.0;
         brdc_level_diagnostics z = {};
