@@ -222,8 +222,9 @@ def main():
                     help="solve the tridiagonal of a .de.bin file instead of the headline input")
     ap.add_argument("--data", default=None,
                     help="MODE[:N] -- solve one of the reference's inputs instead: bench, test, "
-                         "normal, uniform, toeplitz, clustered (its GPU bench's generators) or "
-                         "spectrum-{uniform,normal,clustered,toeplitz} (the paper's DLATMS cache)")
+                         "normal, uniform, toeplitz, clustered (its GPU bench's generators), "
+                         "spectrum-{uniform,normal,clustered,toeplitz} (the paper's DLATMS cache) "
+                         "or family-{uniform,normal,toeplitz,clustered} (the plain-solve families)")
     args = ap.parse_args()
     if args.profile_case:
         run_profile_case(args.profile_case)
@@ -431,8 +432,10 @@ def load_workload(input_path, data_spec):
     --data MODE[:N] generates one of the reference's inputs: the GPU bench's
     modes (bench, test, normal, uniform, toeplitz, clustered) or the paper's
     spectrum-prescribed cache (spectrum-uniform, spectrum-normal,
-    spectrum-clustered through LAPACK DLATMS, spectrum-toeplitz); N defaults
-    to 65,536.  Without either, the headline uniform family."""
+    spectrum-clustered through LAPACK DLATMS, spectrum-toeplitz) or the
+    plain-solve families (family-uniform, family-normal, family-toeplitz,
+    family-clustered); N defaults to 65,536.  Without either, the headline
+    uniform family."""
     from brdc import families, inputs
 
     if input_path:
@@ -450,6 +453,12 @@ def load_workload(input_path, data_spec):
             return (d, e, f"spectrum-prescribed {m} (paper cache), N={n}",
                     "LAPACK DLATMS spectrum-prescribed tridiagonal" if eig is not None
                     else "Toeplitz D=2, E=1/4", exact)
+        if mode.startswith("family-"):
+            fam = mode[len("family-"):]
+            d, e = families.generate(fam, n)
+            exact = families.toeplitz_eigenvalues(n) if fam == "toeplitz" else None
+            return (d, e, f"plain values-only BR solve, {fam} family, N={n}",
+                    f"synthetic (seeded {fam} family)", exact)
         d, e = inputs.generate(mode, n)
         exact = families.toeplitz_eigenvalues(n, 2.0, 0.25) if mode == "toeplitz" else None
         return d, e, f"reference GPU-bench data mode {mode}, N={n}", f"reference generator ({mode})", exact
