@@ -48,7 +48,7 @@ def _stale(target: str, deps) -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
-    deps = _sources() + [os.path.join(HERE, "..", "include", "brdc.h"), __file__]
+    deps = _sources() + [os.path.join(HERE, "..", "include", h) for h in ("brdc.h", "brdc_lapack.h")] + [__file__]
     deps = [d for d in deps if not d.endswith(("probe_fp64.cu", "host_check.cpp", "brdc_inputs.cpp"))]
     if force or _stale(LIB, deps):
         cmd = [_nvcc(), *NVCC_FLAGS, "-o", LIB, os.path.join(CSRC, "brdc_capi.cu")]

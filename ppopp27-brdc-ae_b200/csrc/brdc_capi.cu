@@ -18,6 +18,7 @@
 #include <new>
 #include <vector>
 
+#include "../../include/brdc_lapack.h"
 #include "brdc_backward.cuh"
 #include "brdc_level.cuh"
 #include "brdc_subtree.cuh"
@@ -1498,37 +1499,43 @@ int wprod_nthreads_host() {
 }
 } // namespace
 
-extern "C" void brdc_dstedc_dc_br_(const int *n_, double *d, double *e,
-                                   double *work, const int *lwork_,
-                                   int *iwork, const int *liwork_, int *info) {
-    const int n = *n_;
-    const int lwork = *lwork_, liwork = *liwork_;
+namespace {
+
+// Argument checks and workspace query of DSTEDC_DC_BR
+// (cpu/src/dstedc_dc_br.f:44-75): LWMIN = max(1,(16+2*NTHR)*N) and
+// LIWMIN = max(1,7*N) above the LAPACK crossover (ILAENV(9) = 25), else 1;
+// INFO = -1/-5/-7 for a bad N/LWORK/LIWORK; LWORK = -1 or LIWORK = -1 is a
+// query.  Returns true when the caller goes on to solve.
+bool stebr_check(int n, int lwork, int liwork, int *lwmin, int *liwmin, int *info) {
     *info = 0;
+    *lwmin = 1;
+    *liwmin = 1;
     const bool lquery = (lwork == -1 || liwork == -1);
     if (n < 0) {
         *info = -1;
-        return;
+        return false;
     }
     const int smlsiz = 25; // ILAENV(9, 'DSTEDC', ...)
-    int lwmin = 1, liwmin = 1;
     if (n > smlsiz) {
-        lwmin = std::max(1, (16 + 2 * wprod_nthreads_host()) * n);
-        liwmin = std::max(1, 7 * n);
+        *lwmin = std::max(1, (16 + 2 * wprod_nthreads_host()) * n);
+        *liwmin = std::max(1, 7 * n);
     }
-    work[0] = (double)lwmin;
-    iwork[0] = liwmin;
-    if (lwork < lwmin && !lquery) {
+    if (lwork < *lwmin && !lquery) {
         *info = -5;
-    } else if (liwork < liwmin && !lquery) {
+    } else if (liwork < *liwmin && !lquery) {
         *info = -7;
     }
-    if (*info != 0 || lquery || n == 0 || n == 1) {
-        return;
-    }
+    return !(*info != 0 || lquery || n == 0 || n == 1);
+}
+
+// The GPU solve behind the LAPACK-style entries: host D[n] and E[n-1] in,
+// ascending eigenvalues out in D.  Allocates its device buffers (the caller
+// passes host arrays) and synchronises.  Returns 0, the INFO > 0 of a root
+// that did not converge, or n + 1 when the device could not be used.
+int host_stebr(int n, double *d, const double *e) {
     brdc_handle h = nullptr;
     if (brdc_create(&h) != BRDC_STATUS_SUCCESS) {
-        *info = n + 1;
-        return;
+        return n + 1;
     }
     size_t ws_bytes = 0;
     brdc_dstebr_workspace_size(n, 0, &ws_bytes);
@@ -1563,13 +1570,130 @@ extern "C" void brdc_dstedc_dc_br_(const int *n_, double *d, double *e,
     cudaFree(dW);
     cudaFree(ws);
     brdc_destroy(h);
-    if (fail) {
-        *info = n + 1;
-    } else if (dinfo > 0) {
-        *info = dinfo;
+    return fail ? n + 1 : (dinfo > 0 ? dinfo : 0);
+}
+
+} // namespace
+
+extern "C" void brdc_dstedc_dc_br_(const int *n_, double *d, double *e,
+                                   double *work, const int *lwork_,
+                                   int *iwork, const int *liwork_, int *info) {
+    const int n = *n_;
+    int lwmin = 1, liwmin = 1;
+    const bool go = stebr_check(n, *lwork_, *liwork_, &lwmin, &liwmin, info);
+    if (*info == -1) {
+        return;
     }
     work[0] = (double)lwmin;
     iwork[0] = liwmin;
+    if (!go) {
+        return;
+    }
+    const int r = host_stebr(n, d, e);
+    if (r != 0) {
+        *info = r;
+    }
+    work[0] = (double)lwmin;
+    iwork[0] = liwmin;
+}
+
+// The BR routine under its upstream LAPACK name (README.md:13): the
+// argument list and semantics of DSTEDC_DC_BR.
+extern "C" void dstebr_(const int *n, double *d, double *e, double *work, const int *lwork,
+                        int *iwork, const int *liwork, int *info) {
+    brdc_dstedc_dc_br_(n, d, e, work, lwork, iwork, liwork, info);
+}
+
+// Single precision: the same checks and query (LWMIN counted in reals); the
+// solve runs in FP64 on the GPU and the eigenvalues are rounded to float.
+extern "C" void sstebr_(const int *n_, float *d, float *e, float *work, const int *lwork_,
+                        int *iwork, const int *liwork_, int *info) {
+    const int n = *n_;
+    int lwmin = 1, liwmin = 1;
+    const bool go = stebr_check(n, *lwork_, *liwork_, &lwmin, &liwmin, info);
+    if (*info == -1) {
+        return;
+    }
+    work[0] = (float)lwmin;
+    iwork[0] = liwmin;
+    if (!go) {
+        return;
+    }
+    std::vector<double> dd(d, d + n), ee(e, e + (n - 1));
+    const int r = host_stebr(n, dd.data(), ee.data());
+    if (r != 0) {
+        *info = r;
+    }
+    if (r <= n) { // solved (possibly with a root that hit the cap)
+        for (int i = 0; i < n; ++i) {
+            d[i] = (float)dd[i];
+        }
+    }
+    work[0] = (float)lwmin;
+    iwork[0] = liwmin;
+}
+
+// LAPACKE-style C wrappers (the upstream routine ships them too): the
+// _work form passes the caller's workspace through, the plain form checks
+// D and E for NaN (-2, -3), queries and allocates the workspace itself
+// (LAPACK_WORK_MEMORY_ERROR = -1010 when that fails).
+extern "C" int LAPACKE_dstebr_work(int n, double *d, double *e, double *work, int lwork,
+                                   int *iwork, int liwork) {
+    int info = 0;
+    dstebr_(&n, d, e, work, &lwork, iwork, &liwork, &info);
+    return info;
+}
+
+extern "C" int LAPACKE_sstebr_work(int n, float *d, float *e, float *work, int lwork,
+                                   int *iwork, int liwork) {
+    int info = 0;
+    sstebr_(&n, d, e, work, &lwork, iwork, &liwork, &info);
+    return info;
+}
+
+namespace {
+
+template <typename R, typename Work>
+int lapacke_stebr(int n, R *d, R *e, Work call) {
+    if (n < 0) {
+        return -1;
+    }
+    for (int i = 0; i < n; ++i) {
+        if (d[i] != d[i]) {
+            return -2;
+        }
+    }
+    for (int i = 0; i + 1 < n; ++i) {
+        if (e[i] != e[i]) {
+            return -3;
+        }
+    }
+    R wq = 0;
+    int iwq = 0;
+    int info = call(n, d, e, &wq, -1, &iwq, -1);
+    if (info != 0) {
+        return info;
+    }
+    const int lwork = std::max(1, (int)wq), liwork = std::max(1, iwq);
+    std::vector<R> work;
+    std::vector<int> iwork;
+    try {
+        work.resize((size_t)lwork);
+        iwork.resize((size_t)liwork);
+    } catch (...) {
+        return -1010;
+    }
+    return call(n, d, e, work.data(), lwork, iwork.data(), liwork);
+}
+
+} // namespace
+
+extern "C" int LAPACKE_dstebr(int n, double *d, double *e) {
+    return lapacke_stebr<double>(n, d, e, LAPACKE_dstebr_work);
+}
+
+extern "C" int LAPACKE_sstebr(int n, float *d, float *e) {
+    return lapacke_stebr<float>(n, d, e, LAPACKE_sstebr_work);
 }
 
 // ---------------------------------------------- allocation-free entry point
