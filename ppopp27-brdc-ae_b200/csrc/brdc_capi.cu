@@ -291,6 +291,30 @@ void launch_md(const KArgs &a, int grid, cudaStream_t s) {
     k_merge_deflate<T><<<grid, T, 0, s>>>(a);
 }
 
+// Programmatic dependent launch (the kernels begin with pdl_begin): the
+// launch and block scheduling of a solve kernel overlap the end of the one
+// before it in the stream.  Used for k_norm, k_level and k_plan, whose CTAs
+// take whole SMs or are few (1-2.6% off the solve at n = 4096-65,536).
+cudaLaunchAttribute pdl_attr() {
+    cudaLaunchAttribute at;
+    at.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at.val.programmaticStreamSerializationAllowed = 1;
+    return at;
+}
+
+cudaLaunchConfig_t plain_config(unsigned grid, unsigned block, size_t smem, cudaStream_t s,
+                                cudaLaunchAttribute *at) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    at[0] = pdl_attr();
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cfg;
+}
+
 cudaLaunchConfig_t cluster_config(unsigned grid, int C, cudaStream_t s, cudaLaunchAttribute *at) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
@@ -499,6 +523,8 @@ int launch_sweeps(brdc_handle h, const HostForest &hf, const KArgs &a, cudaStrea
         return -1;
     }
     const int grid = nb * h->sm_count;
+    // an ordinary (not programmatic) cooperative launch: it measured no
+    // faster with the programmatic attribute
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeCooperative;
     at[0].val.cooperative = 1;
@@ -541,14 +567,18 @@ int launch_level_fused(brdc_handle h, const HostForest &hf, const KArgs &a0, boo
     // a plan is needed only where a merge can keep more than kLvlMaxK poles
     const bool big = mmax > kLvlMaxK;
     a.plan_inline = big && a.nodes <= kLvlThreads ? 1 : 0;
-    cudaLaunchAttribute at[1];
+    cudaLaunchAttribute at[2];
     cudaLaunchConfig_t cfg = cluster_config((unsigned)(a.nodes * C), C, s, at);
     cfg.blockDim = dim3(kLvlThreads);
     cfg.dynamicSmemBytes = sizeof(LvlSmem);
+    at[1] = pdl_attr();
+    cfg.numAttrs = 2;
     cudaLaunchKernelEx(&cfg, k_level<kLvlThreads>, a);
     int n = 1;
     if (big && !a.plan_inline) {
-        k_plan<1024><<<1, 1024, 0, s>>>(a);
+        cudaLaunchAttribute pa[1];
+        cudaLaunchConfig_t pc = plain_config(1, 1024, 0, s, pa);
+        cudaLaunchKernelEx(&pc, k_plan<1024>, a);
         ++n;
     }
     mark(h, 3 + 4 * k);
@@ -583,7 +613,9 @@ brdc_status run_forest(brdc_handle h, const HostForest &hf, const Layout &L,
     {
         long long ng = hf.B > 1 ? (hf.B + 7) / 8 : (hf.total_n + 255) / 256;
         ng = std::max<long long>(1, std::min<long long>(ng, (long long)h->sm_count * 4));
-        k_norm<<<(unsigned)ng, 256, 0, s>>>(F, D, E, w.f_norm);
+        cudaLaunchAttribute at[1];
+        cudaLaunchConfig_t cfg = plain_config((unsigned)ng, 256, 0, s, at);
+        cudaLaunchKernelEx(&cfg, k_norm, F, D, E, w.f_norm);
         BRDC_CUDA(h, "brdc.norm", cudaGetLastError());
     }
     h->launches += 2;
@@ -627,6 +659,9 @@ brdc_status run_forest(brdc_handle h, const HostForest &hf, const Layout &L,
         for (int b = 0; b < hf.B; ++b) {
             subs += subtrees_of(hf.lev[b], sub);
         }
+        // an ordinary launch: scheduled while k_norm still ran (programmatic
+        // launch), the subtree CTAs landed on the SMs free at that moment
+        // and the subtree phase took 4-6% longer at n = 16,384-32,768
         if (sub_rows_for(sub) == 256) {
             k_subtree<256><<<(unsigned)subs, 256, sizeof(SubSmem<256>), s>>>(A);
         } else {

@@ -57,6 +57,19 @@ inline int tree_levels(long long n) {
 }
 
 // Per-level control block written by the kernels.
+// Programmatic dependent launch.  Some of the solve's kernels are launched
+// with the programmatic-serialization attribute, so their launch and block
+// scheduling overlap the end of the kernel before them.  Every forward
+// kernel starts with pdl_begin(): it lets the next kernel in the stream be
+// scheduled as soon as all of this grid's CTAs are running (their resources
+// are then already held, so the early CTAs only take what is left), and
+// waits until the previous kernel has finished and its writes are visible.
+// For a kernel launched without the attribute the wait returns at once.
+__device__ __forceinline__ void pdl_begin() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 struct LevelCtl {
     int ticket;      // CTAs of the merge kernel that finished
     int nodes;       // merges at this level

@@ -417,6 +417,7 @@ __device__ inline int leaf_solve_full(const KArgs &a, const LeafGeom &G, int s, 
 // (leafl) and eigenvector (leafv, 16 entries per column) in sorted order.
 __global__ void __launch_bounds__(kLeafWarps * 32)
     k_leaf_full(KArgs a, long long total_leaves) {
+    pdl_begin();
     const int lane = threadIdx.x & 31;
     const int x = lane & 15;
     const int half = lane >> 4;
@@ -460,6 +461,7 @@ __global__ void __launch_bounds__(kLeafWarps * 32)
 
 __global__ void __launch_bounds__(kLeafWarps * 32)
     k_leaf(KArgs a, long long total_leaves) {
+    pdl_begin();
     const int lane = threadIdx.x & 31;
     const int x = lane & 15;
     const int half = lane >> 4;
@@ -514,6 +516,7 @@ __global__ void __launch_bounds__(kLeafWarps * 32)
 // child)/sqrt2, and the block-diagonal projections of the parent's first
 // and last rows.
 __global__ void __launch_bounds__(256) k_merge(KArgs a, long long total_n) {
+    pdl_begin();
     const Ws &w = a.w;
     const double isq2 = 0.70710678118654752440;
     for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x; x < total_n;
@@ -680,6 +683,7 @@ __device__ void level_plan(const KArgs &a, double *red, int *iscan) {
 
 template <int T>
 __global__ void __launch_bounds__(T) k_plan(KArgs a) {
+    pdl_begin();
     __shared__ double red[32];
     __shared__ int iscan[32];
     level_plan<T>(a, red, iscan);
@@ -702,6 +706,7 @@ struct PlanAllArgs {
 
 template <int T>
 __global__ void __launch_bounds__(T) k_plan_all(PlanAllArgs P) {
+    pdl_begin();
     __shared__ double red[32];
     __shared__ int iscan[32];
     const PlanLevel &L = P.lv[blockIdx.x];
@@ -1006,6 +1011,7 @@ __device__ void defl_finish(const KArgs &a, int g, int K, int Kz, double rho, do
 // One CTA per merge node.
 template <int T>
 __global__ void __launch_bounds__(T) k_merge_deflate(KArgs a) {
+    pdl_begin();
     __shared__ double red[32];
     __shared__ int iscan[32];
     __shared__ int s_last;
@@ -1044,6 +1050,7 @@ __global__ void __launch_bounds__(T) k_merge_deflate(KArgs a) {
 // memory after a cluster barrier.
 template <int T>
 __global__ void __launch_bounds__(T) k_merge_deflate_cl(KArgs a) {
+    pdl_begin();
     namespace cg = cooperative_groups;
     __shared__ double red[32];
     __shared__ int iscan[32];
@@ -1949,6 +1956,7 @@ __device__ inline bool grid_barrier(WsHeader *h, LevelCtl *c) {
 // Loewner and rows phases (every merge an instance root).
 __global__ void __launch_bounds__(kSweepThreads)
     k_sweeps(KArgs a, int tiles, int rows, long long total_n) {
+    pdl_begin();
     extern __shared__ __align__(16) double smem[];
     __shared__ __align__(8) uint64_t bars[2];
     WsHeader *h = a.w.hdr;
@@ -2000,6 +2008,7 @@ __global__ void __launch_bounds__(kSweepThreads)
 // atomic per block for a single matrix, one warp per instance for a batch.
 __global__ void __launch_bounds__(256) k_norm(Forest F, const double *D, const double *E,
                                               long long *out) {
+    pdl_begin();
     const int lane = threadIdx.x & 31;
     if (F.B == 1) {
         const long long n = F.n0;

@@ -311,6 +311,7 @@ __device__ void level_ticket(const KArgs &a, LvlSmem &S) {
 // k_merge_deflate_cl does.
 template <int T>
 __global__ void __launch_bounds__(T, 1) k_level(KArgs a) {
+    pdl_begin();
     namespace cg = cooperative_groups;
     extern __shared__ __align__(16) unsigned char lvl_raw[];
     LvlSmem &S = *reinterpret_cast<LvlSmem *>(lvl_raw);

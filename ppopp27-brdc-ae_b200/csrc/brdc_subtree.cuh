@@ -128,6 +128,7 @@ __device__ inline int sub_node_of(const SubSmem<kSubRows> &S, int nk, int x) {
 
 template <int kSubRows>
 __global__ void __launch_bounds__(kSubRows, 512 / kSubRows) k_subtree(SubArgs A) {
+    pdl_begin();
     constexpr int kSubWarps = kSubRows / 32;
     extern __shared__ __align__(16) unsigned char sub_raw[];
     SubSmem<kSubRows> &S = *reinterpret_cast<SubSmem<kSubRows> *>(sub_raw);
