@@ -288,6 +288,22 @@ brdc_status brdc_dstebr_batched_backward(brdc_handle handle, int64_t count,
                                          size_t workspace_size, int keep_forward);
 
 /* Library version string. */
+/* Eigenvalues and eigenvectors: the vector path of the reference's solver
+ * (compute_eigenvectors = 1, gpu/src/tridiag_solver.cu:848-1071).  A
+ * checkpointing values solve records every merge; each node's eigenvector
+ * matrix is then blockdiag(Q_left, Q_right) * M_node, with M_node built from
+ * the recorded permutations, deflation rotations and secular vectors
+ * (Loewner weights), the products by library FP64 GEMMs.  W[n] ascending,
+ * Z column-major n x n (ld ldz >= n), column j the unit eigenvector of
+ * W[j].  The workspace (query below) holds the checkpoints, M and two
+ * levels of eigenvector blocks, about 16 n^2 bytes; n <= 32768.
+ * Synchronises the handle's stream (the per-level GEMM tables come from
+ * the host); not graph-capturable. */
+brdc_status brdc_dstebr_vectors_workspace_size(int64_t n, size_t *bytes);
+brdc_status brdc_dstebr_vectors(brdc_handle handle, int64_t n, const double *d_D,
+                                const double *d_E, double *d_W, double *d_Z,
+                                int64_t ldz, void *workspace, size_t workspace_size);
+
 const char *brdc_version(void);
 
 #ifdef __cplusplus

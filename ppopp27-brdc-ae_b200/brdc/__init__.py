@@ -68,6 +68,8 @@ EXPORTS = (
     "brdc_set_tuning",
     "brdc_get_tuning",
     "brdc_autotune",
+    "brdc_dstebr_vectors_workspace_size",
+    "brdc_dstebr_vectors",
 )
 
 
@@ -189,6 +191,8 @@ def load() -> ctypes.CDLL:
     lib.brdc_version.restype = ctypes.c_char_p
     lib.brdc_set_timing.argtypes = [vp, ctypes.c_int]
     lib.brdc_dstebr_noalloc.argtypes = [vp, i64, vp, vp, vp]
+    lib.brdc_dstebr_vectors_workspace_size.argtypes = [i64, ctypes.POINTER(sz)]
+    lib.brdc_dstebr_vectors.argtypes = [vp, i64, vp, vp, vp, vp, i64, vp, sz]
     lib.brdc_get_last_timings.argtypes = [vp, ctypes.POINTER(Timings)]
     lib.brdc_set_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
     lib.brdc_get_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
@@ -343,6 +347,30 @@ class Solver:
         )
         _check(st, "brdc_dstebr", self.h)
         return W
+
+    def dstebr_vectors(self, D, E, workspace=None):
+        """Eigenvalues W[n] (ascending) and eigenvectors Z (n x n, column j
+        for W[j]) on the device (brdc_dstebr_vectors)."""
+        torch = self._torch
+        n = D.shape[0]
+        if D.dtype != torch.float64 or not D.is_cuda:
+            raise TypeError("D must be a float64 CUDA tensor")
+        D = D.contiguous()
+        E = E.contiguous() if E is not None and E.numel() > 0 else D
+        W = torch.empty(n, dtype=torch.float64, device=D.device)
+        Zt = torch.empty((n, n), dtype=torch.float64, device=D.device)  # row-major Z^T
+        if workspace is None:
+            nb = ctypes.c_size_t(0)
+            _check(load().brdc_dstebr_vectors_workspace_size(n, ctypes.byref(nb)),
+                   "brdc_dstebr_vectors_workspace_size")
+            workspace = torch.empty(nb.value, dtype=torch.uint8, device=D.device)
+        st = load().brdc_dstebr_vectors(
+            self.h, n, ctypes.c_void_p(D.data_ptr()), ctypes.c_void_p(E.data_ptr()),
+            ctypes.c_void_p(W.data_ptr()), ctypes.c_void_p(Zt.data_ptr()), n,
+            ctypes.c_void_p(workspace.data_ptr()), workspace.numel(),
+        )
+        _check(st, "brdc_dstebr_vectors", self.h)
+        return W, Zt.t()
 
     def checkpoint_workspace(self, n: int):
         """Workspace that also records the per-level state the adjoint reads."""

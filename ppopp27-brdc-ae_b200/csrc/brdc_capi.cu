@@ -8,6 +8,7 @@
 // so a solve can be captured in a CUDA graph.  Data-dependent sizes (deflation counts K) travel from kernel to
 // kernel through the workspace header; that replaces the per-level device
 // to host copy of the reference (gpu/src/tridiag_solver.cu:624-630).
+#include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -21,6 +22,7 @@
 #include "../../include/brdc_lapack.h"
 #include "brdc_backward.cuh"
 #include "brdc_level.cuh"
+#include "brdc_vectors.cuh"
 #include "brdc_subtree.cuh"
 
 using namespace brdc;
@@ -53,6 +55,7 @@ struct brdc_handle_struct {
     int timed_levels;
     int has_lowner[BRDC_MAX_LEVELS];
     int fused_levels;
+    cublasHandle_t blas = nullptr; // the eigenvector path's GEMMs, made on first use
 };
 
 namespace {
@@ -76,6 +79,8 @@ void set_error(brdc_handle h, int code, brdc_error_source src,
     } while (0)
 
 constexpr size_t kAlign = 256; // gpu/src/workspace_align.hpp:9
+// largest order of the eigenvector path (n^2 doubles of eigenvectors, 2 n^2 of work)
+constexpr long long kMaxVectorOrder = 32768;
 
 size_t align_up(size_t v) { return (v + kAlign - 1) / kAlign * kAlign; }
 
@@ -800,6 +805,9 @@ extern "C" brdc_status brdc_destroy(brdc_handle h) {
         for (auto &e : h->ev) {
             cudaEventDestroy(e);
         }
+    }
+    if (h->blas != nullptr) {
+        cublasDestroy(h->blas);
     }
     if (h->own_stream != nullptr) {
         cudaStreamDestroy(h->own_stream);
@@ -1729,6 +1737,216 @@ extern "C" int LAPACKE_dstebr(int n, double *d, double *e) {
 
 extern "C" int LAPACKE_sstebr(int n, float *d, float *e) {
     return lapacke_stebr<float>(n, d, e, LAPACKE_sstebr_work);
+}
+
+// ------------------------------------------------------------ eigenvectors
+namespace {
+
+// Workspace of the vector path: the checkpointing layout of the values
+// solve, then two buffers for the eigenvector blocks of consecutive levels
+// (node g's block at gstart * mmax of its level, n x ceil(n/2) doubles at
+// most below the top), M of one level (n x n at the top), the GEMM pointer
+// tables and the row signs.
+struct VecLayout {
+    size_t ckpt, qa, qb, mm, ptrs, sgn, total;
+};
+
+VecLayout vec_layout(const HostForest &hf, long long n) {
+    VecLayout v{};
+    v.ckpt = align_up(make_layout(hf, true).bytes);
+    const size_t half = (size_t)n * (size_t)((n + 1) / 2) * sizeof(double);
+    v.qa = align_up(half);
+    v.qb = align_up(half);
+    v.mm = align_up((size_t)n * (size_t)n * sizeof(double));
+    v.ptrs = align_up(sizeof(double *) * 6 * (size_t)(hf.nn0 + 1));
+    v.sgn = align_up(sizeof(double) * (size_t)n);
+    v.total = v.ckpt + v.qa + v.qb + v.mm + v.ptrs + v.sgn;
+    return v;
+}
+
+__global__ void k_vec_rowscale(double *Z, long long ldz, long long n, const double *sgn) {
+    const long long total = n * n;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long col = t / n, row = t % n;
+        Z[col * ldz + row] *= sgn[row];
+    }
+}
+
+} // namespace
+
+extern "C" brdc_status brdc_dstebr_vectors_workspace_size(int64_t n, size_t *bytes) {
+    if (bytes == nullptr) {
+        return BRDC_STATUS_INVALID_POINTER;
+    }
+    if (n <= 0 || n > kMaxVectorOrder) {
+        return BRDC_STATUS_INVALID_VALUE;
+    }
+    const long long off[2] = {0, (long long)n};
+    HostForest hf;
+    if (!build_forest(1, off, &hf)) {
+        return BRDC_STATUS_INVALID_VALUE;
+    }
+    *bytes = vec_layout(hf, n).total;
+    return BRDC_STATUS_SUCCESS;
+}
+
+extern "C" brdc_status brdc_dstebr_vectors(brdc_handle h, int64_t n, const double *d_D,
+                                           const double *d_E, double *d_W, double *d_Z,
+                                           int64_t ldz, void *workspace, size_t workspace_size) {
+    if (h == nullptr) {
+        return BRDC_STATUS_INVALID_HANDLE;
+    }
+    if (d_D == nullptr || d_W == nullptr || d_Z == nullptr || (n > 1 && d_E == nullptr)) {
+        return BRDC_STATUS_INVALID_POINTER;
+    }
+    if (n <= 0 || n > kMaxVectorOrder || ldz < n) {
+        return BRDC_STATUS_INVALID_VALUE;
+    }
+    const long long off[2] = {0, (long long)n};
+    HostForest hf;
+    if (!build_forest(1, off, &hf)) {
+        return BRDC_STATUS_INVALID_VALUE;
+    }
+    const VecLayout V = vec_layout(hf, n);
+    if (workspace == nullptr || workspace_size < V.total) {
+        return BRDC_STATUS_INVALID_WORKSPACE;
+    }
+    cudaStream_t s = h->stream;
+    if (h->blas == nullptr) {
+        if (cublasCreate(&h->blas) != CUBLAS_STATUS_SUCCESS) {
+            h->blas = nullptr;
+            set_error(h, (int)cudaErrorUnknown, BRDC_ERROR_SRC_CUDA, "brdc.vectors.cublas_create");
+            return BRDC_STATUS_INTERNAL_ERROR;
+        }
+    }
+    cublasSetStream(h->blas, s);
+    const Layout L = make_layout(hf, true);
+    const Ws w = carve(workspace, hf, true);
+    Forest F{};
+    F.B = 1;
+    F.max_levels = hf.max_levels;
+    F.n0 = n;
+    F.L0 = hf.max_levels;
+    // values solve with every merge recorded (and the leaves' eigenvectors)
+    const brdc_status st = run_forest(h, hf, L, F, w, d_D, d_E, d_W);
+    if (st != BRDC_STATUS_SUCCESS) {
+        return st;
+    }
+    char *base = static_cast<char *>(workspace) + V.ckpt;
+    double *qa = reinterpret_cast<double *>(base);
+    double *qb = reinterpret_cast<double *>(base + V.qa);
+    double *M = reinterpret_cast<double *>(base + V.qa + V.qb);
+    double **ptrs = reinterpret_cast<double **>(base + V.qa + V.qb + V.mm);
+    double *sgn = reinterpret_cast<double *>(base + V.qa + V.qb + V.mm + V.ptrs);
+    k_vec_signs<<<1, 32, 0, s>>>(d_E, n, sgn);
+    BRDC_CUDA(h, "brdc.vectors.signs", cudaGetLastError());
+    const int Lv = hf.max_levels;
+    long long eg = (n + 255) / 256;
+    eg = std::max<long long>(1, std::min<long long>(eg, (long long)h->sm_count * 8));
+    long long zg = (n * n + 255) / 256;
+    zg = std::max<long long>(1, std::min<long long>(zg, (long long)h->sm_count * 16));
+    if (Lv == 0) {
+        // one leaf: its eigenvector matrix (ld 16) is the answer
+        k_vec_out<<<(unsigned)zg, 256, 0, s>>>(w.leafv, 16, n, sgn, d_Z, ldz);
+        BRDC_CUDA(h, "brdc.vectors.leaf", cudaGetLastError());
+        return BRDC_STATUS_SUCCESS;
+    }
+    const double one = 1.0, zero = 0.0;
+    double *qprev = nullptr, *qcur = qa;
+    long long prev_mmax = 16;
+    struct Group {
+        int rows, m, lda, ldc;
+        std::vector<const double *> A, B;
+        std::vector<double *> C;
+    };
+    for (int k = 0; k < Lv; ++k) {
+        Ws wl = w;
+        level_view(hf, L, w, k, &wl);
+        const bool top = (k == Lv - 1);
+        const long long mmax = hf.level_mmax[k];
+        VArgs va{};
+        va.F = F;
+        va.w = wl;
+        va.M = M;
+        va.mstride = mmax;
+        va.k = k;
+        va.nodes = hf.level_nodes[k];
+        if (top) {
+            k_vec_lowner<<<(unsigned)std::max<long long>(1, std::min<long long>((n + 7) / 8, h->sm_count * 8)),
+                           256, 0, s>>>(va);
+            BRDC_CUDA(h, "brdc.vectors.lowner", cudaGetLastError());
+        }
+        BRDC_CUDA(h, "brdc.vectors.zero",
+                  cudaMemsetAsync(M, 0, sizeof(double) * (size_t)n * (size_t)mmax, s));
+        k_vec_build<<<(unsigned)eg, 256, 0, s>>>(va, n);
+        BRDC_CUDA(h, "brdc.vectors.build", cudaGetLastError());
+        // Q_node = blockdiag(Q_left, Q_right) * M_node: two GEMMs per node,
+        // batched over nodes of equal shape
+        const double *child = (k == 0) ? wl.leafv : qprev;
+        double *out = top ? d_Z : qcur;
+        std::vector<Group> groups;
+        const int depth = Lv - 1 - k;
+        for (int g = 0; g < hf.level_nodes[k]; ++g) {
+            long long st0 = 0, m = 0;
+            walk_node(n, depth, g, &st0, &m);
+            const int m1 = (int)(m >> 1), m2 = (int)(m - m1);
+            for (int half = 0; half < 2; ++half) {
+                const int rows = half ? m2 : m1;
+                const long long cst = st0 + (half ? m1 : 0);
+                const int lda = (k == 0) ? 16 : rows;
+                const int ldc = top ? (int)ldz : (int)m;
+                const double *A = (k == 0) ? child + cst * 16 : child + cst * prev_mmax;
+                const double *B = M + st0 * mmax + (half ? m1 : 0);
+                double *C = top ? out + (half ? m1 : 0) : out + st0 * mmax + (half ? m1 : 0);
+                Group *gp = nullptr;
+                for (auto &q : groups) {
+                    if (q.rows == rows && q.m == (int)m && q.lda == lda && q.ldc == ldc) {
+                        gp = &q;
+                        break;
+                    }
+                }
+                if (gp == nullptr) {
+                    groups.push_back(Group{rows, (int)m, lda, ldc, {}, {}, {}});
+                    gp = &groups.back();
+                }
+                gp->A.push_back(A);
+                gp->B.push_back(B);
+                gp->C.push_back(C);
+            }
+        }
+        size_t used = 0;
+        for (auto &q : groups) {
+            const size_t cnt = q.A.size();
+            std::vector<const void *> tab;
+            tab.reserve(3 * cnt);
+            for (size_t i = 0; i < cnt; ++i) tab.push_back(q.A[i]);
+            for (size_t i = 0; i < cnt; ++i) tab.push_back(q.B[i]);
+            for (size_t i = 0; i < cnt; ++i) tab.push_back(q.C[i]);
+            double **dev = ptrs + used;
+            BRDC_CUDA(h, "brdc.vectors.ptrs",
+                      cudaMemcpyAsync(dev, tab.data(), sizeof(void *) * tab.size(),
+                                      cudaMemcpyHostToDevice, s));
+            used += tab.size();
+            const cublasStatus_t bs = cublasDgemmBatched(
+                h->blas, CUBLAS_OP_N, CUBLAS_OP_N, q.rows, q.m, q.rows, &one,
+                reinterpret_cast<const double *const *>(dev), q.lda,
+                reinterpret_cast<const double *const *>(dev + cnt), q.m, &zero, dev + 2 * cnt, q.ldc,
+                (int)cnt);
+            if (bs != CUBLAS_STATUS_SUCCESS) {
+                set_error(h, (int)bs, BRDC_ERROR_SRC_CUDA, "brdc.vectors.gemm");
+                return BRDC_STATUS_INTERNAL_ERROR;
+            }
+        }
+        // the pointer tables of this level stay in use until its GEMMs ran
+        BRDC_CUDA(h, "brdc.vectors.level", cudaStreamSynchronize(s));
+        qprev = qcur;
+        qcur = (qcur == qa) ? qb : qa;
+        prev_mmax = mmax;
+    }
+    k_vec_rowscale<<<(unsigned)zg, 256, 0, s>>>(d_Z, ldz, n, sgn);
+    BRDC_CUDA(h, "brdc.vectors.rowscale", cudaGetLastError());
+    return BRDC_STATUS_SUCCESS;
 }
 
 // ---------------------------------------------- allocation-free entry point

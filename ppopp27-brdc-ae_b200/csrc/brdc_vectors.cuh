@@ -1,0 +1,182 @@
+// brdc_vectors.cuh -- eigenvectors from a checkpointed BR solve.
+//
+// The reference's vector path (gpu/src/tridiag_solver.cu:848-1071) carries
+// each node's eigenvector matrix up the tree; the values-only solve carries
+// only its first and last rows.  Here a checkpointing values solve records
+// every merge (merge permutation, deflation lists and Givens chains, poles,
+// roots), and the eigenvectors are then assembled bottom-up:
+//
+//   Q_node = blockdiag(Q_left, Q_right) * M_node
+//
+// where column t of M_node (m x m, rows in the children's eigenvector
+// coordinates) is the node's t-th eigenvector (ascending) in the children's
+// eigenbasis:
+//   root j:          sum_i u_ij P_i,  u_ij = w_i / delta_ij, normalised,
+//                    w the Loewner weights (cpu/src/dlaed9_br.f:181-266),
+//                    P_i the active column of pole i after the chains;
+//   small-z slot q:  the unit column of its merged position;
+//   rotated-out q:   its active column after the chains.
+// An active column after the chains is the chain product applied to unit
+// columns, which is the chains undone on the rows: the row operations of
+// the adjoint's chain reversal.  Rows map to child coordinates through
+// amap/zmap (list -> merged position) and morig (merged position -> child
+// eigenvalue index).  The two products per node are library FP64 GEMMs.
+#pragma once
+
+#include "brdc_kernels.cuh"
+
+namespace brdc {
+
+struct VArgs {
+    Forest F;
+    Ws w;         // the level's checkpoint slices
+    double *M;    // node g's M at M + gstart * mstride, column-major, ld m
+    long long mstride;
+    int k;
+    int nodes;
+};
+
+// Loewner weights of the instance-root merges, which the values solve
+// skips (no parent reads their rows): one warp per pole.
+__global__ void __launch_bounds__(256) k_vec_lowner(VArgs a) {
+    const Ws &w = a.w;
+    const int lane = threadIdx.x & 31;
+    const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+    for (int g = 0; g < a.nodes; ++g) {
+        const NodeGeom G = node_geom(a.F, a.k, g);
+        if (G.depth != 0) {
+            continue;
+        }
+        const int K = w.nK[g];
+        const long long po = G.poff;
+        for (long long i = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < K;
+             i += warps) {
+            const double di = w.pd[po + i];
+            double prod = 1.0;
+            for (int j = lane; j < K; j += 32) {
+                const double dl = (di - w.rdo[po + j]) - w.rtau[po + j];
+                prod *= dl * brdc_rcp(j == i ? 1.0 : di - w.pd[po + j]);
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                prod *= __shfl_xor_sync(0xffffffffu, prod, o);
+            }
+            if (lane == 0) {
+                w.pw[po + i] = K == 1 ? w.pz[po + i] * sqrt(w.nrho[g])
+                                      : lowner_value(w, po, (int)i, prod, w.nrho[g]);
+            }
+        }
+    }
+}
+
+// Row of M (child eigenvector coordinate) of active index a / small-z slot q.
+__device__ inline int vec_row_active(const Ws &w, long long gs, int a) {
+    return w.morig[gs + w.amap[gs + a]];
+}
+__device__ inline int vec_row_small(const Ws &w, long long gs, int q) {
+    return w.morig[gs + w.zmap[gs + q]];
+}
+
+// One thread per slot of the level (root, small-z, rotated-out): its
+// position in the node's ascending order (the placement rule: ties go
+// roots, small-z, rotated-out), then its column of M.  M must be zero.
+__global__ void __launch_bounds__(256) k_vec_build(VArgs a, long long total_n) {
+    const Ws &w = a.w;
+    for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x; x < total_n;
+         x += (long long)gridDim.x * blockDim.x) {
+        int g, m, depth;
+        long long gs;
+        if (!elem_node(a.F, a.k, x, &g, &gs, &m, &depth)) {
+            continue;
+        }
+        const long long po = (gs + g + 1) & ~1LL;
+        const int s = (int)(x - gs);
+        const int K = w.nK[g];
+        const int Kz = w.nKz[g];
+        const int ndz = m - Kz, ndg = Kz - K;
+        const double *zdl = w.zd + gs;
+        const double *gdl = w.gd + gs;
+        const double *rl = w.rlam + po;
+        int pos;
+        if (s < K) {
+            pos = s + lower_bound_d(zdl, ndz, rl[s]) + lower_bound_d(gdl, ndg, rl[s]);
+        } else if (s < K + ndz) {
+            const int q = s - K;
+            pos = q + upper_bound_d(rl, K, zdl[q]) + lower_bound_d(gdl, ndg, zdl[q]);
+        } else {
+            const int q = s - K - ndz;
+            pos = q + upper_bound_d(rl, K, gdl[q]) + upper_bound_d(zdl, ndz, gdl[q]);
+        }
+        double *col = a.M + gs * a.mstride + (long long)pos * m;
+        if (s >= K && s < K + ndz) {
+            col[vec_row_small(w, gs, s - K)] = 1.0; // no chain touches it
+            continue;
+        }
+        if (s < K) {
+            // u_i = w_i / delta_i(s) over the poles, normalised
+            const int org = w.rorg[po + s];
+            const double dorg = w.rdo[po + s], tau = w.rtau[po + s];
+            double s2 = 0.0;
+            for (int i = 0; i < K; ++i) {
+                const double dl = (i == org) ? -tau : (w.pd[po + i] - dorg) - tau;
+                const double u = w.pw[po + i] / dl;
+                s2 += u * u;
+            }
+            const double inv = 1.0 / sqrt(s2);
+            for (int i = 0; i < K; ++i) {
+                const double dl = (i == org) ? -tau : (w.pd[po + i] - dorg) - tau;
+                col[vec_row_active(w, gs, w.pmap[po + i])] = w.pw[po + i] / dl * inv;
+            }
+        } else {
+            col[vec_row_active(w, gs, w.gpos[gs + (s - K - ndz)])] = 1.0;
+        }
+        // undo every Givens chain on the rows (bases have gmark 0, their
+        // members follow with gmark 1, rotated in increasing order)
+        for (int b0 = 0; b0 + 1 < Kz; ++b0) {
+            if (w.gmark[gs + b0] != 0 || w.gmark[gs + b0 + 1] == 0) {
+                continue;
+            }
+            int c = 1;
+            while (b0 + c + 1 < Kz && w.gmark[gs + b0 + c + 1] != 0) {
+                ++c;
+            }
+            const int rb = vec_row_active(w, gs, b0);
+            double vb = col[rb];
+            for (int kk = c; kk >= 1; --kk) {
+                const long long xg = gs + b0 + kk;
+                const double cc = w.gc[xg], ss = w.gs[xg];
+                const int rx = vec_row_active(w, gs, b0 + kk);
+                const double vx = col[rx];
+                col[rx] = ss * vb + cc * vx;
+                vb = cc * vb - ss * vx;
+            }
+            col[rb] = vb;
+            b0 += c;
+        }
+    }
+}
+
+// The top node's eigenvectors into Z (ld ldz) with the signs of E: the
+// solve works on |E|, and T = S |T| S with S = diag(s), s_0 = 1,
+// s_{i+1} = s_i sign(E_i) (+1 for E_i = 0).  sgn holds s.
+__global__ void __launch_bounds__(256) k_vec_signs(const double *E, long long n, double *sgn) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        double s = 1.0;
+        sgn[0] = 1.0;
+        for (long long i = 0; i + 1 < n; ++i) {
+            s = E[i] < 0.0 ? -s : s;
+            sgn[i + 1] = s;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_vec_out(const double *Q, long long ldq, long long n,
+                                                 const double *sgn, double *Z, long long ldz) {
+    const long long total = n * n;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long col = t / n, row = t % n;
+        Z[col * ldz + row] = sgn[row] * Q[col * ldq + row];
+    }
+}
+
+} // namespace brdc

@@ -141,3 +141,14 @@ def test_lapacke_checks_without_device(built_lib, name, ctype):
     assert fn(-2, d, e) == -1
     one = (ctype * 1)(3.25)
     assert fn(1, one, (ctype * 1)()) == 0 and one[0] == 3.25
+
+
+def test_vectors_workspace_query(built_lib):
+    lib = brdc.load()
+    nb = ctypes.c_size_t(0)
+    assert lib.brdc_dstebr_vectors_workspace_size(4096, ctypes.byref(nb)) == brdc.SUCCESS
+    # the checkpoints plus M (n^2) and two half-size eigenvector buffers
+    assert nb.value >= 16 * 4096 * 4096 and nb.value % 256 == 0
+    assert lib.brdc_dstebr_vectors_workspace_size(0, ctypes.byref(nb)) == brdc.INVALID_VALUE
+    assert lib.brdc_dstebr_vectors_workspace_size(1 << 20, ctypes.byref(nb)) == brdc.INVALID_VALUE
+    assert lib.brdc_dstebr_vectors(None, 10, None, None, None, None, 10, None, 0) == brdc.INVALID_HANDLE
