@@ -547,6 +547,47 @@ def bench_paper_inputs(torch, solver, flush, n=8192):
     return out
 
 
+def bench_vectors(torch, brdc, families, sizes=(4096, 16384)):
+    """The eigenvector path (brdc_dstebr_vectors) on the normal family:
+    median ms of 3 calls, max |Z^T Z - I| and max |T Z - Z diag(W)| / ||T||
+    (computed on the device), and the FP64 rate of its (4/3) n^3 GEMM flops."""
+    import ctypes
+
+    out = {}
+    solver = brdc.Solver()
+    for n in sizes:
+        d, e = families.generate("normal", n)
+        D = torch.tensor(d, device="cuda")
+        E = torch.tensor(e, device="cuda")
+        nb = ctypes.c_size_t(0)
+        brdc.load().brdc_dstebr_vectors_workspace_size(n, ctypes.byref(nb))
+        ws = torch.empty(nb.value, dtype=torch.uint8, device="cuda")
+        W, Z = solver.dstebr_vectors(D, E, workspace=ws)
+        ts = []
+        for _ in range(3):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            W, Z = solver.dstebr_vectors(D, E, workspace=ws)
+            e1.record()
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        Zc = Z.contiguous()
+        orth = (Zc.t() @ Zc - torch.eye(n, dtype=torch.float64, device="cuda")).abs().max().item()
+        TZ = D[:, None] * Zc
+        TZ[:-1] += E[:, None] * Zc[1:]
+        TZ[1:] += E[:, None] * Zc[:-1]
+        res = (TZ - Zc * W[None, :]).abs().max().item() / W.abs().max().item()
+        ms = float(np.median(ts))
+        out[str(n)] = {"ms": ms, "max_orth_err": orth, "max_residual_over_normT": res,
+                       "gemm_tflops": (4.0 / 3.0) * n ** 3 / (ms * 1e-3) / 1e12,
+                       "workspace_bytes": nb.value}
+        del ws, Z, Zc, TZ
+        torch.cuda.empty_cache()
+    solver.close()
+    return out
+
+
 def collect_extras(torch, brdc, families, solver, D, E, W, ws, d, e, flush, args):
     out = {}
     headline_tuning = solver.tuning()
@@ -612,6 +653,7 @@ def collect_extras(torch, brdc, families, solver, D, E, W, ws, d, e, flush, args
     solver.set_tuning(**DEFAULT_TUNING)
     out["config2"] = bench_config2(torch, families, solver, flush)
     out["paper_inputs"] = bench_paper_inputs(torch, solver, flush)
+    out["vectors"] = bench_vectors(torch, brdc, families)
     solver.set_tuning(**headline_tuning)
     out["fwd_bwd"] = bench_fwd_bwd(torch, families, solver, flush, args)
     out["batched"] = bench_batched(torch, brdc, families, solver, flush)
