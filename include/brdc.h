@@ -297,8 +297,9 @@ brdc_status brdc_dstebr_batched_backward(brdc_handle handle, int64_t count,
  * Z column-major n x n (ld ldz >= n), column j the unit eigenvector of
  * W[j].  The workspace (query below) holds the checkpoints, M and two
  * levels of eigenvector blocks, about 16 n^2 bytes; n <= 32768.
- * Synchronises the handle's stream (the per-level GEMM tables come from
- * the host); not graph-capturable. */
+ * Asynchronous on the handle's stream.  The first call on a handle creates
+ * its GEMM library handle, so make it outside a graph capture; later calls
+ * can be captured. */
 brdc_status brdc_dstebr_vectors_workspace_size(int64_t n, size_t *bytes);
 brdc_status brdc_dstebr_vectors(brdc_handle handle, int64_t n, const double *d_D,
                                 const double *d_E, double *d_W, double *d_Z,

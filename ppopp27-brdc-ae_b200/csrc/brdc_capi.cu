@@ -1855,11 +1855,6 @@ extern "C" brdc_status brdc_dstebr_vectors(brdc_handle h, int64_t n, const doubl
     const double one = 1.0, zero = 0.0;
     double *qprev = nullptr, *qcur = qa;
     long long prev_mmax = 16;
-    struct Group {
-        int rows, m, lda, ldc;
-        std::vector<const double *> A, B;
-        std::vector<double *> C;
-    };
     for (int k = 0; k < Lv; ++k) {
         Ws wl = w;
         level_view(hf, L, w, k, &wl);
@@ -1882,64 +1877,64 @@ extern "C" brdc_status brdc_dstebr_vectors(brdc_handle h, int64_t n, const doubl
         k_vec_build<<<(unsigned)eg, 256, 0, s>>>(va, n);
         BRDC_CUDA(h, "brdc.vectors.build", cudaGetLastError());
         // Q_node = blockdiag(Q_left, Q_right) * M_node: two GEMMs per node,
-        // batched over nodes of equal shape
-        const double *child = (k == 0) ? wl.leafv : qprev;
-        double *out = top ? d_Z : qcur;
-        std::vector<Group> groups;
+        // batched over the nodes of equal shape (tables built on the device)
         const int depth = Lv - 1 - k;
-        for (int g = 0; g < hf.level_nodes[k]; ++g) {
+        const int nodes = hf.level_nodes[k];
+        int msmall = 0, mlarge = 0, cs = 0, cl = 0;
+        for (int g = 0; g < nodes; ++g) {
             long long st0 = 0, m = 0;
             walk_node(n, depth, g, &st0, &m);
-            const int m1 = (int)(m >> 1), m2 = (int)(m - m1);
-            for (int half = 0; half < 2; ++half) {
-                const int rows = half ? m2 : m1;
-                const long long cst = st0 + (half ? m1 : 0);
-                const int lda = (k == 0) ? 16 : rows;
-                const int ldc = top ? (int)ldz : (int)m;
-                const double *A = (k == 0) ? child + cst * 16 : child + cst * prev_mmax;
-                const double *B = M + st0 * mmax + (half ? m1 : 0);
-                double *C = top ? out + (half ? m1 : 0) : out + st0 * mmax + (half ? m1 : 0);
-                Group *gp = nullptr;
-                for (auto &q : groups) {
-                    if (q.rows == rows && q.m == (int)m && q.lda == lda && q.ldc == ldc) {
-                        gp = &q;
-                        break;
-                    }
-                }
-                if (gp == nullptr) {
-                    groups.push_back(Group{rows, (int)m, lda, ldc, {}, {}, {}});
-                    gp = &groups.back();
-                }
-                gp->A.push_back(A);
-                gp->B.push_back(B);
-                gp->C.push_back(C);
+            if (msmall == 0 || m < msmall) {
+                msmall = (int)m;
             }
+            mlarge = std::max(mlarge, (int)m);
         }
-        size_t used = 0;
-        for (auto &q : groups) {
-            const size_t cnt = q.A.size();
-            std::vector<const void *> tab;
-            tab.reserve(3 * cnt);
-            for (size_t i = 0; i < cnt; ++i) tab.push_back(q.A[i]);
-            for (size_t i = 0; i < cnt; ++i) tab.push_back(q.B[i]);
-            for (size_t i = 0; i < cnt; ++i) tab.push_back(q.C[i]);
-            double **dev = ptrs + used;
-            BRDC_CUDA(h, "brdc.vectors.ptrs",
-                      cudaMemcpyAsync(dev, tab.data(), sizeof(void *) * tab.size(),
-                                      cudaMemcpyHostToDevice, s));
-            used += tab.size();
+        for (int g = 0; g < nodes; ++g) {
+            long long st0 = 0, m = 0;
+            walk_node(n, depth, g, &st0, &m);
+            ((int)m == msmall ? cs : cl) += 1;
+        }
+        VecTables vt{};
+        vt.n = n;
+        vt.depth = depth;
+        vt.nodes = nodes;
+        vt.msmall = msmall;
+        vt.cs = cs;
+        vt.cl = cl;
+        vt.off[0] = 0;
+        vt.off[1] = 3LL * cs;
+        vt.off[2] = 6LL * cs;
+        vt.off[3] = 6LL * cs + 3LL * cl;
+        vt.child = (k == 0) ? wl.leafv : qprev;
+        vt.leafchild = (k == 0) ? 1 : 0;
+        vt.child_stride = prev_mmax;
+        vt.M = M;
+        vt.mstride = mmax;
+        vt.out = top ? d_Z : qcur;
+        vt.top = top ? 1 : 0;
+        vt.tab = const_cast<const double **>(ptrs);
+        k_vec_tables<<<1, 1024, 0, s>>>(vt);
+        BRDC_CUDA(h, "brdc.vectors.tables", cudaGetLastError());
+        for (int grp = 0; grp < 4; ++grp) {
+            const int cnt = grp < 2 ? cs : cl;
+            if (cnt == 0) {
+                continue;
+            }
+            const int m = grp < 2 ? msmall : mlarge;
+            const int rows = (grp & 1) ? m - (m >> 1) : (m >> 1);
+            const int lda = (k == 0) ? 16 : rows;
+            const int ldc = top ? (int)ldz : m;
+            double **dev = ptrs + vt.off[grp];
             const cublasStatus_t bs = cublasDgemmBatched(
-                h->blas, CUBLAS_OP_N, CUBLAS_OP_N, q.rows, q.m, q.rows, &one,
-                reinterpret_cast<const double *const *>(dev), q.lda,
-                reinterpret_cast<const double *const *>(dev + cnt), q.m, &zero, dev + 2 * cnt, q.ldc,
-                (int)cnt);
+                h->blas, CUBLAS_OP_N, CUBLAS_OP_N, rows, m, rows, &one,
+                reinterpret_cast<const double *const *>(dev), lda,
+                reinterpret_cast<const double *const *>(dev + cnt), m, &zero, dev + 2 * cnt, ldc,
+                cnt);
             if (bs != CUBLAS_STATUS_SUCCESS) {
                 set_error(h, (int)bs, BRDC_ERROR_SRC_CUDA, "brdc.vectors.gemm");
                 return BRDC_STATUS_INTERNAL_ERROR;
             }
         }
-        // the pointer tables of this level stay in use until its GEMMs ran
-        BRDC_CUDA(h, "brdc.vectors.level", cudaStreamSynchronize(s));
         qprev = qcur;
         qcur = (qcur == qa) ? qb : qa;
         prev_mmax = mmax;

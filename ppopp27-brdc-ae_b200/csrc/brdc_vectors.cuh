@@ -155,6 +155,60 @@ __global__ void __launch_bounds__(256) k_vec_build(VArgs a, long long total_n) {
     }
 }
 
+// GEMM pointer tables of one level, written on the device so the level's
+// products need nothing from the host: nodes have at most two sizes per
+// level (the tree splits floor/ceil), so the shapes fall in up to four
+// groups -- (top half, bottom half) x (smaller, larger node) -- each stored
+// as A[cnt], B[cnt], C[cnt] from tab + off[group], a node's slot being its
+// rank among the level's nodes of its size.
+struct VecTables {
+    long long n;
+    int depth, nodes;
+    int msmall, cs, cl; // smaller node size, nodes of each size
+    long long off[4];
+    const double *child; // the leaves' eigenvectors (ld 16) or the level below's blocks
+    int leafchild;
+    long long child_stride; // mmax of the level below
+    const double *M;
+    long long mstride;
+    double *out;
+    int top;
+    const double **tab;
+};
+
+__global__ void __launch_bounds__(1024) k_vec_tables(VecTables t) {
+    __shared__ int iscan[32];
+    int carry = 0;
+    for (int base = 0; base < t.nodes; base += 1024) {
+        const int g = base + threadIdx.x;
+        long long st = 0, m = 0;
+        if (g < t.nodes) {
+            walk_node(t.n, t.depth, g, &st, &m);
+        }
+        const int small = (g < t.nodes && (int)m == t.msmall) ? 1 : 0;
+        int tot;
+        const int ex = block_exscan<1024>(small, iscan, &tot);
+        if (g < t.nodes) {
+            const int rs = carry + ex;
+            const int idx = small ? rs : g - rs;
+            const int cnt = small ? t.cs : t.cl;
+            const long long h1 = m >> 1;
+            for (int half = 0; half < 2; ++half) {
+                const long long cst = st + (half ? h1 : 0);
+                const double *A = t.leafchild ? t.child + cst * 16 : t.child + cst * t.child_stride;
+                const double *B = t.M + st * t.mstride + (half ? h1 : 0);
+                double *C = t.top ? t.out + (half ? h1 : 0) : t.out + st * t.mstride + (half ? h1 : 0);
+                const long long o = t.off[(small ? 0 : 2) + half];
+                t.tab[o + idx] = A;
+                t.tab[o + cnt + idx] = B;
+                t.tab[o + 2 * cnt + idx] = C;
+            }
+        }
+        carry += tot;
+        __syncthreads();
+    }
+}
+
 // The top node's eigenvectors into Z (ld ldz) with the signs of E: the
 // solve works on |E|, and T = S |T| S with S = diag(s), s_0 = 1,
 // s_{i+1} = s_i sign(E_i) (+1 for E_i = 0).  sgn holds s.

@@ -75,3 +75,47 @@ def test_zero_and_negative_couplings(solver):
     e[::37] = 0.0
     e[5::11] *= -1.0
     check(solver, d, e, 1e-12, 1e-13)
+
+
+@pytest.mark.parametrize("n", [3001, 5000])
+def test_two_node_sizes(solver, n):
+    # orders that are not powers of two: every level has nodes of two sizes,
+    # hence four GEMM shapes
+    d, e = families.generate("normal", n)
+    check(solver, d, e, 1e-11, 1e-12)
+
+
+def test_graph_capture(solver):
+    import ctypes
+
+    import torch
+
+    import brdc
+
+    n = 3001
+    d, e = families.generate("uniform", n)
+    D = torch.tensor(d, device="cuda")
+    E = torch.tensor(e, device="cuda")
+    s = brdc.Solver()
+    g = None
+    try:
+        nb = ctypes.c_size_t(0)
+        brdc.load().brdc_dstebr_vectors_workspace_size(n, ctypes.byref(nb))
+        ws = torch.empty(nb.value, dtype=torch.uint8, device="cuda")
+        stream = torch.cuda.Stream()
+        stream.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(stream):
+            s.set_stream(stream)
+            W0, Z0 = s.dstebr_vectors(D, E, workspace=ws)  # creates the GEMM handle
+            W0, Z0 = W0.clone(), Z0.clone()
+            stream.synchronize()
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=stream):
+                W1, Z1 = s.dstebr_vectors(D, E, workspace=ws)
+            g.replay()
+            stream.synchronize()
+        assert torch.equal(W0, W1) and torch.equal(Z0, Z1)
+    finally:
+        del g
+        s.set_stream(torch.cuda.current_stream())
+        s.close()
