@@ -188,6 +188,15 @@ def run_profile_case(spec):
     from brdc import families
 
     parts = spec.split(":")
+    if parts[0] == "vectors":
+        # vectors:family:n -- one eigenvector solve (brdc_dstebr_vectors)
+        fam, n = parts[1], int(parts[2])
+        d, e = families.generate(fam, n)
+        solver = brdc.Solver()
+        W, Z = solver.dstebr_vectors(torch.tensor(d, device="cuda"), torch.tensor(e, device="cuda"))
+        torch.cuda.synchronize()
+        solver.close()
+        return
     fam, n = parts[0], int(parts[1])
     solves = int(parts[2]) if len(parts) > 2 else 1
     adjoint = len(parts) > 3 and parts[3] == "bwd"
@@ -217,7 +226,8 @@ def main():
     ap.add_argument("--profile-case", default=None,
                     help="family:n[:solves[:bwd]] -- run that many plain solves (default 1) of "
                          "the seeded instance, each followed by the adjoint with bwd, and exit; "
-                         "a fixed launch sequence for profilers")
+                         "vectors:family:n -- one eigenvector solve; a fixed launch sequence "
+                         "for profilers")
     ap.add_argument("--input", default=None,
                     help="solve the tridiagonal of a .de.bin file instead of the headline input")
     ap.add_argument("--data", default=None,

@@ -1839,7 +1839,7 @@ extern "C" brdc_status brdc_dstebr_vectors(brdc_handle h, int64_t n, const doubl
     double *M = reinterpret_cast<double *>(base + V.qa + V.qb);
     double **ptrs = reinterpret_cast<double **>(base + V.qa + V.qb + V.mm);
     double *sgn = reinterpret_cast<double *>(base + V.qa + V.qb + V.mm + V.ptrs);
-    k_vec_signs<<<1, 32, 0, s>>>(d_E, n, sgn);
+    k_vec_signs<<<1, 1024, 0, s>>>(d_E, n, sgn);
     BRDC_CUDA(h, "brdc.vectors.signs", cudaGetLastError());
     const int Lv = hf.max_levels;
     long long eg = (n + 255) / 256;

@@ -211,15 +211,23 @@ __global__ void __launch_bounds__(1024) k_vec_tables(VecTables t) {
 
 // The top node's eigenvectors into Z (ld ldz) with the signs of E: the
 // solve works on |E|, and T = S |T| S with S = diag(s), s_0 = 1,
-// s_{i+1} = s_i sign(E_i) (+1 for E_i = 0).  sgn holds s.
-__global__ void __launch_bounds__(256) k_vec_signs(const double *E, long long n, double *sgn) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        double s = 1.0;
-        sgn[0] = 1.0;
-        for (long long i = 0; i + 1 < n; ++i) {
-            s = E[i] < 0.0 ? -s : s;
-            sgn[i + 1] = s;
-        }
+// s_{i+1} = s_i sign(E_i) (+1 for E_i = 0), i.e. s_i = (-1)^(negative E_j,
+// j < i).  One block: each thread counts the negatives of a contiguous
+// chunk, a block scan gives every chunk its parity.
+__global__ void __launch_bounds__(1024) k_vec_signs(const double *E, long long n, double *sgn) {
+    __shared__ int iscan[32];
+    const long long chunk = (n + 1023) / 1024;
+    const long long lo = (long long)threadIdx.x * chunk;
+    const long long hi = lo + chunk < n ? lo + chunk : n;
+    int neg = 0;
+    for (long long i = lo; i < hi; ++i) {
+        neg += (i > 0 && E[i - 1] < 0.0) ? 1 : 0;
+    }
+    int tot;
+    int par = block_exscan<1024>(neg, iscan, &tot);
+    for (long long i = lo; i < hi; ++i) {
+        par += (i > 0 && E[i - 1] < 0.0) ? 1 : 0;
+        sgn[i] = (par & 1) ? -1.0 : 1.0;
     }
 }
 
