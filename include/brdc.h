@@ -291,15 +291,19 @@ brdc_status brdc_dstebr_batched_backward(brdc_handle handle, int64_t count,
 /* Eigenvalues and eigenvectors: the vector path of the reference's solver
  * (compute_eigenvectors = 1, gpu/src/tridiag_solver.cu:848-1071).  A
  * checkpointing values solve records every merge; each node's eigenvector
- * matrix is then blockdiag(Q_left, Q_right) * M_node, with M_node built from
- * the recorded permutations, deflation rotations and secular vectors
+ * matrix is then assembled from its children's: the deflated eigenvectors
+ * are children's eigenvectors (or short rotation combinations of them),
+ * the K root eigenvectors blockdiag(Q_left, Q_right) * M_node[:, :K], M
+ * built from the recorded permutations, rotations and secular vectors
  * (Loewner weights), the products by library FP64 GEMMs.  W[n] ascending,
  * Z column-major n x n (ld ldz >= n), column j the unit eigenvector of
- * W[j].  The workspace (query below) holds the checkpoints, M and two
- * levels of eigenvector blocks, about 16 n^2 bytes; n <= 32768.
- * Asynchronous on the handle's stream.  The first call on a handle creates
- * its GEMM library handle, so make it outside a graph capture; later calls
- * can be captured. */
+ * W[j].  The workspace (query below) holds the checkpoints, M, the
+ * products and two levels of eigenvector blocks, about 24 n^2 bytes;
+ * n <= 32768.  It reads each level's largest K back once (a stream
+ * synchronisation) to size the products; inside a graph capture it reads
+ * nothing and multiplies every column instead (same result, more flops).
+ * The first call on a handle creates its GEMM library handle, so make it
+ * outside a capture. */
 brdc_status brdc_dstebr_vectors_workspace_size(int64_t n, size_t *bytes);
 brdc_status brdc_dstebr_vectors(brdc_handle handle, int64_t n, const double *d_D,
                                 const double *d_E, double *d_W, double *d_Z,

@@ -1745,10 +1745,11 @@ namespace {
 // Workspace of the vector path: the checkpointing layout of the values
 // solve, then two buffers for the eigenvector blocks of consecutive levels
 // (node g's block at gstart * mmax of its level, n x ceil(n/2) doubles at
-// most below the top), M of one level (n x n at the top), the GEMM pointer
-// tables and the row signs.
+// most below the top), the root columns of M of one level and their
+// products (n x Kmax each), the GEMM pointer tables, the row signs and the
+// per-level Kmax.
 struct VecLayout {
-    size_t ckpt, qa, qb, mm, ptrs, sgn, total;
+    size_t ckpt, qa, qb, mm, cm, ptrs, sgn, kmax, total;
 };
 
 VecLayout vec_layout(const HostForest &hf, long long n) {
@@ -1758,9 +1759,11 @@ VecLayout vec_layout(const HostForest &hf, long long n) {
     v.qa = align_up(half);
     v.qb = align_up(half);
     v.mm = align_up((size_t)n * (size_t)n * sizeof(double));
+    v.cm = v.mm;
     v.ptrs = align_up(sizeof(double *) * 6 * (size_t)(hf.nn0 + 1));
     v.sgn = align_up(sizeof(double) * (size_t)n);
-    v.total = v.ckpt + v.qa + v.qb + v.mm + v.ptrs + v.sgn;
+    v.kmax = align_up(sizeof(int) * (size_t)(hf.max_levels + 1));
+    v.total = v.ckpt + v.qa + v.qb + v.mm + v.cm + v.ptrs + v.sgn + v.kmax;
     return v;
 }
 
@@ -1837,13 +1840,15 @@ extern "C" brdc_status brdc_dstebr_vectors(brdc_handle h, int64_t n, const doubl
     double *qa = reinterpret_cast<double *>(base);
     double *qb = reinterpret_cast<double *>(base + V.qa);
     double *M = reinterpret_cast<double *>(base + V.qa + V.qb);
-    double **ptrs = reinterpret_cast<double **>(base + V.qa + V.qb + V.mm);
-    double *sgn = reinterpret_cast<double *>(base + V.qa + V.qb + V.mm + V.ptrs);
+    double *Cm = reinterpret_cast<double *>(base + V.qa + V.qb + V.mm);
+    double **ptrs = reinterpret_cast<double **>(base + V.qa + V.qb + V.mm + V.cm);
+    double *sgn = reinterpret_cast<double *>(base + V.qa + V.qb + V.mm + V.cm + V.ptrs);
+    int *dkmax = reinterpret_cast<int *>(base + V.qa + V.qb + V.mm + V.cm + V.ptrs + V.sgn);
     k_vec_signs<<<1, 1024, 0, s>>>(d_E, n, sgn);
     BRDC_CUDA(h, "brdc.vectors.signs", cudaGetLastError());
     const int Lv = hf.max_levels;
-    long long eg = (n + 255) / 256;
-    eg = std::max<long long>(1, std::min<long long>(eg, (long long)h->sm_count * 8));
+    long long eg = (n + 7) / 8; // one warp per slot, 8 warps a block
+    eg = std::max<long long>(1, std::min<long long>(eg, (long long)h->sm_count * 16));
     long long zg = (n * n + 255) / 256;
     zg = std::max<long long>(1, std::min<long long>(zg, (long long)h->sm_count * 16));
     if (Lv == 0) {
@@ -1851,6 +1856,28 @@ extern "C" brdc_status brdc_dstebr_vectors(brdc_handle h, int64_t n, const doubl
         k_vec_out<<<(unsigned)zg, 256, 0, s>>>(w.leafv, 16, n, sgn, d_Z, ldz);
         BRDC_CUDA(h, "brdc.vectors.leaf", cudaGetLastError());
         return BRDC_STATUS_SUCCESS;
+    }
+    // the largest K of every level sizes its products (the one read back);
+    // inside a graph capture nothing can be read, and every level takes
+    // its largest node's order instead (the same result, more flops)
+    std::vector<int> kmax(Lv, 0);
+    cudaStreamCaptureStatus capst = cudaStreamCaptureStatusNone;
+    BRDC_CUDA(h, "brdc.vectors.capture", cudaStreamIsCapturing(s, &capst));
+    if (capst != cudaStreamCaptureStatusNone) {
+        for (int k = 0; k < Lv; ++k) {
+            kmax[k] = hf.level_mmax[k];
+        }
+    } else {
+        BRDC_CUDA(h, "brdc.vectors.kmax_zero", cudaMemsetAsync(dkmax, 0, sizeof(int) * Lv, s));
+        for (int k = 0; k < Lv; ++k) {
+            Ws wl = w;
+            level_view(hf, L, w, k, &wl);
+            k_vec_kmax<<<1, 256, 0, s>>>(wl.nK, hf.level_nodes[k], dkmax + k);
+        }
+        BRDC_CUDA(h, "brdc.vectors.kmax", cudaGetLastError());
+        BRDC_CUDA(h, "brdc.vectors.kmax_read",
+                  cudaMemcpyAsync(kmax.data(), dkmax, sizeof(int) * Lv, cudaMemcpyDeviceToHost, s));
+        BRDC_CUDA(h, "brdc.vectors.kmax_sync", cudaStreamSynchronize(s));
     }
     const double one = 1.0, zero = 0.0;
     double *qprev = nullptr, *qcur = qa;
@@ -1860,24 +1887,42 @@ extern "C" brdc_status brdc_dstebr_vectors(brdc_handle h, int64_t n, const doubl
         level_view(hf, L, w, k, &wl);
         const bool top = (k == Lv - 1);
         const long long mmax = hf.level_mmax[k];
+        const int Km = kmax[k];
         VArgs va{};
         va.F = F;
         va.w = wl;
         va.M = M;
-        va.mstride = mmax;
+        va.mstride = std::max(Km, 1);
         va.k = k;
         va.nodes = hf.level_nodes[k];
+        va.child = (k == 0) ? wl.leafv : qprev;
+        va.leafchild = (k == 0) ? 1 : 0;
+        va.child_stride = prev_mmax;
+        va.out = top ? d_Z : qcur;
+        va.out_stride = mmax;
+        va.top = top ? 1 : 0;
+        va.ldout = ldz;
         if (top) {
             k_vec_lowner<<<(unsigned)std::max<long long>(1, std::min<long long>((n + 7) / 8, h->sm_count * 8)),
                            256, 0, s>>>(va);
             BRDC_CUDA(h, "brdc.vectors.lowner", cudaGetLastError());
         }
-        BRDC_CUDA(h, "brdc.vectors.zero",
-                  cudaMemsetAsync(M, 0, sizeof(double) * (size_t)n * (size_t)mmax, s));
+        if (Km > 0) {
+            BRDC_CUDA(h, "brdc.vectors.zero",
+                      cudaMemsetAsync(M, 0, sizeof(double) * (size_t)n * (size_t)Km, s));
+        }
+        // root columns of M; the deflated eigenvectors straight to the blocks
         k_vec_build<<<(unsigned)eg, 256, 0, s>>>(va, n);
         BRDC_CUDA(h, "brdc.vectors.build", cudaGetLastError());
-        // Q_node = blockdiag(Q_left, Q_right) * M_node: two GEMMs per node,
-        // batched over the nodes of equal shape (tables built on the device)
+        if (Km == 0) {
+            qprev = qcur;
+            qcur = (qcur == qa) ? qb : qa;
+            prev_mmax = mmax;
+            continue;
+        }
+        // the roots: C = blockdiag(Q_left, Q_right) * M[:, :Kmax], two GEMMs
+        // per node, batched over the nodes of equal shape (tables built on
+        // the device), then each root column to its place
         const int depth = Lv - 1 - k;
         const int nodes = hf.level_nodes[k];
         int msmall = 0, mlarge = 0, cs = 0, cl = 0;
@@ -1905,13 +1950,12 @@ extern "C" brdc_status brdc_dstebr_vectors(brdc_handle h, int64_t n, const doubl
         vt.off[1] = 3LL * cs;
         vt.off[2] = 6LL * cs;
         vt.off[3] = 6LL * cs + 3LL * cl;
-        vt.child = (k == 0) ? wl.leafv : qprev;
-        vt.leafchild = (k == 0) ? 1 : 0;
+        vt.child = va.child;
+        vt.leafchild = va.leafchild;
         vt.child_stride = prev_mmax;
         vt.M = M;
-        vt.mstride = mmax;
-        vt.out = top ? d_Z : qcur;
-        vt.top = top ? 1 : 0;
+        vt.C = Cm;
+        vt.stride = va.mstride;
         vt.tab = const_cast<const double **>(ptrs);
         k_vec_tables<<<1, 1024, 0, s>>>(vt);
         BRDC_CUDA(h, "brdc.vectors.tables", cudaGetLastError());
@@ -1923,18 +1967,19 @@ extern "C" brdc_status brdc_dstebr_vectors(brdc_handle h, int64_t n, const doubl
             const int m = grp < 2 ? msmall : mlarge;
             const int rows = (grp & 1) ? m - (m >> 1) : (m >> 1);
             const int lda = (k == 0) ? 16 : rows;
-            const int ldc = top ? (int)ldz : m;
             double **dev = ptrs + vt.off[grp];
             const cublasStatus_t bs = cublasDgemmBatched(
-                h->blas, CUBLAS_OP_N, CUBLAS_OP_N, rows, m, rows, &one,
+                h->blas, CUBLAS_OP_N, CUBLAS_OP_N, rows, Km, rows, &one,
                 reinterpret_cast<const double *const *>(dev), lda,
-                reinterpret_cast<const double *const *>(dev + cnt), m, &zero, dev + 2 * cnt, ldc,
+                reinterpret_cast<const double *const *>(dev + cnt), m, &zero, dev + 2 * cnt, m,
                 cnt);
             if (bs != CUBLAS_STATUS_SUCCESS) {
                 set_error(h, (int)bs, BRDC_ERROR_SRC_CUDA, "brdc.vectors.gemm");
                 return BRDC_STATUS_INTERNAL_ERROR;
             }
         }
+        k_vec_scatter<<<(unsigned)eg, 256, 0, s>>>(va, Cm, n);
+        BRDC_CUDA(h, "brdc.vectors.scatter", cudaGetLastError());
         qprev = qcur;
         qcur = (qcur == qa) ? qb : qa;
         prev_mmax = mmax;

@@ -30,10 +30,21 @@ namespace brdc {
 struct VArgs {
     Forest F;
     Ws w;         // the level's checkpoint slices
-    double *M;    // node g's M at M + gstart * mstride, column-major, ld m
+    double *M;    // node g's root columns at M + gstart * mstride, column-major, ld m
     long long mstride;
     int k;
     int nodes;
+    // eigenvector blocks of the children: the leaves (ld 16) or the level
+    // below (node at gstart * child_stride, ld its rows)
+    const double *child;
+    int leafchild;
+    long long child_stride;
+    // this level's blocks: node at gstart * out_stride, ld m; the top node
+    // at out with ld ldout
+    double *out;
+    long long out_stride;
+    int top;
+    long long ldout;
 };
 
 // Loewner weights of the instance-root merges, which the values solve
@@ -76,13 +87,37 @@ __device__ inline int vec_row_small(const Ws &w, long long gs, int q) {
     return w.morig[gs + w.zmap[gs + q]];
 }
 
-// One thread per slot of the level (root, small-z, rotated-out): its
-// position in the node's ascending order (the placement rule: ties go
-// roots, small-z, rotated-out), then its column of M.  M must be zero.
+// Position of slot s of a node in its ascending order (the placement rule:
+// ties go roots, small-z, rotated-out).
+__device__ inline int vec_pos(const Ws &w, long long gs, long long po, int s, int K, int ndz,
+                              int ndg) {
+    const double *zdl = w.zd + gs;
+    const double *gdl = w.gd + gs;
+    const double *rl = w.rlam + po;
+    if (s < K) {
+        return s + lower_bound_d(zdl, ndz, rl[s]) + lower_bound_d(gdl, ndg, rl[s]);
+    }
+    if (s < K + ndz) {
+        const int q = s - K;
+        return q + upper_bound_d(rl, K, zdl[q]) + lower_bound_d(gdl, ndg, zdl[q]);
+    }
+    const int q = s - K - ndz;
+    return q + upper_bound_d(rl, K, gdl[q]) + upper_bound_d(zdl, ndz, gdl[q]);
+}
+
+// One warp per slot of the level (lanes over rows and poles).  A root s
+// writes its column of M at column s (u_i = w_i / delta_i(s) over the
+// poles, normalised, then the chains undone on the rows -- chains touch
+// disjoint rows, so lanes take different chains); the products turn these
+// into the node's root eigenvectors.  A deflated slot is a child
+// eigenvector (small-z) or a short rotation combination of some (rotated
+// out), written straight to its place in the node's block.  M must be zero.
 __global__ void __launch_bounds__(256) k_vec_build(VArgs a, long long total_n) {
     const Ws &w = a.w;
-    for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x; x < total_n;
-         x += (long long)gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31;
+    const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long x = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); x < total_n;
+         x += warps) {
         int g, m, depth;
         long long gs;
         if (!elem_node(a.F, a.k, x, &g, &gs, &m, &depth)) {
@@ -93,65 +128,140 @@ __global__ void __launch_bounds__(256) k_vec_build(VArgs a, long long total_n) {
         const int K = w.nK[g];
         const int Kz = w.nKz[g];
         const int ndz = m - Kz, ndg = Kz - K;
-        const double *zdl = w.zd + gs;
-        const double *gdl = w.gd + gs;
-        const double *rl = w.rlam + po;
-        int pos;
+        const int m1 = m >> 1;
         if (s < K) {
-            pos = s + lower_bound_d(zdl, ndz, rl[s]) + lower_bound_d(gdl, ndg, rl[s]);
-        } else if (s < K + ndz) {
-            const int q = s - K;
-            pos = q + upper_bound_d(rl, K, zdl[q]) + lower_bound_d(gdl, ndg, zdl[q]);
-        } else {
-            const int q = s - K - ndz;
-            pos = q + upper_bound_d(rl, K, gdl[q]) + upper_bound_d(zdl, ndz, gdl[q]);
-        }
-        double *col = a.M + gs * a.mstride + (long long)pos * m;
-        if (s >= K && s < K + ndz) {
-            col[vec_row_small(w, gs, s - K)] = 1.0; // no chain touches it
-            continue;
-        }
-        if (s < K) {
-            // u_i = w_i / delta_i(s) over the poles, normalised
+            double *col = a.M + gs * a.mstride + (long long)s * m;
             const int org = w.rorg[po + s];
             const double dorg = w.rdo[po + s], tau = w.rtau[po + s];
             double s2 = 0.0;
-            for (int i = 0; i < K; ++i) {
+            for (int i = lane; i < K; i += 32) {
                 const double dl = (i == org) ? -tau : (w.pd[po + i] - dorg) - tau;
                 const double u = w.pw[po + i] / dl;
                 s2 += u * u;
             }
+            s2 = warp_sum(s2);
             const double inv = 1.0 / sqrt(s2);
-            for (int i = 0; i < K; ++i) {
+            for (int i = lane; i < K; i += 32) {
                 const double dl = (i == org) ? -tau : (w.pd[po + i] - dorg) - tau;
                 col[vec_row_active(w, gs, w.pmap[po + i])] = w.pw[po + i] / dl * inv;
             }
-        } else {
-            col[vec_row_active(w, gs, w.gpos[gs + (s - K - ndz)])] = 1.0;
+            __syncwarp();
+            // chains: a base has gmark 0 and a member after it
+            for (int b0 = lane; b0 + 1 < Kz; b0 += 32) {
+                if (w.gmark[gs + b0] != 0 || w.gmark[gs + b0 + 1] == 0) {
+                    continue;
+                }
+                int c = 1;
+                while (b0 + c + 1 < Kz && w.gmark[gs + b0 + c + 1] != 0) {
+                    ++c;
+                }
+                const int rb = vec_row_active(w, gs, b0);
+                double vb = col[rb];
+                for (int kk = c; kk >= 1; --kk) {
+                    const long long xg = gs + b0 + kk;
+                    const double cc = w.gc[xg], ss = w.gs[xg];
+                    const int rx = vec_row_active(w, gs, b0 + kk);
+                    const double vx = col[rx];
+                    col[rx] = ss * vb + cc * vx;
+                    vb = cc * vb - ss * vx;
+                }
+                col[rb] = vb;
+            }
+            continue;
         }
-        // undo every Givens chain on the rows (bases have gmark 0, their
-        // members follow with gmark 1, rotated in increasing order)
-        for (int b0 = 0; b0 + 1 < Kz; ++b0) {
-            if (w.gmark[gs + b0] != 0 || w.gmark[gs + b0 + 1] == 0) {
-                continue;
-            }
-            int c = 1;
-            while (b0 + c + 1 < Kz && w.gmark[gs + b0 + c + 1] != 0) {
-                ++c;
-            }
-            const int rb = vec_row_active(w, gs, b0);
-            double vb = col[rb];
-            for (int kk = c; kk >= 1; --kk) {
-                const long long xg = gs + b0 + kk;
-                const double cc = w.gc[xg], ss = w.gs[xg];
-                const int rx = vec_row_active(w, gs, b0 + kk);
-                const double vx = col[rx];
-                col[rx] = ss * vb + cc * vx;
-                vb = cc * vb - ss * vx;
-            }
-            col[rb] = vb;
-            b0 += c;
+        // deflated: a child eigenvector (small-z), or a rotated-out member
+        // whose chain, undone on its unit column, leaves c_t at the member
+        // (t), s_k * v at the earlier members k and v at the base, v running
+        // -s_t, times c_k going down: summed child eigenvectors
+        const int pos = vec_pos(w, gs, po, s, K, ndz, ndg);
+        double *dst = a.top ? a.out + (long long)pos * a.ldout
+                            : a.out + gs * a.out_stride + (long long)pos * m;
+        for (int r = lane; r < m; r += 32) {
+            dst[r] = 0.0;
         }
+        __syncwarp();
+        auto add_child = [&](int e, double cf) {
+            if (cf == 0.0) {
+                return;
+            }
+            if (e < m1) {
+                const double *c = a.leafchild ? a.child + (gs + e) * 16
+                                              : a.child + gs * a.child_stride + (long long)e * m1;
+                for (int r = lane; r < m1; r += 32) {
+                    dst[r] += cf * c[r];
+                }
+            } else {
+                const int er = e - m1, m2 = m - m1;
+                const double *c = a.leafchild
+                                      ? a.child + (gs + m1 + er) * 16
+                                      : a.child + (gs + m1) * a.child_stride + (long long)er * m2;
+                for (int r = lane; r < m2; r += 32) {
+                    dst[m1 + r] += cf * c[r];
+                }
+            }
+        };
+        if (s < K + ndz) {
+            add_child(vec_row_small(w, gs, s - K), 1.0);
+            continue;
+        }
+        const int act = w.gpos[gs + (s - K - ndz)];
+        int b0 = act;
+        while (b0 > 0 && w.gmark[gs + b0] != 0) {
+            --b0;
+        }
+        const int t0 = act - b0;
+        add_child(vec_row_active(w, gs, act), w.gc[gs + act]);
+        double v = -w.gs[gs + act];
+        for (int kk = t0 - 1; kk >= 1; --kk) {
+            const long long xg = gs + b0 + kk;
+            add_child(vec_row_active(w, gs, b0 + kk), w.gs[xg] * v);
+            v *= w.gc[xg];
+        }
+        add_child(vec_row_active(w, gs, b0), v);
+    }
+}
+
+// Root eigenvectors from the products (node's block of C, columns in root
+// order) to their places in the node's ascending order: one warp per root.
+__global__ void __launch_bounds__(256) k_vec_scatter(VArgs a, const double *C, long long total_n) {
+    const Ws &w = a.w;
+    const int lane = threadIdx.x & 31;
+    const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long x = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); x < total_n;
+         x += warps) {
+        int g, m, depth;
+        long long gs;
+        if (!elem_node(a.F, a.k, x, &g, &gs, &m, &depth)) {
+            continue;
+        }
+        const long long po = (gs + g + 1) & ~1LL;
+        const int s = (int)(x - gs);
+        const int K = w.nK[g];
+        if (s >= K) {
+            continue;
+        }
+        const int Kz = w.nKz[g];
+        const int pos = vec_pos(w, gs, po, s, K, m - Kz, Kz - K);
+        const double *src = C + gs * a.mstride + (long long)s * m;
+        double *dst = a.top ? a.out + (long long)pos * a.ldout
+                            : a.out + gs * a.out_stride + (long long)pos * m;
+        for (int r = lane; r < m; r += 32) {
+            dst[r] = src[r];
+        }
+    }
+}
+
+// Largest K over one level's merges, for the host to size the products.
+__global__ void __launch_bounds__(256) k_vec_kmax(const int *nK, int nodes, int *kmax) {
+    int mx = 0;
+    for (int g = threadIdx.x; g < nodes; g += blockDim.x) {
+        mx = max(mx, nK[g]);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(kmax, mx);
     }
 }
 
@@ -160,7 +270,8 @@ __global__ void __launch_bounds__(256) k_vec_build(VArgs a, long long total_n) {
 // level (the tree splits floor/ceil), so the shapes fall in up to four
 // groups -- (top half, bottom half) x (smaller, larger node) -- each stored
 // as A[cnt], B[cnt], C[cnt] from tab + off[group], a node's slot being its
-// rank among the level's nodes of its size.
+// rank among the level's nodes of its size.  B (the node's root columns of
+// M) and C (their products) sit at gstart * stride, ld m.
 struct VecTables {
     long long n;
     int depth, nodes;
@@ -170,9 +281,8 @@ struct VecTables {
     int leafchild;
     long long child_stride; // mmax of the level below
     const double *M;
-    long long mstride;
-    double *out;
-    int top;
+    double *C;
+    long long stride;
     const double **tab;
 };
 
@@ -196,8 +306,8 @@ __global__ void __launch_bounds__(1024) k_vec_tables(VecTables t) {
             for (int half = 0; half < 2; ++half) {
                 const long long cst = st + (half ? h1 : 0);
                 const double *A = t.leafchild ? t.child + cst * 16 : t.child + cst * t.child_stride;
-                const double *B = t.M + st * t.mstride + (half ? h1 : 0);
-                double *C = t.top ? t.out + (half ? h1 : 0) : t.out + st * t.mstride + (half ? h1 : 0);
+                const double *B = t.M + st * t.stride + (half ? h1 : 0);
+                double *C = t.C + st * t.stride + (half ? h1 : 0);
                 const long long o = t.off[(small ? 0 : 2) + half];
                 t.tab[o + idx] = A;
                 t.tab[o + cnt + idx] = B;

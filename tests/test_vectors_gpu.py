@@ -114,7 +114,10 @@ def test_graph_capture(solver):
                 W1, Z1 = s.dstebr_vectors(D, E, workspace=ws)
             g.replay()
             stream.synchronize()
-        assert torch.equal(W0, W1) and torch.equal(Z0, Z1)
+        # captured, every level multiplies all of its columns (nothing can
+        # be read back to size the products): the same vectors to rounding
+        assert torch.equal(W0, W1)
+        assert (Z0 - Z1).abs().max().item() < 1e-13
     finally:
         del g
         s.set_stream(torch.cuda.current_stream())
