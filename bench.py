@@ -560,7 +560,7 @@ def bench_paper_inputs(torch, solver, flush, n=8192):
 def bench_vectors(torch, brdc, families, sizes=(4096, 16384)):
     """The eigenvector path (brdc_dstebr_vectors) on the normal family:
     median ms of 3 calls, max |Z^T Z - I| and max |T Z - Z diag(W)| / ||T||
-    (computed on the device), and the FP64 rate of its (4/3) n^3 GEMM flops."""
+    (computed on the device)."""
     import ctypes
 
     out = {}
@@ -590,7 +590,6 @@ def bench_vectors(torch, brdc, families, sizes=(4096, 16384)):
         res = (TZ - Zc * W[None, :]).abs().max().item() / W.abs().max().item()
         ms = float(np.median(ts))
         out[str(n)] = {"ms": ms, "max_orth_err": orth, "max_residual_over_normT": res,
-                       "gemm_tflops": (4.0 / 3.0) * n ** 3 / (ms * 1e-3) / 1e12,
                        "workspace_bytes": nb.value}
         del ws, Z, Zc, TZ
         torch.cuda.empty_cache()
