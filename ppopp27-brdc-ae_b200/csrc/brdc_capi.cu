@@ -1767,15 +1767,6 @@ VecLayout vec_layout(const HostForest &hf, long long n) {
     return v;
 }
 
-__global__ void k_vec_rowscale(double *Z, long long ldz, long long n, const double *sgn) {
-    const long long total = n * n;
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
-         t += (long long)gridDim.x * blockDim.x) {
-        const long long col = t / n, row = t % n;
-        Z[col * ldz + row] *= sgn[row];
-    }
-}
-
 } // namespace
 
 extern "C" brdc_status brdc_dstebr_vectors_workspace_size(int64_t n, size_t *bytes) {
@@ -1902,6 +1893,7 @@ extern "C" brdc_status brdc_dstebr_vectors(brdc_handle h, int64_t n, const doubl
         va.out_stride = mmax;
         va.top = top ? 1 : 0;
         va.ldout = ldz;
+        va.sgn = sgn;
         if (top) {
             k_vec_lowner<<<(unsigned)std::max<long long>(1, std::min<long long>((n + 7) / 8, h->sm_count * 8)),
                            256, 0, s>>>(va);
@@ -1984,8 +1976,6 @@ extern "C" brdc_status brdc_dstebr_vectors(brdc_handle h, int64_t n, const doubl
         qcur = (qcur == qa) ? qb : qa;
         prev_mmax = mmax;
     }
-    k_vec_rowscale<<<(unsigned)zg, 256, 0, s>>>(d_Z, ldz, n, sgn);
-    BRDC_CUDA(h, "brdc.vectors.rowscale", cudaGetLastError());
     return BRDC_STATUS_SUCCESS;
 }
 

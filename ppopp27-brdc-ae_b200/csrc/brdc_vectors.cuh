@@ -45,6 +45,9 @@ struct VArgs {
     long long out_stride;
     int top;
     long long ldout;
+    // the top level writes T's eigenvectors: row i times the sign s_i of
+    // T = S |T| S (k_vec_signs)
+    const double *sgn;
 };
 
 // Loewner weights of the instance-root merges, which the values solve
@@ -188,7 +191,7 @@ __global__ void __launch_bounds__(256) k_vec_build(VArgs a, long long total_n) {
                 const double *c = a.leafchild ? a.child + (gs + e) * 16
                                               : a.child + gs * a.child_stride + (long long)e * m1;
                 for (int r = lane; r < m1; r += 32) {
-                    dst[r] += cf * c[r];
+                    dst[r] += a.top ? cf * c[r] * a.sgn[r] : cf * c[r];
                 }
             } else {
                 const int er = e - m1, m2 = m - m1;
@@ -196,7 +199,7 @@ __global__ void __launch_bounds__(256) k_vec_build(VArgs a, long long total_n) {
                                       ? a.child + (gs + m1 + er) * 16
                                       : a.child + (gs + m1) * a.child_stride + (long long)er * m2;
                 for (int r = lane; r < m2; r += 32) {
-                    dst[m1 + r] += cf * c[r];
+                    dst[m1 + r] += a.top ? cf * c[r] * a.sgn[m1 + r] : cf * c[r];
                 }
             }
         };
@@ -246,7 +249,7 @@ __global__ void __launch_bounds__(256) k_vec_scatter(VArgs a, const double *C, l
         double *dst = a.top ? a.out + (long long)pos * a.ldout
                             : a.out + gs * a.out_stride + (long long)pos * m;
         for (int r = lane; r < m; r += 32) {
-            dst[r] = src[r];
+            dst[r] = a.top ? src[r] * a.sgn[r] : src[r];
         }
     }
 }
