@@ -300,7 +300,8 @@ def main():
 
     extras = {}
     if rank == 0 and not args.no_extras:
-        extras = collect_extras(torch, brdc, families, solver, D, E, W, ws, d, e, flush, args)
+        extras = collect_extras(torch, brdc, families, solver, D, E, W, ws, d, e, flush, args,
+                                head_ms=ms)
 
     if rank == 0:
         diag = solver.diagnostics(N_HEAD, ws)
@@ -597,7 +598,129 @@ def bench_vectors(torch, brdc, families, sizes=(4096, 16384)):
     return out
 
 
-def collect_extras(torch, brdc, families, solver, D, E, W, ws, d, e, flush, args):
+def xstedc_probe():
+    """Whether cuSOLVER on this machine exports cusolverDnXstedc, the
+    routine the reference's GPU bench compares against
+    (gpu/bench/tridiag_dc_bench.cu:1144, 1277): an exported-name lookup of
+    each libcusolver the process can find, nothing more."""
+    import ctypes
+    import glob
+
+    cands = sorted(set(glob.glob("/usr/local/cuda/lib64/libcusolver.so*")))
+    try:
+        import nvidia.cusolver as nc
+
+        cands += sorted(glob.glob(os.path.join(list(nc.__path__)[0], "lib", "libcusolver.so*")))
+    except Exception:
+        pass
+    found = []
+    for path in cands:
+        try:
+            lib = ctypes.CDLL(path)
+        except OSError:
+            continue
+        found.append({"library": path, "exports_cusolverDnXstedc": hasattr(lib, "cusolverDnXstedc")})
+    exported = any(f["exports_cusolverDnXstedc"] for f in found)
+    return {"libraries": found, "available": exported,
+            "note": None if exported else "unavailable on this box: no cuSOLVER here exports "
+                                          "cusolverDnXstedc"}
+
+
+def ref_gpu_times(torch, R, D, E, W, steps, warmup, flush):
+    """Per-solve device times (ms) of the reference CUDA prototype on its own
+    stream, with the same L2 flush before every timed solve as ours."""
+    with torch.cuda.stream(R.stream):
+        for _ in range(warmup):
+            R.solve(D, E, W)
+        R.stream.synchronize()
+        times = []
+        for _ in range(steps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(R.stream)
+            R.solve(D, E, W)
+            e1.record(R.stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+    return times
+
+
+def bench_ref_gpu(torch, families, solver, flush, args, head_ms, fam_ms, paper):
+    """The reference CUDA prototype (the reference's gpu/src, compiled for
+    sm_100a from its own sources into oracle/_ref and called through its
+    solve entry tridiag_solver_run_from_device_tridiagonal,
+    gpu/src/tridiag_solver.cu:2541) timed on this GPU in this run, beside
+    this build, on the same inputs with the same L2 flush: the four families
+    at the headline order (the headline family with the headline's steps and
+    warm-up), the reference GPU bench's own data modes at the headline order
+    (this build timed beside it with its default launch shapes), and the
+    paper inputs at 8,192 whose times this line already carries.  A
+    comparison leg only: nothing of it is this build's timed work."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_gpu
+    from brdc import inputs
+
+    out = {"cusolver_xstedc": xstedc_probe()}
+    if not ref_gpu.available():
+        out["unavailable"] = "oracle/_ref not built: the reference tree was absent when building"
+        return out
+    R = ref_gpu.RefSolver()
+    try:
+        rows = {}
+        Wr = torch.empty(N_HEAD, dtype=torch.float64, device="cuda")
+
+        def row(spec, d, e, exact, steps, warmup, ours_ms):
+            Dt = torch.tensor(d, device="cuda")
+            Et = torch.tensor(e, device="cuda")
+            W1 = torch.empty(len(d), dtype=torch.float64, device="cuda") if len(d) != N_HEAD else Wr
+            tt = ref_gpu_times(torch, R, Dt, Et, W1, steps, warmup, flush)
+            ms = float(np.mean(tt))
+            err = input_error(d, e, np.sort(W1.cpu().numpy()), exact)
+            rows[spec] = {"ms": ms, "ms_median": float(np.median(tt)), "solves": steps,
+                          "workspace_bytes": ref_gpu.workspace_size(len(d)),
+                          "max_err_over_normT": err, "ours_ms": ours_ms,
+                          "speedup": ms / ours_ms if ours_ms else None}
+
+        for fam in ("uniform", "normal", "toeplitz", "clustered"):
+            d, e = families.generate(fam, N_HEAD)
+            exact = families.toeplitz_eigenvalues(N_HEAD) if fam == "toeplitz" else None
+            head = fam == FAMILY_HEAD
+            row(f"family-{fam}:{N_HEAD}", d, e, exact, args.steps if head else (3 if fam == "toeplitz" else 5),
+                args.warmup if head else 1, head_ms if head else fam_ms.get(fam))
+        # the reference GPU bench's data modes at the headline order; this
+        # build with its default launch shapes on the same inputs
+        saved = solver.tuning()
+        solver.set_tuning(**DEFAULT_TUNING)
+        ws = solver.workspace(N_HEAD)
+        for mode in inputs.GPU_BENCH_MODES:
+            if mode == "test":
+                continue  # the bench's small self-test mode
+            d, e, _, _, exact = load_workload(None, f"{mode}:{N_HEAD}")
+            Dt = torch.tensor(d, device="cuda")
+            Et = torch.tensor(e, device="cuda")
+            for _ in range(2):
+                solver.dstebr(Dt, Et, W=Wr, workspace=ws)
+            torch.cuda.synchronize()
+            ours = float(np.mean(time_solves(torch, solver, Dt, Et, Wr, ws, 5, flush)))
+            row(f"{mode}:{N_HEAD}", d, e, exact, 3, 1, ours)
+        solver.set_tuning(**saved)
+        # the paper inputs at the order bench_paper_inputs used
+        n = paper["n"]
+        for spec, rec in paper.items():
+            if spec == "n":
+                continue
+            d, e, _, _, exact = load_workload(None, f"{spec}:{n}")
+            row(f"{spec}:{n}", d, e, exact, 3, 1, rec["ms"])
+        out.update(rows[f"family-{FAMILY_HEAD}:{N_HEAD}"])
+        out["rows"] = rows
+    finally:
+        R.close()
+        solver._ws.clear()
+    return out
+
+
+def collect_extras(torch, brdc, families, solver, D, E, W, ws, d, e, flush, args, head_ms=None):
     out = {}
     headline_tuning = solver.tuning()
 
@@ -667,6 +790,8 @@ def collect_extras(torch, brdc, families, solver, D, E, W, ws, d, e, flush, args
     out["fwd_bwd"] = bench_fwd_bwd(torch, families, solver, flush, args)
     out["batched"] = bench_batched(torch, brdc, families, solver, flush)
     out["fit"] = bench_fit(torch, brdc, families, flush)
+    out["ref_gpu"] = bench_ref_gpu(torch, families, solver, flush, args, head_ms, fam_ms,
+                                   out["paper_inputs"])
 
     # CPU baseline: the oracle on a bounded sample of the same workload
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -1004,12 +1129,20 @@ DEFAULT_TUNING = {"subtree_levels": -1, "deflate_cluster": 16, "sweep_lanes_targ
 _FP64 = None
 
 
+def fp64_probe_lib() -> str:
+    """libbench_fp64.so beside this file (built from bench_fp64.cu when stale)."""
+    import build as brdc_build
+
+    return brdc_build.nvcc_shared(os.path.join(ROOT, "bench_fp64.cu"),
+                                  os.path.join(ROOT, "libbench_fp64.so"))
+
+
 def fp64_peak_gflops():
     global _FP64
     if _FP64 is None:
         import ctypes
 
-        lib = ctypes.CDLL(os.path.join(ROOT, "ppopp27-brdc-ae_b200", "brdc", "libbrdc_probe.so"))
+        lib = ctypes.CDLL(fp64_probe_lib())
         lib.brdc_probe_dfma_gflops.restype = ctypes.c_double
         lib.brdc_probe_dfma_gflops.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
         best = 0.0

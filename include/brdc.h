@@ -117,11 +117,18 @@ brdc_status brdc_dstebr(brdc_handle handle, int64_t n, const double *d_D,
  *    (other streams, other host threads) race and corrupt each other.
  *    Serialise them on one stream.  The array keeps the last call's data;
  *    every solve writes what it reads, so nothing needs clearing.
- *  - Status of the device side (brdc_get_info) is not available for this
- *    entry; use brdc_dstebr with a workspace when it is needed. */
+ *  - The device-side status of the last solve (unconverged roots, non-finite
+ *    input, a wait that ran out) is read by brdc_dstebr_noalloc_get_info. */
 brdc_status brdc_dstebr_noalloc(brdc_handle handle, int64_t n,
                                 const double *d_D, const double *d_E,
                                 double *d_W);
+
+/* brdc_get_info for the allocation-free entry: the status word that the
+ * last brdc_dstebr_noalloc solve on the handle's device left in the static
+ * scratch array (synchronises the handle's stream; same info and return
+ * values as brdc_get_info).  INVALID_VALUE when no such solve ran yet on
+ * that device.  No reference counterpart. */
+brdc_status brdc_dstebr_noalloc_get_info(brdc_handle handle, int *info);
 
 /* Adjoint of brdc_dstebr for the loss L = sum_i G[i] * W[i]: writes
  * dL/dD[n] and dL/dE[n-1] (device) without forming eigenvectors, by
@@ -138,8 +145,13 @@ brdc_status brdc_dstebr_backward(brdc_handle handle, int64_t n,
 
 /* Device status of the last solve on this workspace; synchronises the
  * stream.  *info = 0 on success, > 0 = number of secular roots that did
- * not converge, < 0 = internal device error code.  Returns
- * BRDC_STATUS_NOT_CONVERGED when *info > 0. */
+ * not converge (BRDC_STATUS_NOT_CONVERGED), < 0 = the solve stopped early
+ * (BRDC_STATUS_INTERNAL_ERROR, the code also recorded as the last error
+ * with source BRDC_ERROR_SRC_DEVICE):
+ *   -1  a wait for a tile copy into shared memory ran out (wait limit)
+ *   -3  a wait at a grid-wide barrier ran out (wait limit)
+ *   -4  D or E holds a NaN or an infinity: nothing was solved.
+ * After a negative info W (or dL/dD, dL/dE) holds no result. */
 brdc_status brdc_get_info(brdc_handle handle, const void *workspace,
                           int *info);
 
@@ -229,6 +241,29 @@ typedef struct brdc_tuning {
 brdc_status brdc_set_tuning(brdc_handle handle, const brdc_tuning *tuning);
 brdc_status brdc_get_tuning(brdc_handle handle, brdc_tuning *tuning);
 
+/* Failure limits of a handle's solves, stored in the workspace by each
+ * solve.  No reference counterpart: the reference caps the secular
+ * iteration at a compile-time 50 (gpu/src/tridiag_solver_secular.cuh:12)
+ * and its waits are host synchronisations.
+ *   secular_max_iter  iterations of one secular root before it stops and is
+ *                     counted as not converged (brdc_get_info > 0);
+ *                     1..1000, default 64
+ *   wait_limit_ns     bound of every device-side wait: the grid-wide
+ *                     barriers of the per-level sweep kernel and the waits
+ *                     for tile copies into shared memory.  A wait that runs
+ *                     out stops the solve (brdc_get_info < 0); a block whose
+ *                     tile wait ran out first waits up to 2 s more for its
+ *                     copies in flight.  0..1e12, default 2e10 (20 s).
+ * Out-of-range values -> BRDC_STATUS_INVALID_VALUE. */
+typedef struct brdc_limits {
+    int secular_max_iter;
+    int reserved;            /* 0 */
+    long long wait_limit_ns;
+} brdc_limits;
+
+brdc_status brdc_set_limits(brdc_handle handle, const brdc_limits *limits);
+brdc_status brdc_get_limits(brdc_handle handle, brdc_limits *limits);
+
 /* Autotuner: times the batched solve of this exact input (count = 1 is the
  * plain solve) under candidate tunings on the handle's stream -- coordinate
  * descent over subtree depth, deflation cluster and sweep lanes, median of
@@ -262,7 +297,16 @@ void brdc_dstedc_dc_br_(const int *n, double *d, double *e, double *work,
  * (the E slot at offsets[b+1]-1 is ignored), W likewise.  offsets is a host
  * array of count+1 int64 values (offsets[0] = 0).  All levels of all
  * instances run in one pass of kernels per level.  No reference
- * counterpart (the reference solves one matrix per call). */
+ * counterpart (the reference solves one matrix per call).
+ * Per-instance tables: a batched call made outside a stream capture copies
+ * small per-instance tables (offsets, levels, prefixes) into the workspace
+ * ahead of its kernels, so the workspace may be used for anything between
+ * calls.  A call made while the stream is being captured copies nothing
+ * (the graph holds kernels only): it needs the previous non-captured
+ * batched call (or backward) on this handle to have used the same
+ * workspace, offsets and checkpoint size, otherwise it returns
+ * BRDC_STATUS_INVALID_VALUE; and the workspace then belongs to the graph
+ * until the graph's last replay. */
 brdc_status brdc_dstebr_batched_workspace_size(int64_t count,
                                                const int64_t *offsets,
                                                size_t *bytes);

@@ -2,8 +2,10 @@
 # Compile the reference CUDA prototype (values-only BR solver) from its own
 # sources, without its CMake build, for sm_100a, into oracle/_ref/.  Test
 # and benchmark infrastructure only (a checker and a timed comparison); the
-# product never links it.  Needs the reference tree (REF, default
-# /root/reference); the built library travels with the repository.
+# product never links it.  Reads the reference tree (REF, by default its
+# mount point in the build container); where the tree is absent the script
+# exits with status 1 and builds nothing.  The built library travels with
+# the repository.
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
 REF="${REF:-/root/reference}"

@@ -70,6 +70,9 @@ EXPORTS = (
     "brdc_autotune",
     "brdc_dstebr_vectors_workspace_size",
     "brdc_dstebr_vectors",
+    "brdc_set_limits",
+    "brdc_get_limits",
+    "brdc_dstebr_noalloc_get_info",
 )
 
 
@@ -127,6 +130,17 @@ class Tuning(ctypes.Structure):
 
     def as_dict(self) -> dict:
         return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class Limits(ctypes.Structure):
+    _fields_ = [
+        ("secular_max_iter", ctypes.c_int),
+        ("reserved", ctypes.c_int),
+        ("wait_limit_ns", ctypes.c_longlong),
+    ]
+
+    def as_dict(self) -> dict:
+        return {"secular_max_iter": self.secular_max_iter, "wait_limit_ns": self.wait_limit_ns}
 
 
 class Timings(ctypes.Structure):
@@ -198,13 +212,17 @@ def load() -> ctypes.CDLL:
     lib.brdc_get_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
     lib.brdc_autotune.argtypes = [vp, i64, ctypes.POINTER(i64), vp, vp, vp, vp, sz,
                                   ctypes.POINTER(Tuning)]
+    lib.brdc_set_limits.argtypes = [vp, ctypes.POINTER(Limits)]
+    lib.brdc_dstebr_noalloc_get_info.argtypes = [vp, ip]
+    lib.brdc_get_limits.argtypes = [vp, ctypes.POINTER(Limits)]
     for f in ("brdc_create", "brdc_destroy", "brdc_set_stream", "brdc_get_stream",
               "brdc_get_last_error", "brdc_dstebr_workspace_size", "brdc_dstebr",
               "brdc_dstebr_backward", "brdc_get_info", "brdc_get_diagnostics",
               "brdc_dstebr_batched_workspace_size", "brdc_dstebr_batched",
               "brdc_set_timing", "brdc_get_last_timings", "brdc_dstebr_noalloc",
               "brdc_dstebr_batched_checkpoint_workspace_size", "brdc_dstebr_batched_backward",
-              "brdc_set_tuning", "brdc_get_tuning", "brdc_autotune"):
+              "brdc_set_tuning", "brdc_get_tuning", "brdc_autotune",
+              "brdc_set_limits", "brdc_get_limits", "brdc_dstebr_noalloc_get_info"):
         getattr(lib, f).restype = ctypes.c_int
     _lib = lib
     return lib
@@ -288,6 +306,26 @@ class Solver:
         cur.update(kw)
         t = Tuning(**cur)
         _check(load().brdc_set_tuning(self.h, ctypes.byref(t)), "set_tuning", self.h)
+
+    def limits(self) -> dict:
+        lim = Limits()
+        _check(load().brdc_get_limits(self.h, ctypes.byref(lim)), "get_limits", self.h)
+        return lim.as_dict()
+
+    def set_limits(self, **kw) -> None:
+        """Change failure limits (secular_max_iter, wait_limit_ns); the
+        others keep their values."""
+        cur = self.limits()
+        cur.update(kw)
+        lim = Limits(secular_max_iter=int(cur["secular_max_iter"]), reserved=0,
+                     wait_limit_ns=int(cur["wait_limit_ns"]))
+        _check(load().brdc_set_limits(self.h, ctypes.byref(lim)), "set_limits", self.h)
+
+    def last_error(self):
+        """(code, source, site) of the handle's last recorded error."""
+        code, src, site = ctypes.c_int(), ctypes.c_int(), ctypes.c_char_p()
+        load().brdc_get_last_error(self.h, ctypes.byref(code), ctypes.byref(src), ctypes.byref(site))
+        return code.value, src.value, (site.value.decode() if site.value else None)
 
     def autotune(self, D, E, offsets=None, workspace=None) -> dict:
         """Time this input (one matrix, or a packed batch with offsets) under
@@ -373,8 +411,15 @@ class Solver:
         return W, Zt.t()
 
     def checkpoint_workspace(self, n: int):
-        """Workspace that also records the per-level state the adjoint reads."""
+        """Workspace that also records the per-level state the adjoint reads
+        (cached per order on this solver: the next solve of order n on it
+        overwrites the checkpoints)."""
         return self.workspace(n, FLAG_KEEP_CHECKPOINTS)
+
+    def new_checkpoint_workspace(self, n: int):
+        """A fresh, uncached checkpointing workspace for one solve of order n."""
+        nbytes = workspace_size(n, FLAG_KEEP_CHECKPOINTS)
+        return self._torch.empty(nbytes, dtype=self._torch.uint8, device="cuda")
 
     def dstebr_backward(self, D, E, G, workspace=None, keep_forward: bool = False,
                         gD=None, gE=None):
@@ -414,13 +459,27 @@ class Solver:
         _check(st, "brdc_dstebr_noalloc", self.h)
         return W
 
+    def noalloc_info_status(self):
+        """(info, status) of the last allocation-free solve on this device."""
+        out = ctypes.c_int()
+        st = load().brdc_dstebr_noalloc_get_info(self.h, ctypes.byref(out))
+        if st not in (SUCCESS, NOT_CONVERGED, INTERNAL_ERROR):
+            _check(st, "brdc_dstebr_noalloc_get_info", self.h)
+        return int(out.value), int(st)
+
     def info(self, n: int, workspace=None) -> int:
+        """Device status of the last solve on the workspace: 0, the number of
+        unconverged roots (> 0), or a negative device error code."""
+        return self.info_status(n, workspace)[0]
+
+    def info_status(self, n: int, workspace=None):
+        """(info, status) of brdc_get_info for the workspace."""
         ws = self.workspace(n) if workspace is None else workspace
         out = ctypes.c_int()
         st = load().brdc_get_info(self.h, ctypes.c_void_p(ws.data_ptr()), ctypes.byref(out))
-        if st not in (SUCCESS, NOT_CONVERGED):
+        if st not in (SUCCESS, NOT_CONVERGED, INTERNAL_ERROR):
             _check(st, "brdc_get_info", self.h)
-        return int(out.value)
+        return int(out.value), int(st)
 
     def diagnostics(self, n: int, workspace=None) -> dict:
         ws = self.workspace(n) if workspace is None else workspace

@@ -16,9 +16,13 @@ class TridiagEigvals(torch.autograd.Function):
     @staticmethod
     def forward(ctx, D, E, solver: Solver):
         n = D.shape[0]
-        ws = solver.checkpoint_workspace(n)
+        # A workspace of its own for every forward: the backward reads this
+        # forward's checkpoints, which a later forward of the same order
+        # (a second matrix in the same loss) would otherwise overwrite.
+        ws = solver.new_checkpoint_workspace(n)
         W = solver.dstebr(D, E, workspace=ws)
         ctx.solver = solver
+        ctx.ws = ws
         ctx.save_for_backward(D, E)
         return W
 
@@ -26,8 +30,9 @@ class TridiagEigvals(torch.autograd.Function):
     def backward(ctx, G):
         D, E = ctx.saved_tensors
         solver = ctx.solver
-        ws = solver.checkpoint_workspace(D.shape[0])
-        gD, gE = solver.dstebr_backward(D, E, G.contiguous(), workspace=ws, keep_forward=True)
+        gD, gE = solver.dstebr_backward(D, E, G.contiguous(), workspace=ctx.ws,
+                                        keep_forward=True)
+        ctx.ws = None
         return gD, gE, None
 
 

@@ -19,7 +19,6 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "brdc")
 LIB = os.path.join(OUT, "libbrdc_b200.so")
 HOSTLIB = os.path.join(OUT, "libbrdc_hostcheck.so")
-PROBELIB = os.path.join(OUT, "libbrdc_probe.so")
 INPUTLIB = os.path.join(OUT, "libbrdc_inputs.so")
 
 NVCC_FLAGS = [
@@ -49,15 +48,12 @@ def _stale(target: str, deps) -> bool:
 
 def build(force: bool = False, verbose: bool = False) -> str:
     deps = _sources() + [os.path.join(HERE, "..", "include", h) for h in ("brdc.h", "brdc_lapack.h")] + [__file__]
-    deps = [d for d in deps if not d.endswith(("probe_fp64.cu", "host_check.cpp", "brdc_inputs.cpp"))]
+    deps = [d for d in deps if not d.endswith(("host_check.cpp", "brdc_inputs.cpp"))]
     if force or _stale(LIB, deps):
         cmd = [_nvcc(), *NVCC_FLAGS, "-o", LIB, os.path.join(CSRC, "brdc_capi.cu"), "-lcublas"]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
         subprocess.run(cmd, check=True)
-    pdeps = [os.path.join(CSRC, "probe_fp64.cu"), os.path.join(CSRC, "brdc_secular.cuh")]
-    if force or _stale(PROBELIB, pdeps):
-        subprocess.run([_nvcc(), *NVCC_FLAGS, "-o", PROBELIB, pdeps[0]], check=True)
     cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
     hdeps = [os.path.join(CSRC, "host_check.cpp"), os.path.join(CSRC, "brdc_secular.cuh")]
     if force or _stale(HOSTLIB, hdeps):
@@ -73,6 +69,15 @@ def build(force: bool = False, verbose: bool = False) -> str:
             check=True,
         )
     return LIB
+
+
+def nvcc_shared(src: str, out: str, deps=(), includes=(), force: bool = False) -> str:
+    """Compile one stand-alone .cu file into a shared library for sm_100a
+    (the bench's FP64 probe and test helpers use it), when out is stale."""
+    if force or _stale(out, [src, *deps]):
+        cmd = [_nvcc(), *NVCC_FLAGS, *[f"-I{d}" for d in includes], "-o", out, src]
+        subprocess.run(cmd, check=True)
+    return out
 
 
 if __name__ == "__main__":

@@ -53,6 +53,9 @@ __device__ inline double sgn(double x) { return (double)((x > 0.0) - (x < 0.0));
 // node's ascending order.  Instance roots read dL/dW and have no row
 // cotangents.
 __global__ void __launch_bounds__(256) k_bw_unplace(BArgs a, long long total_n) {
+    if (halted(a.w.hdr)) {
+        return;
+    }
     const Ws &w = a.w;
     for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x; x < total_n;
          x += (long long)gridDim.x * blockDim.x) {
@@ -154,6 +157,9 @@ __device__ inline bool warp_item(const Ws &w, const LevelCtl *ctl, int wi, WarpI
 // the origin's dd and dz terms for the pole kernel and its drho term, which
 // k_bw_undeflate sums in a fixed order.
 __global__ void __launch_bounds__(kSweepThreads) k_bw_roots(BArgs a) {
+    if (halted(a.w.hdr)) {
+        return;
+    }
     const Ws &w = a.w;
     const LevelCtl *ctl = &w.hdr->lvl[a.k];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -247,6 +253,9 @@ __global__ void __launch_bounds__(kSweepThreads) k_bw_roots(BArgs a) {
 // the (at most two) roots j in {i-1, i} with origin i add their stored
 // origin terms instead.
 __global__ void __launch_bounds__(kSweepThreads) k_bw_poles(BArgs a) {
+    if (halted(a.w.hdr)) {
+        return;
+    }
     const Ws &w = a.w;
     const LevelCtl *ctl = &w.hdr->lvl[a.k];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -363,6 +372,9 @@ __global__ void __launch_bounds__(kSweepThreads) k_bw_poles(BArgs a) {
 // average); the lanes stride over the roots and combine by shuffles.  Every warp runs the same number of trips,
 // so the shuffles stay convergent.
 __global__ void __launch_bounds__(256) k_bw_defl(BArgs a, long long total_n) {
+    if (halted(a.w.hdr)) {
+        return;
+    }
     const Ws &w = a.w;
     const LevelCtl *ctl = &w.hdr->lvl[a.k];
     const long long ndefl = a.level_rows - ctl->total_k;
@@ -500,6 +512,9 @@ __device__ inline bool bw_reverse_chain(const Ws &w, long long gs, int b0, int K
 // sqrt 2), and dL/dE at the cut.
 template <int T>
 __global__ void __launch_bounds__(T) k_bw_undeflate(BArgs a) {
+    if (halted(a.w.hdr)) {
+        return;
+    }
     __shared__ int iscan[32];
     __shared__ double red[32];
     const int g = blockIdx.x;
@@ -597,6 +612,9 @@ __global__ void __launch_bounds__(T) k_bw_undeflate(BArgs a) {
 
 // poles and rotated-out members -> active positions
 __global__ void __launch_bounds__(256) k_bw_ud_active(BArgs a, long long total_n) {
+    if (halted(a.w.hdr)) {
+        return;
+    }
     const Ws &w = a.w;
     for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x; x < total_n;
          x += (long long)gridDim.x * blockDim.x) {
@@ -629,6 +647,9 @@ __global__ void __launch_bounds__(256) k_bw_ud_active(BArgs a, long long total_n
 
 // Givens chains, one thread per active index (chain bases do the work)
 __global__ void __launch_bounds__(256) k_bw_ud_chains(BArgs a, long long total_n) {
+    if (halted(a.w.hdr)) {
+        return;
+    }
     const Ws &w = a.w;
     for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x; x < total_n;
          x += (long long)gridDim.x * blockDim.x) {
@@ -647,6 +668,9 @@ __global__ void __launch_bounds__(256) k_bw_ud_chains(BArgs a, long long total_n
 
 // active and small-z lists -> merged positions
 __global__ void __launch_bounds__(256) k_bw_ud_merged(BArgs a, long long total_n) {
+    if (halted(a.w.hdr)) {
+        return;
+    }
     const Ws &w = a.w;
     for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x; x < total_n;
          x += (long long)gridDim.x * blockDim.x) {
@@ -677,6 +701,9 @@ __global__ void __launch_bounds__(256) k_bw_ud_merged(BArgs a, long long total_n
 // merged positions -> children (z = last row of the left child / first row
 // of the right child, over sqrt 2)
 __global__ void __launch_bounds__(256) k_bw_ud_children(BArgs a, long long total_n) {
+    if (halted(a.w.hdr)) {
+        return;
+    }
     const Ws &w = a.w;
     const double isq2 = 0.70710678118654752440;
     for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x; x < total_n;
@@ -704,6 +731,9 @@ __global__ void __launch_bounds__(256) k_bw_ud_children(BArgs a, long long total
 // dL/drho of every merge summed over its roots by one warp, in a fixed
 // order, and dL/dE at its cut
 __global__ void __launch_bounds__(256) k_bw_ud_rho(BArgs a) {
+    if (halted(a.w.hdr)) {
+        return;
+    }
     const Ws &w = a.w;
     const int lane = threadIdx.x & 31;
     const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
@@ -732,6 +762,9 @@ __global__ void __launch_bounds__(256) k_bw_ud_rho(BArgs a) {
 // of the cuts.
 __global__ void __launch_bounds__(kLeafWarps * 32)
     k_bw_leaf(BArgs a, long long total_leaves) {
+    if (halted(a.w.hdr)) {
+        return;
+    }
     __shared__ double sV[kLeafWarps * 2][16][17];
     __shared__ double sC[kLeafWarps * 2][16][17];
     __shared__ double sLam[kLeafWarps * 2][16], sV0[kLeafWarps * 2][16], sV1[kLeafWarps * 2][16];
@@ -845,6 +878,9 @@ __global__ void __launch_bounds__(kLeafWarps * 32)
 // 2 sign(E_c) dL/drho stored by k_bw_undeflate.  One thread per leaf (the
 // leaf left of the cut), so the sum has a fixed order.
 __global__ void __launch_bounds__(256) k_bw_cuts(BArgs a, long long total_leaves) {
+    if (halted(a.w.hdr)) {
+        return;
+    }
     for (long long leaf = (long long)blockIdx.x * blockDim.x + threadIdx.x; leaf < total_leaves;
          leaf += (long long)gridDim.x * blockDim.x) {
         const LeafGeom LG = leaf_geom(a.F, leaf);

@@ -35,16 +35,24 @@ struct brdc_handle_struct {
     const char *last_site;
     int sm_count;
     int device;
-    // batched: signature of the forest whose tables sit in a workspace
+    // batched: signature of the forest whose tables the last non-captured
+    // batched call wrote into a workspace, the host copy of those tables
+    // (alive until their copy has run, prep_ev) and the event itself
     const void *prep_ws;
     bool prep_ckpt = false;
     int prep_sub = -1;
+    std::vector<int> prep_tab;
+    cudaEvent_t prep_ev = nullptr;
+    bool prep_pending = false;
     // merge levels solved inside the subtree kernel (0: leaves alone,
     // -1: chosen per solve from the tree height)
     int sub_levels = -1;
     int defl_cluster = 16;        // largest deflation cluster (8 for k_merge_deflate_cl)
     int lanes_target = 303104;    // root-sweep parallelism target
     int lvl_rows = 1 << 30;       // largest merge of a level run by k_level (0: none)
+    // failure limits (brdc_set_limits): secular iteration cap, device wait bound
+    int max_iter = kSecularMaxIter;
+    unsigned long long wait_ns = kDefaultWaitNs;
     std::vector<long long> prep_off;
     // phase timing (off by default)
     int timing;
@@ -613,14 +621,15 @@ brdc_status run_forest(brdc_handle h, const HostForest &hf, const Layout &L,
     h->launches = 0;
     h->timed_levels = hf.max_levels;
     mark(h, 0);
-    k_init<<<1, 64, 0, s>>>(w.hdr, hf.max_levels, hf.B, hf.total_n, hf.leaves, 0, w.f_norm);
+    k_init<<<1, 64, 0, s>>>(w.hdr, hf.max_levels, hf.B, hf.total_n, hf.leaves, 0, w.f_norm,
+                            h->max_iter, h->wait_ns);
     BRDC_CUDA(h, "brdc.init", cudaGetLastError());
     {
         long long ng = hf.B > 1 ? (hf.B + 7) / 8 : (hf.total_n + 255) / 256;
         ng = std::max<long long>(1, std::min<long long>(ng, (long long)h->sm_count * 4));
         cudaLaunchAttribute at[1];
         cudaLaunchConfig_t cfg = plain_config((unsigned)ng, 256, 0, s, at);
-        cudaLaunchKernelEx(&cfg, k_norm, F, D, E, w.f_norm);
+        cudaLaunchKernelEx(&cfg, k_norm, F, D, E, w.f_norm, w.hdr);
         BRDC_CUDA(h, "brdc.norm", cudaGetLastError());
     }
     h->launches += 2;
@@ -809,6 +818,9 @@ extern "C" brdc_status brdc_destroy(brdc_handle h) {
     if (h->blas != nullptr) {
         cublasDestroy(h->blas);
     }
+    if (h->prep_ev != nullptr) {
+        cudaEventDestroy(h->prep_ev);
+    }
     if (h->own_stream != nullptr) {
         cudaStreamDestroy(h->own_stream);
     }
@@ -833,6 +845,35 @@ extern "C" brdc_status brdc_set_tuning(brdc_handle h, const brdc_tuning *t) {
     h->defl_cluster = c;
     h->lanes_target = t->sweep_lanes_target;
     h->lvl_rows = t->fused_level_rows;
+    return BRDC_STATUS_SUCCESS;
+}
+
+extern "C" brdc_status brdc_set_limits(brdc_handle h, const brdc_limits *l) {
+    if (h == nullptr) {
+        return BRDC_STATUS_INVALID_HANDLE;
+    }
+    if (l == nullptr) {
+        return BRDC_STATUS_INVALID_POINTER;
+    }
+    if (l->secular_max_iter < 1 || l->secular_max_iter > 1000 || l->wait_limit_ns < 0 ||
+        l->wait_limit_ns > 1000000000000LL) {
+        return BRDC_STATUS_INVALID_VALUE;
+    }
+    h->max_iter = l->secular_max_iter;
+    h->wait_ns = (unsigned long long)l->wait_limit_ns;
+    return BRDC_STATUS_SUCCESS;
+}
+
+extern "C" brdc_status brdc_get_limits(brdc_handle h, brdc_limits *l) {
+    if (h == nullptr) {
+        return BRDC_STATUS_INVALID_HANDLE;
+    }
+    if (l == nullptr) {
+        return BRDC_STATUS_INVALID_POINTER;
+    }
+    l->secular_max_iter = h->max_iter;
+    l->reserved = 0;
+    l->wait_limit_ns = (long long)h->wait_ns;
     return BRDC_STATUS_SUCCESS;
 }
 
@@ -954,6 +995,10 @@ extern "C" brdc_status brdc_dstebr(brdc_handle h, int64_t n, const double *d_D,
     return run_forest(h, hf, L, F, w, d_D, d_E, d_W);
 }
 
+namespace {
+cudaError_t noalloc_cached_address(int device, void **out);
+}
+
 extern "C" brdc_status brdc_get_info(brdc_handle h, const void *workspace,
                                      int *info) {
     if (h == nullptr) {
@@ -1067,9 +1112,14 @@ extern "C" brdc_status brdc_get_last_timings(brdc_handle h, brdc_timings *out) {
 namespace {
 
 // Forest descriptor of a batch.  With more than one instance the
-// per-instance tables live in the workspace; they are uploaded once per
-// (workspace, layout, offsets), so later calls with the same triple only
-// enqueue kernels and can be captured in a CUDA graph.
+// per-instance tables (row offsets, levels, node, leaf and subtree
+// prefixes) live in the workspace.  Every call outside a stream capture
+// writes them, because anything may have reused the workspace since the
+// last batched call (a single solve carves the same bytes differently, and
+// a caching allocator hands addresses back).  A captured call writes none,
+// so the graph replays only kernels: it needs the last non-captured batched
+// call of this handle to have written the tables for the same workspace,
+// offsets and layout, and the workspace to stay reserved for the graph.
 brdc_status prepare_forest(brdc_handle h, const HostForest &hf, const Ws &w,
                            const void *workspace, bool ckpt, Forest *F) {
     *F = Forest{};
@@ -1080,49 +1130,73 @@ brdc_status prepare_forest(brdc_handle h, const HostForest &hf, const Ws &w,
         F->L0 = hf.max_levels;
         return BRDC_STATUS_SUCCESS;
     }
-    const bool same = h->prep_ws == workspace && h->prep_ckpt == ckpt &&
-                      h->prep_sub == effective_sub_levels(h, hf) &&
-                      h->prep_off.size() == (size_t)hf.B + 1 &&
-                      std::equal(h->prep_off.begin(), h->prep_off.end(), hf.off.begin());
-    if (!same) {
-        std::vector<int> node_prefix((size_t)(hf.B + 1) * std::max(hf.max_levels, 1), 0);
+    const int sub = effective_sub_levels(h, hf);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    BRDC_CUDA(h, "brdc.batched.capture_status", cudaStreamIsCapturing(h->stream, &cap));
+    if (cap != cudaStreamCaptureStatusNone) {
+        const bool same = h->prep_ws == workspace && h->prep_ckpt == ckpt &&
+                          h->prep_sub == sub && h->prep_off.size() == (size_t)hf.B + 1 &&
+                          std::equal(h->prep_off.begin(), h->prep_off.end(), hf.off.begin());
+        if (!same) {
+            set_error(h, 0, BRDC_ERROR_SRC_NONE,
+                      "brdc.batched: a captured call needs a non-captured call with the "
+                      "same workspace and offsets first");
+            return BRDC_STATUS_INVALID_VALUE;
+        }
+    } else {
+        // the host tables of the previous upload stay alive until its copies ran
+        if (h->prep_ev == nullptr) {
+            BRDC_CUDA(h, "brdc.batched.event_create",
+                      cudaEventCreateWithFlags(&h->prep_ev, cudaEventDisableTiming));
+        }
+        if (h->prep_pending) {
+            BRDC_CUDA(h, "brdc.batched.event_wait", cudaEventSynchronize(h->prep_ev));
+            h->prep_pending = false;
+        }
+        const size_t B1 = (size_t)hf.B + 1;
+        const size_t Lm = (size_t)std::max(hf.max_levels, 1);
+        // [lev (B) | node prefixes (B+1 per level) | leaf prefix (B+1) | subtree prefix (B+1)]
+        std::vector<int> &tab = h->prep_tab;
+        tab.assign((size_t)hf.B + B1 * Lm + 2 * B1, 0);
+        int *lev = tab.data();
+        int *node_prefix = lev + hf.B;
+        int *leaf_prefix = node_prefix + B1 * Lm;
+        int *sub_prefix = leaf_prefix + B1;
+        for (int b = 0; b < hf.B; ++b) {
+            lev[b] = hf.lev[b];
+        }
         for (int k = 0; k < hf.max_levels; ++k) {
-            int *row = node_prefix.data() + (size_t)k * (hf.B + 1);
-            row[0] = 0;
+            int *row = node_prefix + (size_t)k * B1;
             for (int b = 0; b < hf.B; ++b) {
                 const int L = hf.lev[b];
                 row[b + 1] = row[b] + (L > k ? (1 << (L - 1 - k)) : 0);
             }
         }
-        std::vector<int> leaf_prefix(hf.B + 1, 0);
-        std::vector<int> sub_prefix(hf.B + 1, 0);
         for (int b = 0; b < hf.B; ++b) {
             leaf_prefix[b + 1] = leaf_prefix[b] + (1 << hf.lev[b]);
-            sub_prefix[b + 1] = sub_prefix[b] + (int)subtrees_of(hf.lev[b], effective_sub_levels(h, hf));
+            sub_prefix[b + 1] = sub_prefix[b] + (int)subtrees_of(hf.lev[b], sub);
         }
+        h->prep_off = hf.off;
         BRDC_CUDA(h, "brdc.batched.upload_off",
-                  cudaMemcpyAsync(w.f_off, hf.off.data(), sizeof(long long) * (hf.B + 1),
+                  cudaMemcpyAsync(w.f_off, h->prep_off.data(), sizeof(long long) * B1,
                                   cudaMemcpyHostToDevice, h->stream));
         BRDC_CUDA(h, "brdc.batched.upload_lev",
-                  cudaMemcpyAsync(w.f_lev, hf.lev.data(), sizeof(int) * hf.B,
-                                  cudaMemcpyHostToDevice, h->stream));
+                  cudaMemcpyAsync(w.f_lev, lev, sizeof(int) * hf.B, cudaMemcpyHostToDevice,
+                                  h->stream));
         BRDC_CUDA(h, "brdc.batched.upload_nodes",
-                  cudaMemcpyAsync(w.f_node_prefix, node_prefix.data(),
-                                  sizeof(int) * node_prefix.size(), cudaMemcpyHostToDevice,
-                                  h->stream));
+                  cudaMemcpyAsync(w.f_node_prefix, node_prefix, sizeof(int) * B1 * Lm,
+                                  cudaMemcpyHostToDevice, h->stream));
         BRDC_CUDA(h, "brdc.batched.upload_leaves",
-                  cudaMemcpyAsync(w.f_leaf_prefix, leaf_prefix.data(),
-                                  sizeof(int) * leaf_prefix.size(), cudaMemcpyHostToDevice,
-                                  h->stream));
+                  cudaMemcpyAsync(w.f_leaf_prefix, leaf_prefix, sizeof(int) * B1,
+                                  cudaMemcpyHostToDevice, h->stream));
         BRDC_CUDA(h, "brdc.batched.upload_subtrees",
-                  cudaMemcpyAsync(w.f_sub_prefix, sub_prefix.data(),
-                                  sizeof(int) * sub_prefix.size(), cudaMemcpyHostToDevice,
-                                  h->stream));
-        BRDC_CUDA(h, "brdc.batched.upload_sync", cudaStreamSynchronize(h->stream));
+                  cudaMemcpyAsync(w.f_sub_prefix, sub_prefix, sizeof(int) * B1,
+                                  cudaMemcpyHostToDevice, h->stream));
+        BRDC_CUDA(h, "brdc.batched.upload_record", cudaEventRecord(h->prep_ev, h->stream));
+        h->prep_pending = true;
         h->prep_ws = workspace;
         h->prep_ckpt = ckpt;
-        h->prep_sub = effective_sub_levels(h, hf);
-        h->prep_off = hf.off;
+        h->prep_sub = sub;
     }
     F->off = w.f_off;
     F->lev = w.f_lev;
@@ -1869,6 +1943,11 @@ extern "C" brdc_status brdc_dstebr_vectors(brdc_handle h, int64_t n, const doubl
         BRDC_CUDA(h, "brdc.vectors.kmax_read",
                   cudaMemcpyAsync(kmax.data(), dkmax, sizeof(int) * Lv, cudaMemcpyDeviceToHost, s));
         BRDC_CUDA(h, "brdc.vectors.kmax_sync", cudaStreamSynchronize(s));
+        // a failed values solve (its status word set) leaves the counts
+        // unwritten: keep the products inside their buffers whatever was read
+        for (int k = 0; k < Lv; ++k) {
+            kmax[k] = std::min(std::max(kmax[k], 0), (int)hf.level_mmax[k]);
+        }
     }
     const double one = 1.0, zero = 0.0;
     double *qprev = nullptr, *qcur = qa;
@@ -2014,7 +2093,32 @@ cudaError_t noalloc_address(int device, void **out) {
     *out = g_noalloc_addr[device];
     return cudaSuccess;
 }
+
+// The address looked up by an earlier brdc_dstebr_noalloc call on `device`
+// (nullptr when there was none).
+cudaError_t noalloc_cached_address(int device, void **out) {
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    *out = (device >= 0 && device < kNoAllocMaxDevices) ? g_noalloc_addr[device] : nullptr;
+    return cudaSuccess;
+}
 } // namespace
+
+extern "C" brdc_status brdc_dstebr_noalloc_get_info(brdc_handle h, int *info) {
+    if (h == nullptr) {
+        return BRDC_STATUS_INVALID_HANDLE;
+    }
+    if (info == nullptr) {
+        return BRDC_STATUS_INVALID_POINTER;
+    }
+    void *scratch = nullptr;
+    noalloc_cached_address(h->device, &scratch);
+    if (scratch == nullptr) {
+        set_error(h, 0, BRDC_ERROR_SRC_NONE,
+                  "brdc.noalloc: no allocation-free solve on this device yet");
+        return BRDC_STATUS_INVALID_VALUE;
+    }
+    return brdc_get_info(h, scratch, info);
+}
 
 extern "C" brdc_status brdc_dstebr_noalloc(brdc_handle h, int64_t n,
                                            const double *d_D, const double *d_E,

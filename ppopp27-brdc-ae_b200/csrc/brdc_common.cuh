@@ -97,7 +97,8 @@ struct WsHeader {
     int nonconv;     // roots that hit the iteration cap
     int leaf_sweeps_max;
     int leaf_count;
-    int pad[2];
+    int max_iter;    // iteration cap of one secular root (the handle's limit)
+    unsigned long long wait_ns; // bound of every device-side wait, in ns
     LevelCtl lvl[BRDC_MAX_LEVELS];
     brdc_level_diagnostics diag[BRDC_MAX_LEVELS];
 };
@@ -105,10 +106,22 @@ struct WsHeader {
 // Device error codes written to WsHeader::status.
 enum DeviceError : int {
     kErrNone = 0,
-    kErrBarrierTimeout = 1,
+    kErrBarrierTimeout = 1,     // a tile copy's mbarrier wait ran out
     kErrBadGeometry = 2,
-    kErrGridBarrierTimeout = 3,
+    kErrGridBarrierTimeout = 3, // a grid-wide barrier wait ran out
+    kErrNonFinite = 4,          // D or E holds a NaN or an infinity
 };
+
+// A solve whose status word is set (non-finite input, a wait that ran out)
+// does no further work: every kernel after the one that set it returns at
+// once.  Only k_norm and k_sweeps set the word, and every later kernel
+// waits for them to finish before it reads it, so all CTAs of a kernel read
+// the same value (no cluster or grid barrier can lose a member to it).
+#if defined(__CUDACC__)
+__device__ __forceinline__ bool halted(const WsHeader *h) {
+    return *(const volatile int *)&h->status != 0;
+}
+#endif
 
 // Forest description passed by value to every kernel.
 struct Forest {
@@ -518,10 +531,23 @@ __device__ inline int upper_bound_d(const T *a, int n, T x) {
 
 // -------------------------------------------- TMA bulk copies + mbarriers
 // One-dimensional cp.async.bulk global -> shared with transaction-count
-// completion on an mbarrier.  Every wait is bounded: on timeout the kernel
-// records kErrBarrierTimeout and the caller abandons the work item.
+// completion on an mbarrier.  Every wait is bounded in time (the handle's
+// wait limit, from the workspace header): on timeout the kernel records
+// kErrBarrierTimeout, waits (bounded again) for the copies it still has in
+// flight, and the caller abandons the work item.
 
-constexpr unsigned kMbarSpinLimit = 1u << 26;
+// Default bound of every device-side wait (tile copies, grid barriers):
+// far above any legitimate wait (the longest grid-barrier wait of a level,
+// the slowest block's share of its secular phase, is milliseconds).
+constexpr unsigned long long kDefaultWaitNs = 20ull * 1000ull * 1000ull * 1000ull;
+// Bound of the wait for copies still in flight after a timeout.
+constexpr unsigned long long kDrainWaitNs = 2ull * 1000ull * 1000ull * 1000ull;
+
+__device__ inline unsigned long long globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 
 __device__ inline unsigned smem_u32(const void *p) {
     return (unsigned)__cvta_generic_to_shared(p);
@@ -558,10 +584,12 @@ __device__ inline void bulk_g2s(void *dst, const void *src, unsigned bytes,
         : "memory");
 }
 
-// Returns true when the phase completed, false on timeout.
-__device__ inline bool mbar_wait(uint64_t *bar, unsigned phase) {
+// Returns true when the phase completed, false when it had not after
+// limit_ns (measured on %globaltimer).
+__device__ inline bool mbar_wait(uint64_t *bar, unsigned phase, unsigned long long limit_ns) {
     const unsigned a = smem_u32(bar);
-    for (unsigned it = 0; it < kMbarSpinLimit; ++it) {
+    const unsigned long long t0 = globaltimer_ns();
+    for (;;) {
         unsigned done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -573,8 +601,10 @@ __device__ inline bool mbar_wait(uint64_t *bar, unsigned phase) {
         if (done) {
             return true;
         }
+        if (globaltimer_ns() - t0 > limit_ns) {
+            return false;
+        }
     }
-    return false;
 }
 
 #endif // __CUDACC__

@@ -418,6 +418,9 @@ __device__ inline int leaf_solve_full(const KArgs &a, const LeafGeom &G, int s, 
 __global__ void __launch_bounds__(kLeafWarps * 32)
     k_leaf_full(KArgs a, long long total_leaves) {
     pdl_begin();
+    if (halted(a.w.hdr)) {
+        return;
+    }
     const int lane = threadIdx.x & 31;
     const int x = lane & 15;
     const int half = lane >> 4;
@@ -462,6 +465,9 @@ __global__ void __launch_bounds__(kLeafWarps * 32)
 __global__ void __launch_bounds__(kLeafWarps * 32)
     k_leaf(KArgs a, long long total_leaves) {
     pdl_begin();
+    if (halted(a.w.hdr)) {
+        return;
+    }
     const int lane = threadIdx.x & 31;
     const int x = lane & 15;
     const int half = lane >> 4;
@@ -517,6 +523,9 @@ __global__ void __launch_bounds__(kLeafWarps * 32)
 // and last rows.
 __global__ void __launch_bounds__(256) k_merge(KArgs a, long long total_n) {
     pdl_begin();
+    if (halted(a.w.hdr)) {
+        return;
+    }
     const Ws &w = a.w;
     const double isq2 = 0.70710678118654752440;
     for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x; x < total_n;
@@ -684,6 +693,9 @@ __device__ void level_plan(const KArgs &a, double *red, int *iscan) {
 template <int T>
 __global__ void __launch_bounds__(T) k_plan(KArgs a) {
     pdl_begin();
+    if (halted(a.w.hdr)) {
+        return;
+    }
     __shared__ double red[32];
     __shared__ int iscan[32];
     level_plan<T>(a, red, iscan);
@@ -707,6 +719,9 @@ struct PlanAllArgs {
 template <int T>
 __global__ void __launch_bounds__(T) k_plan_all(PlanAllArgs P) {
     pdl_begin();
+    if (halted(P.base.w.hdr)) {
+        return;
+    }
     __shared__ double red[32];
     __shared__ int iscan[32];
     const PlanLevel &L = P.lv[blockIdx.x];
@@ -1012,6 +1027,9 @@ __device__ void defl_finish(const KArgs &a, int g, int K, int Kz, double rho, do
 template <int T>
 __global__ void __launch_bounds__(T) k_merge_deflate(KArgs a) {
     pdl_begin();
+    if (halted(a.w.hdr)) {
+        return;
+    }
     __shared__ double red[32];
     __shared__ int iscan[32];
     __shared__ int s_last;
@@ -1051,6 +1069,9 @@ __global__ void __launch_bounds__(T) k_merge_deflate(KArgs a) {
 template <int T>
 __global__ void __launch_bounds__(T) k_merge_deflate_cl(KArgs a) {
     pdl_begin();
+    if (halted(a.w.hdr)) {
+        return;
+    }
     namespace cg = cooperative_groups;
     __shared__ double red[32];
     __shared__ int iscan[32];
@@ -1155,6 +1176,8 @@ struct TileSet {
     int ntiles;
     bool resident;
     bool loaded;
+    unsigned pend;               // stages with a copy issued and not yet waited for
+    unsigned long long wait_ns;  // bound of one tile wait
 };
 
 template <int NA>
@@ -1172,6 +1195,37 @@ __device__ inline void tiles_issue(TileSet<NA> &ts, int stage, int tile) {
                      &ts.bar[stage]);
         }
     }
+    ts.pend |= 1u << stage;
+}
+
+// Wait for the copies of one stage, every thread of the block; true when
+// they landed within the wait limit for all threads.  On a timeout the
+// stage stays pending (tiles_drain waits for it) and the phase unchanged.
+template <int NA>
+__device__ inline bool tiles_wait(TileSet<NA> &ts, int stage) {
+    const bool ok = mbar_wait(&ts.bar[stage], ts.phase[stage], ts.wait_ns);
+    if (!__syncthreads_and(ok)) {
+        return false;
+    }
+    ts.phase[stage] ^= 1u;
+    ts.pend &= ~(1u << stage);
+    return true;
+}
+
+// After a timeout: wait (bounded by kDrainWaitNs) for the copies still in
+// flight into this block's shared memory, so none lands after the block
+// has moved on or exited.
+template <int NA>
+__device__ inline void tiles_drain(TileSet<NA> &ts) {
+#pragma unroll
+    for (int st = 0; st < 2; ++st) {
+        if (ts.pend & (1u << st)) {
+            mbar_wait(&ts.bar[st], ts.phase[st], kDrainWaitNs);
+            ts.phase[st] ^= 1u;
+        }
+    }
+    ts.pend = 0u;
+    __syncthreads();
 }
 
 // Runs one sweep over the slice; body(j0, cnt, bufs) consumes a tile whose
@@ -1184,13 +1238,10 @@ __device__ inline bool tiles_sweep(TileSet<NA> &ts, Body body) {
             if (ts.ntiles > 1) {
                 tiles_issue(ts, 1, 1);
             }
-            bool ok = mbar_wait(&ts.bar[0], ts.phase[0]);
-            ts.phase[0] ^= 1u;
-            if (ts.ntiles > 1) {
-                ok = mbar_wait(&ts.bar[1], ts.phase[1]) && ok;
-                ts.phase[1] ^= 1u;
+            if (!tiles_wait(ts, 0)) {
+                return false;
             }
-            if (!__syncthreads_and(ok)) {
+            if (ts.ntiles > 1 && !tiles_wait(ts, 1)) {
                 return false;
             }
             ts.loaded = true;
@@ -1206,9 +1257,7 @@ __device__ inline bool tiles_sweep(TileSet<NA> &ts, Body body) {
     tiles_issue(ts, 1, 1);
     for (int t = 0; t < ts.ntiles; ++t) {
         const int st = t & 1;
-        const bool ok = mbar_wait(&ts.bar[st], ts.phase[st]);
-        ts.phase[st] ^= 1u;
-        if (!__syncthreads_and(ok)) {
+        if (!tiles_wait(ts, st)) {
             return false;
         }
         const int first = t * kTile;
@@ -1225,7 +1274,7 @@ __device__ inline bool tiles_sweep(TileSet<NA> &ts, Body body) {
 template <int NA>
 __device__ inline void tiles_setup(TileSet<NA> &ts, double *smem, uint64_t *bar,
                                    const double *const *src, long long poff,
-                                   int count) {
+                                   int count, unsigned long long wait_ns) {
 #pragma unroll
     for (int st = 0; st < 2; ++st) {
 #pragma unroll
@@ -1243,6 +1292,8 @@ __device__ inline void tiles_setup(TileSet<NA> &ts, double *smem, uint64_t *bar,
     ts.ntiles = (count + kTile - 1) / kTile;
     ts.resident = ts.ntiles <= 2;
     ts.loaded = false;
+    ts.pend = 0u;
+    ts.wait_ns = wait_ns;
 }
 
 __device__ inline void record_error(WsHeader *h, int code) {
@@ -1406,6 +1457,7 @@ __device__ bool sweep_secular(const KArgs &a, int cta_blocks, double *smem, uint
     const Ws &w = a.w;
     const LevelCtl *ctl = &w.hdr->lvl[a.k];
     const double eps = DBL_EPSILON;
+    const int max_iter = w.hdr->max_iter;
 
     if ((int)blockIdx.x >= cta_blocks) {
         const int tpr = ctl->tpr_w;
@@ -1452,7 +1504,7 @@ __device__ bool sweep_secular(const KArgs &a, int cta_blocks, double *smem, uint
                 }
                 sums_reduce(sum, tpr);
                 if (active && st.stage != 2) {
-                    sec_after_sweep(st, sum, eps);
+                    sec_after_sweep(st, sum, eps, max_iter);
                 }
                 if (__all_sync(0xffffffffu, (!active) || st.stage == 2)) {
                     break;
@@ -1509,7 +1561,7 @@ __device__ bool sweep_secular(const KArgs &a, int cta_blocks, double *smem, uint
         }
         TileSet<2> ts;
         const double *srcs[2] = {w.pd, w.pz};
-        tiles_setup<2>(ts, smem, bars, srcs, po, K);
+        tiles_setup<2>(ts, smem, bars, srcs, po, K, w.hdr->wait_ns);
         ts.phase[0] = ph[0];
         ts.phase[1] = ph[1];
         SecRoot st;
@@ -1589,7 +1641,7 @@ __device__ bool sweep_secular(const KArgs &a, int cta_blocks, double *smem, uint
             if (wlive) {
                 sums_reduce(sum, tpr);
                 if (live) {
-                    sec_after_sweep(st, sum, eps);
+                    sec_after_sweep(st, sum, eps, max_iter);
                 }
                 if (__all_sync(0xffffffffu, (!active) || st.stage == 2)) {
                     if (active && lane == 0) {
@@ -1604,6 +1656,7 @@ __device__ bool sweep_secular(const KArgs &a, int cta_blocks, double *smem, uint
         ph[0] = ts.phase[0];
         ph[1] = ts.phase[1];
         if (!ok) {
+            tiles_drain(ts);
             record_error(w.hdr, kErrBarrierTimeout);
             return false;
         }
@@ -1696,7 +1749,7 @@ __device__ bool sweep_lowner(const KArgs &a, int cta_blocks, double *smem, uint6
         double prod = 1.0, prod2 = 1.0;
         TileSet<3> ts;
         const double *srcs[3] = {w.rdo, w.rtau, w.pd};
-        tiles_setup<3>(ts, smem, bars, srcs, po, K);
+        tiles_setup<3>(ts, smem, bars, srcs, po, K, w.hdr->wait_ns);
         ts.phase[0] = ph[0];
         ts.phase[1] = ph[1];
         const bool ok = tiles_sweep<3>(ts, [&](int j0, int cnt, double *const *b) {
@@ -1720,6 +1773,7 @@ __device__ bool sweep_lowner(const KArgs &a, int cta_blocks, double *smem, uint6
         ph[0] = ts.phase[0];
         ph[1] = ts.phase[1];
         if (!ok) {
+            tiles_drain(ts);
             record_error(w.hdr, kErrBarrierTimeout);
             return false;
         }
@@ -1811,7 +1865,7 @@ __device__ bool sweep_rows(const KArgs &a, int cta_blocks, double *smem, uint64_
         double a1 = 0.0, a2 = 0.0, s2 = 0.0;
         TileSet<4> ts;
         const double *srcs[4] = {w.pd, w.pw, w.pf, w.pl};
-        tiles_setup<4>(ts, smem, bars, srcs, po, K);
+        tiles_setup<4>(ts, smem, bars, srcs, po, K, w.hdr->wait_ns);
         ts.phase[0] = ph[0];
         ts.phase[1] = ph[1];
         const bool ok = tiles_sweep<4>(ts, [&](int j0, int cnt, double *const *b) {
@@ -1828,6 +1882,7 @@ __device__ bool sweep_rows(const KArgs &a, int cta_blocks, double *smem, uint64_
         ph[0] = ts.phase[0];
         ph[1] = ts.phase[1];
         if (!ok) {
+            tiles_drain(ts);
             record_error(w.hdr, kErrBarrierTimeout);
             return false;
         }
@@ -1909,15 +1964,8 @@ __device__ void place_rows(const KArgs &a, long long total_n) {
 // ------------------------------------------------------------ k_sweeps
 // Grid-wide barrier of a cooperative launch (every block resident), on the
 // level's counter pair: arrivals, then a generation bump by the last block.
-// The wait is bounded (kGridBarrierNs); on timeout the status records it and
-// the caller leaves.
-constexpr unsigned long long kGridBarrierNs = 20ull * 1000ull * 1000ull * 1000ull;
-
-__device__ inline unsigned long long globaltimer_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
+// The wait is bounded by the handle's wait limit (WsHeader::wait_ns); on
+// timeout the status records it and the caller leaves.
 
 __device__ inline bool grid_barrier(WsHeader *h, LevelCtl *c) {
     __syncthreads();
@@ -1932,9 +1980,10 @@ __device__ inline bool grid_barrier(WsHeader *h, LevelCtl *c) {
             atomicAdd(&c->bar_gen, 1u);
         } else {
             const unsigned long long t0 = globaltimer_ns();
+            const unsigned long long limit = h->wait_ns;
             while (*gen == g) {
                 __nanosleep(100);
-                if (globaltimer_ns() - t0 > kGridBarrierNs) {
+                if (globaltimer_ns() - t0 > limit) {
                     ok = 0;
                     record_error(h, kErrGridBarrierTimeout);
                     break;
@@ -1957,6 +2006,9 @@ __device__ inline bool grid_barrier(WsHeader *h, LevelCtl *c) {
 __global__ void __launch_bounds__(kSweepThreads)
     k_sweeps(KArgs a, int tiles, int rows, long long total_n) {
     pdl_begin();
+    if (halted(a.w.hdr)) {
+        return;
+    }
     extern __shared__ __align__(16) double smem[];
     __shared__ __align__(8) uint64_t bars[2];
     WsHeader *h = a.w.hdr;
@@ -2006,24 +2058,35 @@ __global__ void __launch_bounds__(kSweepThreads)
 // Max-norm max(|D|, |E|) of every instance, as the bits of a non-negative
 // double (which order like the integers): grid-wide with one
 // atomic per block for a single matrix, one warp per instance for a batch.
+// A NaN or an infinity anywhere in D or E (the ignored E slot at the end
+// of each instance excepted) sets kErrNonFinite: nothing after k_norm runs,
+// and brdc_get_info reports it.  (fmax would drop a NaN silently.)
 __global__ void __launch_bounds__(256) k_norm(Forest F, const double *D, const double *E,
-                                              long long *out) {
+                                              long long *out, WsHeader *h) {
     pdl_begin();
     const int lane = threadIdx.x & 31;
+    bool bad = false;
     if (F.B == 1) {
         const long long n = F.n0;
         double mx = 0.0;
         for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
              i += (long long)gridDim.x * blockDim.x) {
-            mx = fmax(mx, fabs(D[i]));
+            const double dv = fabs(D[i]);
+            bad |= !(dv <= DBL_MAX);
+            mx = fmax(mx, dv);
             if (i + 1 < n) {
-                mx = fmax(mx, fabs(E[i]));
+                const double ev = fabs(E[i]);
+                bad |= !(ev <= DBL_MAX);
+                mx = fmax(mx, ev);
             }
         }
         __shared__ double red[32];
         mx = block_max<256>(mx, red);
         if (threadIdx.x == 0) {
             atomicMax(out, __double_as_longlong(mx));
+        }
+        if (bad) {
+            record_error(h, kErrNonFinite);
         }
         return;
     }
@@ -2033,9 +2096,13 @@ __global__ void __launch_bounds__(256) k_norm(Forest F, const double *D, const d
         const long long lo = F.off[b], hi = F.off[b + 1];
         double mx = 0.0;
         for (long long i = lo + lane; i < hi; i += 32) {
-            mx = fmax(mx, fabs(D[i]));
+            const double dv = fabs(D[i]);
+            bad |= !(dv <= DBL_MAX);
+            mx = fmax(mx, dv);
             if (i + 1 < hi) {
-                mx = fmax(mx, fabs(E[i]));
+                const double ev = fabs(E[i]);
+                bad |= !(ev <= DBL_MAX);
+                mx = fmax(mx, ev);
             }
         }
         mx = warp_max(mx);
@@ -2043,10 +2110,14 @@ __global__ void __launch_bounds__(256) k_norm(Forest F, const double *D, const d
             out[b] = __double_as_longlong(mx);
         }
     }
+    if (bad) {
+        record_error(h, kErrNonFinite);
+    }
 }
 
 __global__ void k_init(WsHeader *h, int levels, int B, long long total_n,
-                       long long leaves, int flags, long long *norm) {
+                       long long leaves, int flags, long long *norm, int max_iter,
+                       unsigned long long wait_ns) {
     const int t = threadIdx.x;
     if (t == 0) {
         norm[0] = 0;
@@ -2061,6 +2132,8 @@ __global__ void k_init(WsHeader *h, int levels, int B, long long total_n,
         h->status = 0;
         h->nonconv = 0;
         h->leaf_sweeps_max = 0;
+        h->max_iter = max_iter;
+        h->wait_ns = wait_ns;
     }
     for (int k = t; k < BRDC_MAX_LEVELS; k += blockDim.x) {
         h->lvl[k].ticket = 0;

@@ -115,6 +115,7 @@ __device__ void level_roots(LvlSmem &S, cooperative_groups::cluster_group &cl, c
     const long long po = G.poff;
     const int x = threadIdx.x, lane = x & 31;
     const double eps = DBL_EPSILON;
+    const int max_iter = a.w.hdr->max_iter;
     for (int i = x; i < K; i += T) {
         S.pd[i] = w.pd[po + i];
         S.pz[i] = w.pz[po + i];
@@ -168,7 +169,7 @@ __device__ void level_roots(LvlSmem &S, cooperative_groups::cluster_group &cl, c
                 }
                 sums_reduce(sum, tp);
                 if (live) {
-                    sec_after_sweep(st, sum, eps);
+                    sec_after_sweep(st, sum, eps, max_iter);
                 }
                 if (__all_sync(kFull, !act || st.stage == 2)) {
                     break;
@@ -312,6 +313,9 @@ __device__ void level_ticket(const KArgs &a, LvlSmem &S) {
 template <int T>
 __global__ void __launch_bounds__(T, 1) k_level(KArgs a) {
     pdl_begin();
+    if (halted(a.w.hdr)) {
+        return;
+    }
     namespace cg = cooperative_groups;
     extern __shared__ __align__(16) unsigned char lvl_raw[];
     LvlSmem &S = *reinterpret_cast<LvlSmem *>(lvl_raw);

@@ -37,6 +37,8 @@
 
 namespace brdc {
 
+// Default cap on the iterations of one root; a handle may set another
+// (brdc_set_limits), which the kernels read from the workspace header.
 constexpr int kSecularMaxIter = 64;
 
 // 1/x for the pole-root pair loops.  IEEE division carries a branch to its
@@ -250,9 +252,11 @@ __host__ __device__ inline double sec_clamp_tau(double t, double lo, double hi) 
 }
 
 // Advance the state after a sweep evaluated at (eorg_d, etau).  Returns the
-// new stage (2 once converged or failed).
+// new stage (2 once converged or failed).  A root still unconverged after
+// max_iter iterations, or whose secular function evaluates to NaN, is
+// finished with r.failed set.
 __host__ __device__ inline int sec_after_sweep(SecRoot &r, const SecSums &s,
-                                               double eps) {
+                                               double eps, int max_iter = kSecularMaxIter) {
     if (r.stage == 2) {
         return 2;
     }
@@ -364,7 +368,14 @@ __host__ __device__ inline int sec_after_sweep(SecRoot &r, const SecSums &s,
         erretm = 8.0 * (-tq - psil) + err - tq + r.rhoinv + fabs(tau) * dw;
     }
 
-    if (fabs(w) <= eps * erretm || !(w == w)) {
+    if (!(w == w)) {
+        // NaN: tau on a pole (a zero delta) or non-finite data; no step can
+        // follow from it
+        r.failed = 1;
+        r.stage = 2;
+        return 2;
+    }
+    if (fabs(w) <= eps * erretm) {
         r.stage = 2;
         return 2;
     }
@@ -373,9 +384,9 @@ __host__ __device__ inline int sec_after_sweep(SecRoot &r, const SecSums &s,
     } else {
         r.hi = (tau < r.hi) ? tau : r.hi;
     }
-    if (r.hi - r.lo <= 2.0 * eps * fabs(tau) || r.iter >= kSecularMaxIter) {
+    if (r.hi - r.lo <= 2.0 * eps * fabs(tau) || r.iter >= max_iter) {
         // bracket collapsed to rounding level: accept; iteration cap: flag
-        if (r.iter >= kSecularMaxIter && !(r.hi - r.lo <= 2.0 * eps * fabs(tau))) {
+        if (r.iter >= max_iter && !(r.hi - r.lo <= 2.0 * eps * fabs(tau))) {
             r.failed = 1;
         }
         r.stage = 2;
@@ -462,7 +473,7 @@ __host__ __device__ inline int sec_solve_serial(int K, const double *d,
                                                 const double *z, double rho,
                                                 double znorm2, int i, int *org,
                                                 double *tau, int *failed,
-                                                double eps) {
+                                                double eps, int max_iter = kSecularMaxIter) {
     if (K == 1) {
         *org = 0;
         *tau = rho * z[0] * z[0];
@@ -479,7 +490,7 @@ __host__ __device__ inline int sec_solve_serial(int K, const double *d,
             sec_accum(s, r, j, d[j], z[j]);
         }
         ++sweeps;
-        sec_after_sweep(r, s, eps);
+        sec_after_sweep(r, s, eps, max_iter);
     }
     *org = r.org;
     *tau = r.tau;

@@ -129,6 +129,9 @@ __device__ inline int sub_node_of(const SubSmem<kSubRows> &S, int nk, int x) {
 template <int kSubRows>
 __global__ void __launch_bounds__(kSubRows, 512 / kSubRows) k_subtree(SubArgs A) {
     pdl_begin();
+    if (halted(A.a.w.hdr)) {
+        return;
+    }
     constexpr int kSubWarps = kSubRows / 32;
     extern __shared__ __align__(16) unsigned char sub_raw[];
     SubSmem<kSubRows> &S = *reinterpret_cast<SubSmem<kSubRows> *>(sub_raw);
@@ -137,6 +140,7 @@ __global__ void __launch_bounds__(kSubRows, 512 / kSubRows) k_subtree(SubArgs A)
     const int x = threadIdx.x;
     const int warp = x >> 5, lane = x & 31;
     const double eps = DBL_EPSILON;
+    const int max_iter = a.w.hdr->max_iter;
     const double isq2 = 0.70710678118654752440;
 
     // subtree -> instance, its levels and rows
@@ -477,7 +481,7 @@ __global__ void __launch_bounds__(kSubRows, 512 / kSubRows) k_subtree(SubArgs A)
                                          *zu = pz[u];
                                      });
                         sums_reduce(sum, 32);
-                        sec_after_sweep(st, sum, eps);
+                        sec_after_sweep(st, sum, eps, max_iter);
                     }
                     if (lane == 0) {
                         sec_park(st, S.dyn[id]);
@@ -516,7 +520,7 @@ __global__ void __launch_bounds__(kSubRows, 512 / kSubRows) k_subtree(SubArgs A)
             }
             sums_reduce(sum, tp);
             if (act) {
-                sec_after_sweep(st, sum, eps);
+                sec_after_sweep(st, sum, eps, max_iter);
             }
             // one barrier per round: round r appends to qc[r % 3], and
             // qc[(r+2) % 3], last read in round r-1, is cleared after this

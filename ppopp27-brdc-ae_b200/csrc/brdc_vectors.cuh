@@ -53,6 +53,9 @@ struct VArgs {
 // Loewner weights of the instance-root merges, which the values solve
 // skips (no parent reads their rows): one warp per pole.
 __global__ void __launch_bounds__(256) k_vec_lowner(VArgs a) {
+    if (halted(a.w.hdr)) {
+        return;
+    }
     const Ws &w = a.w;
     const int lane = threadIdx.x & 31;
     const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
@@ -116,6 +119,9 @@ __device__ inline int vec_pos(const Ws &w, long long gs, long long po, int s, in
 // eigenvector (small-z) or a short rotation combination of some (rotated
 // out), written straight to its place in the node's block.  M must be zero.
 __global__ void __launch_bounds__(256) k_vec_build(VArgs a, long long total_n) {
+    if (halted(a.w.hdr)) {
+        return;
+    }
     const Ws &w = a.w;
     const int lane = threadIdx.x & 31;
     const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
@@ -227,6 +233,9 @@ __global__ void __launch_bounds__(256) k_vec_build(VArgs a, long long total_n) {
 // Root eigenvectors from the products (node's block of C, columns in root
 // order) to their places in the node's ascending order: one warp per root.
 __global__ void __launch_bounds__(256) k_vec_scatter(VArgs a, const double *C, long long total_n) {
+    if (halted(a.w.hdr)) {
+        return;
+    }
     const Ws &w = a.w;
     const int lane = threadIdx.x & 31;
     const long long warps = (long long)gridDim.x * (blockDim.x >> 5);

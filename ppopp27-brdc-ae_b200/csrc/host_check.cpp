@@ -11,3 +11,11 @@ extern "C" int brdc_host_secular_root(int K, const double *d, const double *z,
     return brdc::sec_solve_serial(K, d, z, rho, znorm2, i, org, tau, failed,
                                   DBL_EPSILON);
 }
+
+// The same with an iteration cap of its own (the failure path).
+extern "C" int brdc_host_secular_root_capped(int K, const double *d, const double *z,
+                                             double rho, double znorm2, int i, int max_iter,
+                                             int *org, double *tau, int *failed) {
+    return brdc::sec_solve_serial(K, d, z, rho, znorm2, i, org, tau, failed,
+                                  DBL_EPSILON, max_iter);
+}

@@ -158,6 +158,32 @@ def test_autograd_function(solver):
     assert np.max(np.abs(E.grad.cpu().numpy() - re)) < 1e-9 * sc
 
 
+def test_autograd_two_matrices_of_one_order_in_one_loss(solver):
+    """Two forwards of the same order before one backward: each backward
+    must read its own forward's checkpoints."""
+    import torch
+
+    from brdc.autograd import eigvalsh_tridiagonal
+
+    n = 800
+    mats = [families.generate("normal", n, instance=s) for s in (11, 12)]
+    rng = np.random.default_rng(5)
+    gs = [rng.standard_normal(n) for _ in mats]
+    leaves = []
+    loss = 0.0
+    for (d, e), g in zip(mats, gs):
+        D = torch.tensor(d, device="cuda", requires_grad=True)
+        E = torch.tensor(e, device="cuda", requires_grad=True)
+        leaves.append((D, E))
+        loss = loss + (eigvalsh_tridiagonal(D, E, solver) * torch.tensor(g, device="cuda")).sum()
+    loss.backward()
+    for (d, e), g, (D, E) in zip(mats, gs, leaves):
+        rd, re = eig_ref_grads(d, e, g)
+        sc = max(np.max(np.abs(rd)), np.max(np.abs(re)))
+        assert np.max(np.abs(D.grad.cpu().numpy() - rd)) < 1e-9 * sc
+        assert np.max(np.abs(E.grad.cpu().numpy() - re)) < 1e-9 * sc
+
+
 def test_keep_forward_matches_rerun(solver):
     import torch
 

@@ -122,6 +122,35 @@ def test_graph_capture_batched(solver):
     assert torch.equal(W, ref)
 
 
+def test_batched_workspace_reused_between_calls(solver):
+    """A batched call, then other use of the same workspace bytes (a single
+    solve carves them its own way; a caching allocator may hand them to
+    anything), then the same batched call again: its per-instance tables
+    must be rewritten, not assumed."""
+    import torch
+
+    import brdc
+
+    off, D, E, orders, _ = families.batch(24, 17, 1500, seed=5)
+    Dt = torch.tensor(D, device="cuda")
+    Et = torch.tensor(E, device="cuda")
+    ws = solver.batched_workspace(off)
+    W0 = solver.dstebr_batched(off, Dt, Et, workspace=ws).cpu().numpy()
+    assert per_instance_errors(off, W0, D, E).max() < TOL
+    n = int(off[-1]) // 2
+    assert brdc.workspace_size(n) <= ws.numel()
+    d, e = families.generate("normal", n)
+    w1 = solver.dstebr(torch.tensor(d, device="cuda"), torch.tensor(e, device="cuda"),
+                       workspace=ws).cpu().numpy()
+    ref1 = oracle.dstedc_dc_br(d, e)
+    assert np.max(np.abs(w1 - ref1)) < TOL * np.max(np.abs(ref1))
+    W2 = solver.dstebr_batched(off, Dt, Et, workspace=ws).cpu().numpy()
+    assert per_instance_errors(off, W2, D, E).max() < TOL
+    ws.fill_(255)  # every byte, tables included
+    W3 = solver.dstebr_batched(off, Dt, Et, workspace=ws).cpu().numpy()
+    assert per_instance_errors(off, W3, D, E).max() < TOL
+
+
 def test_batched_tunings_agree(solver):
     """A batch of mixed orders (tiny ones solved wholly inside the subtree
     kernel, large ones continuing with per-level kernels) gives the same

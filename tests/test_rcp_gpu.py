@@ -9,12 +9,20 @@ import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
-ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-PROBE = os.path.join(ROOT, "ppopp27-brdc-ae_b200", "brdc", "libbrdc_probe.so")
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(os.path.dirname(HERE), "ppopp27-brdc-ae_b200", "csrc")
+
+
+def probe_lib() -> str:
+    import build as brdc_build
+
+    return brdc_build.nvcc_shared(os.path.join(HERE, "rcp_ulps.cu"),
+                                  os.path.join(HERE, "librcp_ulps.so"),
+                                  deps=[os.path.join(CSRC, "brdc_secular.cuh")], includes=[CSRC])
 
 
 def ulps(x):
-    lib = ctypes.CDLL(PROBE)
+    lib = ctypes.CDLL(probe_lib())
     lib.brdc_probe_rcp_ulps.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
     x = np.ascontiguousarray(x, dtype=np.float64)
     out = np.empty_like(x)

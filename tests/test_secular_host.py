@@ -84,3 +84,44 @@ def test_two_poles_closed_form(hostlib):
     for i in range(2):
         lam, _, _ = _root(hostlib, d, z, rho, i)
         assert abs(lam - ev[i]) < 1e-15 * 4
+
+
+def _root_capped(lib, d, z, rho, i, max_iter):
+    dp = ctypes.POINTER(ctypes.c_double)
+    lib.brdc_host_secular_root_capped.argtypes = [
+        ctypes.c_int, dp, dp, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int,
+        ctypes.POINTER(ctypes.c_int), dp, ctypes.POINTER(ctypes.c_int),
+    ]
+    org, tau, f = ctypes.c_int(), ctypes.c_double(), ctypes.c_int()
+    sweeps = lib.brdc_host_secular_root_capped(len(d), d.ctypes.data_as(dp), z.ctypes.data_as(dp),
+                                               rho, float(np.nansum(z * z)), i, max_iter,
+                                               ctypes.byref(org), ctypes.byref(tau), ctypes.byref(f))
+    return sweeps, f.value
+
+
+def test_iteration_cap_reports_failure(hostlib):
+    """With a cap of one iteration no root of a generic problem converges:
+    every one stops and is flagged; with the default cap none is."""
+    rng = np.random.default_rng(21)
+    K = 60
+    d = np.sort(rng.standard_normal(K))
+    z = rng.standard_normal(K)
+    z /= np.linalg.norm(z)
+    flagged = 0
+    for i in range(K):
+        sweeps, failed = _root_capped(hostlib, d, z, 1.0, i, 1)
+        assert sweeps <= 2
+        flagged += failed
+        assert _root_capped(hostlib, d, z, 1.0, i, 64)[1] == 0
+    assert flagged == K
+
+
+def test_nan_secular_function_is_a_failure(hostlib):
+    """A NaN in the data makes the secular function NaN: the root must stop
+    and be reported failed, not accepted as converged."""
+    d = np.array([0.0, 0.5, 1.0, 2.0])
+    z = np.array([0.5, np.nan, 0.5, 0.5])
+    for i in range(len(d)):
+        sweeps, failed = _root_capped(hostlib, d, z, 1.0, i, 64)
+        assert failed == 1
+        assert sweeps <= 2
