@@ -30,7 +30,14 @@ workload and prints the same metric with "impl": "reference".
 With --gpus N > 1 (torchrun, one process per GPU) every rank solves its own
 replica (a single solve does not shard: the tree funnels into one root
 merge); value is the max over ranks of the per-solve time and
-solves_per_s is the whole-job rate.
+solves_per_s is the whole-job rate.  The batch of config 3 does shard:
+"sharded_batch" gives its whole-job solves/s with each rank solving its
+share of the 4096 instances (no collective on the data path).
+
+Beside this build, the default line times the reference CUDA prototype
+(built from the reference's sources into oracle/_ref) on the same inputs on
+the same GPU ("ref_gpu"), and records whether cuSOLVER exports
+cusolverDnXstedc.
 """
 from __future__ import annotations
 
@@ -266,7 +273,9 @@ def main():
         import torch.distributed as dist_mod
 
         dist = dist_mod
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        # rank 0 alone measures the extras (minutes) while the others wait
+        # at the closing barrier
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
 
     solver = brdc.Solver()
     d, e = families.generate(FAMILY_HEAD, N_HEAD, instance=rank)
@@ -297,6 +306,11 @@ def main():
     from brdc.sharding import max_over_ranks
 
     ms = max_over_ranks(float(np.mean(times)), dist, device="cuda")
+
+    # config 3's batch sharded over the ranks (every rank takes part)
+    sharded = None
+    if world > 1 and not args.no_extras:
+        sharded = bench_sharded_batch(torch, brdc, families, rank, world, dist, flush)
 
     extras = {}
     if rank == 0 and not args.no_extras:
@@ -338,6 +352,8 @@ def main():
             "clocks": clocks,
         }
         line.update({k: v for k, v in extras.items() if k != "launches"})
+        if sharded is not None:
+            line["sharded_batch"] = sharded
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
@@ -939,6 +955,50 @@ def bench_batched(torch, brdc, families, solver, flush):
             "max_rel_err_vs_lapack": max(errs),
             "lapack_sample": f"{len(errs)} instances (every 16th)",
             "workspace_bytes": ws.numel()}
+
+
+def bench_sharded_batch(torch, brdc, families, rank, world, dist, flush):
+    """Config 3's batch (4096 tridiagonals, N log-uniform in [32, 8192], the
+    four families in turn) sharded over the ranks: each rank solves its
+    partition_instances share (balanced by sum n^2) as one batched solve
+    replayed from a CUDA graph, with no collective on the data path.  Time =
+    max over ranks of the mean of 5 replays (L2 flushed before each);
+    solves_per_s is the whole job's rate."""
+    from brdc.sharding import max_over_ranks, pack, partition_instances
+
+    count = 4096
+    off, D, E, orders, _ = families.batch(count, 32, 8192, seed=3)
+    idx = partition_instances(orders, world)[rank]
+    o2, D2, E2 = pack(off, D, E, idx)
+    solver = brdc.Solver()
+    Dt = torch.tensor(D2, device="cuda")
+    Et = torch.tensor(E2, device="cuda")
+    W = torch.empty(int(o2[-1]), dtype=torch.float64, device="cuda")
+    ws = solver.batched_workspace(o2)
+    stream = torch.cuda.Stream()
+    stream.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(stream):
+        solver.set_stream(stream)
+        solver.set_tuning(subtree_levels=5)
+        solver.dstebr_batched(o2, Dt, Et, W=W, workspace=ws)  # writes the forest tables
+        stream.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=stream):
+            solver.dstebr_batched(o2, Dt, Et, W=W, workspace=ws)
+        g.replay()
+        stream.synchronize()
+        t = float(np.mean(_event_ms(torch, g.replay, 5, flush, stream)))
+    torch.cuda.synchronize()
+    info = solver.info_status(0, ws)[0]
+    del g
+    solver.close()
+    t_max = max_over_ranks(t, dist, device="cuda")
+    sum_n2 = float(np.sum(np.asarray(orders, dtype=np.float64)[idx] ** 2))
+    sum_n2_max = max_over_ranks(sum_n2, dist, device="cuda")
+    return {"count": count, "ranks": world, "ms": t_max, "solves_per_s": count * 1e3 / t_max,
+            "balance_sum_n2_max_over_mean": sum_n2_max / (float(np.sum(orders.astype(np.float64) ** 2)) / world),
+            "info_rank0": info,
+            "timing": "max over ranks of each rank's mean graph replay (5, L2 flushed before each)"}
 
 
 def bench_fit(torch, brdc, families, flush, steps=200, lr=0.1):

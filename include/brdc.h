@@ -187,6 +187,31 @@ typedef struct brdc_diagnostics {
 brdc_status brdc_get_diagnostics(brdc_handle handle, const void *workspace,
                                  brdc_diagnostics *out);
 
+/* Deflation record of one merge level of the last solve of order n on a
+ * checkpointing workspace (BRDC_FLAG_KEEP_CHECKPOINTS; synchronises the
+ * stream; one matrix, not a batch).  Host arrays of n entries, indexed by
+ * the row's position in its node's merged list (the two children's
+ * eigenvalues in ascending order; the nodes' slices in row order):
+ *   d, z     the pole and its weight as the merge formed them
+ *            (z = child boundary row / sqrt(2))
+ *   row      the pole's row within its node before the merge
+ *            (row < floor(size/2): from the left child)
+ *   state    0 secular pole, 1 deflated by the small-z test |rho z| <= tol,
+ *            2 rotated out by close-pole deflation
+ *   link     state 0: its index among the node's K poles (ascending d);
+ *            state 2: merged position of the chain base it was rotated
+ *            into; state 1: -1
+ *   c, s     state 2: the Givens pair that zeroed its z (else 0)
+ * and, per node of the level (2^(levels-1-level) of them, in row order),
+ * K, rho and tol.  The record of the reference's merge kernels (mask, map,
+ * dcount, cc, ss: gpu/src/tridiag_solver_merge_kernels.cuh:143-290), which
+ * the tests compare with the reference's own decisions on the same data. */
+brdc_status brdc_get_merge_trace(brdc_handle handle, const void *workspace,
+                                 size_t workspace_size, int64_t n, int level,
+                                 double *d, double *z, int *row, int *state, int *link,
+                                 double *c, double *s, int *node_K, double *node_rho,
+                                 double *node_tol);
+
 /* Per-phase device timings of the last solve enqueued with timing on,
  * measured with CUDA events on the handle's stream between the kernels.
  * Replaces evd_get_last_stage_timings (gpu/include/evd/evd.h:27-29,

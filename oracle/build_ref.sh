@@ -15,7 +15,9 @@ SRC="$REF/gpu/src"
 [ -d "$SRC" ] || { echo "reference sources not found under $REF" >&2; exit 1; }
 mkdir -p "$OUT"
 LIB="$OUT/libref_brdc_gpu.so"
-if [ -f "$LIB" ] && [ "$LIB" -nt "$HERE/ref_shim.cu" ] && [ "$LIB" -nt "$0" ]; then
+MERGE_LIB="$OUT/libref_merge.so"
+if [ -f "$LIB" ] && [ "$LIB" -nt "$HERE/ref_shim.cu" ] && [ "$LIB" -nt "$0" ] &&
+   [ -f "$MERGE_LIB" ] && [ "$MERGE_LIB" -nt "$HERE/ref_merge.cu" ] && [ "$MERGE_LIB" -nt "$0" ]; then
   exit 0
 fi
 FLAGS=(-gencode arch=compute_100a,code=sm_100a -O3 -std=c++17 -Xcompiler -fPIC
@@ -29,4 +31,6 @@ trap 'rm -rf "$TMP"' EXIT
 "$NVCC" "${FLAGS[@]}" -c "$HERE/ref_shim.cu" -o "$TMP/ref_shim.o"
 "$NVCC" -shared -gencode arch=compute_100a,code=sm_100a -o "$LIB" "$TMP"/*.o \
   -lcublas -lcusolver -ldl
+# the reference's deflation kernels alone, driven on caller-supplied merge inputs
+"$NVCC" "${FLAGS[@]}" -shared -o "$MERGE_LIB" "$HERE/ref_merge.cu"
 echo "$LIB"

@@ -16,7 +16,45 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_ref", "libref_brdc_gpu.so")
+MERGE_LIB_PATH = os.path.join(_HERE, "_ref", "libref_merge.so")
 _lib = None
+_merge_lib = None
+
+
+def merge_available() -> bool:
+    return os.path.exists(MERGE_LIB_PATH)
+
+
+def merge_level(child_sizes, D, E, first_rows, last_rows) -> dict:
+    """The reference's own deflation kernels (ref_merge.cu) on one merge
+    level: child_sizes [2 per merge], D, E, first_rows, last_rows by row.
+    Returns mask0, mask, map, md, ndd, dcount, z, cc, ss, tol, rho."""
+    global _merge_lib
+    if _merge_lib is None:
+        if not merge_available():
+            raise RuntimeError("reference deflation kernels not built (oracle/build_ref.sh)")
+        lib = ctypes.CDLL(MERGE_LIB_PATH)
+        ip = ctypes.POINTER(ctypes.c_int)
+        dp = ctypes.POINTER(ctypes.c_double)
+        lib.ref_merge_level.argtypes = [ctypes.c_int, ctypes.c_int, ip, dp, dp, dp, dp,
+                                        ip, ip, ip, dp, ip, ip, dp, dp, dp, dp, dp]
+        _merge_lib = lib
+    cs = np.ascontiguousarray(child_sizes, dtype=np.int32)
+    n = int(cs.sum())
+    args = [np.ascontiguousarray(a, dtype=np.float64) for a in (D, E, first_rows, last_rows)]
+    out = {k: np.zeros(n, dtype=np.int32) for k in ("mask0", "mask", "map", "ndd", "dcount")}
+    out.update({k: np.zeros(n) for k in ("md", "z", "cc", "ss", "tol", "rho")})
+    ip = ctypes.POINTER(ctypes.c_int)
+    dp = ctypes.POINTER(ctypes.c_double)
+    st = _merge_lib.ref_merge_level(
+        n, len(cs) // 2, cs.ctypes.data_as(ip), *[a.ctypes.data_as(dp) for a in args],
+        out["mask0"].ctypes.data_as(ip), out["mask"].ctypes.data_as(ip), out["map"].ctypes.data_as(ip),
+        out["md"].ctypes.data_as(dp), out["ndd"].ctypes.data_as(ip), out["dcount"].ctypes.data_as(ip),
+        out["z"].ctypes.data_as(dp), out["cc"].ctypes.data_as(dp), out["ss"].ctypes.data_as(dp),
+        out["tol"].ctypes.data_as(dp), out["rho"].ctypes.data_as(dp))
+    if st != 0:
+        raise RuntimeError(f"ref_merge_level status {st}")
+    return out
 
 
 def available() -> bool:

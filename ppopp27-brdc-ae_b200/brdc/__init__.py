@@ -73,6 +73,7 @@ EXPORTS = (
     "brdc_set_limits",
     "brdc_get_limits",
     "brdc_dstebr_noalloc_get_info",
+    "brdc_get_merge_trace",
 )
 
 
@@ -214,6 +215,9 @@ def load() -> ctypes.CDLL:
                                   ctypes.POINTER(Tuning)]
     lib.brdc_set_limits.argtypes = [vp, ctypes.POINTER(Limits)]
     lib.brdc_dstebr_noalloc_get_info.argtypes = [vp, ip]
+    dpp = ctypes.POINTER(ctypes.c_double)
+    lib.brdc_get_merge_trace.argtypes = [vp, vp, sz, i64, ctypes.c_int, dpp, dpp, ip, ip, ip,
+                                         dpp, dpp, ip, dpp, dpp]
     lib.brdc_get_limits.argtypes = [vp, ctypes.POINTER(Limits)]
     for f in ("brdc_create", "brdc_destroy", "brdc_set_stream", "brdc_get_stream",
               "brdc_get_last_error", "brdc_dstebr_workspace_size", "brdc_dstebr",
@@ -222,7 +226,8 @@ def load() -> ctypes.CDLL:
               "brdc_set_timing", "brdc_get_last_timings", "brdc_dstebr_noalloc",
               "brdc_dstebr_batched_checkpoint_workspace_size", "brdc_dstebr_batched_backward",
               "brdc_set_tuning", "brdc_get_tuning", "brdc_autotune",
-              "brdc_set_limits", "brdc_get_limits", "brdc_dstebr_noalloc_get_info"):
+              "brdc_set_limits", "brdc_get_limits", "brdc_dstebr_noalloc_get_info",
+              "brdc_get_merge_trace"):
         getattr(lib, f).restype = ctypes.c_int
     _lib = lib
     return lib
@@ -480,6 +485,27 @@ class Solver:
         if st not in (SUCCESS, NOT_CONVERGED, INTERNAL_ERROR):
             _check(st, "brdc_get_info", self.h)
         return int(out.value), int(st)
+
+    def merge_trace(self, n: int, level: int, workspace) -> dict:
+        """Deflation record of one merge level of the last solve on a
+        checkpointing workspace (brdc_get_merge_trace), as numpy arrays."""
+        L = self.diagnostics(n, workspace)["levels"]
+        nodes = 1 << (L - 1 - level)
+        out = {k: np.zeros(n) for k in ("d", "z", "c", "s")}
+        out.update({k: np.zeros(n, dtype=np.int32) for k in ("row", "state", "link")})
+        out["K"] = np.zeros(nodes, dtype=np.int32)
+        out["rho"] = np.zeros(nodes)
+        out["tol"] = np.zeros(nodes)
+        dp = ctypes.POINTER(ctypes.c_double)
+        ipt = ctypes.POINTER(ctypes.c_int)
+        st = load().brdc_get_merge_trace(
+            self.h, ctypes.c_void_p(workspace.data_ptr()), workspace.numel(), int(n), int(level),
+            out["d"].ctypes.data_as(dp), out["z"].ctypes.data_as(dp), out["row"].ctypes.data_as(ipt),
+            out["state"].ctypes.data_as(ipt), out["link"].ctypes.data_as(ipt),
+            out["c"].ctypes.data_as(dp), out["s"].ctypes.data_as(dp), out["K"].ctypes.data_as(ipt),
+            out["rho"].ctypes.data_as(dp), out["tol"].ctypes.data_as(dp))
+        _check(st, "brdc_get_merge_trace", self.h)
+        return out
 
     def diagnostics(self, n: int, workspace=None) -> dict:
         ws = self.workspace(n) if workspace is None else workspace

@@ -176,7 +176,7 @@ struct SlotDesc {
 const SlotDesc kSlots[] = {
     SD(cd, CN_NT, false, false), SD(cf, CN_NT, false, false), SD(cl, CN_NT, false, false),
     SD(nd, CN_NT, false, false), SD(nf, CN_NT, false, false), SD(nl, CN_NT, false, false),
-    SD(md, CN_NT, false, false), SD(mz, CN_NT, false, false), SD(mf, CN_NT, false, false),
+    SD(md, CN_NT, true, false), SD(mz, CN_NT, true, false), SD(mf, CN_NT, false, false),
     SD(ml, CN_NT, false, false), SI(morig, CN_NT, true, false),
     SD(ad, CN_NT, false, false), SD(az, CN_NT, false, false), SD(af, CN_NT, true, false),
     SD(al, CN_NT, true, false), SI(amap, CN_NT, true, false), SI(gmark, CN_NT, true, false),
@@ -190,7 +190,7 @@ const SlotDesc kSlots[] = {
     SI(rorg, CN_NP, true, false), SD(rdo, CN_NP, true, false), SD(rtau, CN_NP, true, false),
     SD(rlam, CN_NP, true, false), SD(rf, CN_NP, false, false), SD(rl, CN_NP, false, false),
     SI(nK, CN_NN, true, false), SI(nKz, CN_NN, true, false), SD(nrho, CN_NN, true, false),
-    SD(ntol, CN_NN, false, false), SD(nzn, CN_NN, false, false),
+    SD(ntol, CN_NN, true, false), SD(nzn, CN_NN, false, false),
     SI(pref_w, CN_NN1, true, false), SI(pref_c, CN_NN1, true, false),
     SI(items_w, CN_ITW, true, false), SI(items_c, CN_ITC, true, false),
     SL(f_off, CN_B1, false, false), SI(f_lev, CN_B, false, false),
@@ -1047,6 +1047,104 @@ extern "C" brdc_status brdc_get_diagnostics(brdc_handle h, const void *workspace
             hd.diag[k].size_sum - hd.diag[k].dd_before_sum;
         out->level[k].close_deflated_total =
             hd.diag[k].dd_before_sum - hd.diag[k].dd_after_sum;
+    }
+    return BRDC_STATUS_SUCCESS;
+}
+
+extern "C" brdc_status brdc_get_merge_trace(brdc_handle h, const void *workspace,
+                                            size_t workspace_size, int64_t n, int level,
+                                            double *d, double *z, int *row, int *state,
+                                            int *link, double *c, double *s, int *node_K,
+                                            double *node_rho, double *node_tol) {
+    if (h == nullptr) {
+        return BRDC_STATUS_INVALID_HANDLE;
+    }
+    if (workspace == nullptr || d == nullptr || z == nullptr || row == nullptr ||
+        state == nullptr || link == nullptr || c == nullptr || s == nullptr ||
+        node_K == nullptr || node_rho == nullptr || node_tol == nullptr) {
+        return BRDC_STATUS_INVALID_POINTER;
+    }
+    const long long off[2] = {0, (long long)n};
+    HostForest hf;
+    if (n <= 0 || n > (1LL << 30) || !build_forest(1, off, &hf) || level < 0 ||
+        level >= hf.max_levels) {
+        return BRDC_STATUS_INVALID_VALUE;
+    }
+    const Layout L = make_layout(hf, true);
+    if (workspace_size < L.bytes) {
+        return BRDC_STATUS_INVALID_WORKSPACE;
+    }
+    Ws w = carve(const_cast<void *>(workspace), hf, true);
+    level_view(hf, L, w, level, &w);
+    const int depth = hf.max_levels - 1 - level;
+    const int nodes = 1 << depth;
+    std::vector<double> md(n), mz(n), gc(n), gsn(n);
+    std::vector<int> morig(n), amap(n), gmark(n), gbase(n), zmap(n), pmap(L.np), nK(nodes), nKz(nodes);
+    std::vector<double> nrho(nodes), ntol(nodes);
+    auto get = [&](void *dst, const void *src, size_t bytes) {
+        return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, h->stream);
+    };
+    const size_t nd = sizeof(double) * (size_t)n, ni = sizeof(int) * (size_t)n;
+    cudaError_t e = cudaSuccess;
+    e = e != cudaSuccess ? e : get(md.data(), w.md, nd);
+    e = e != cudaSuccess ? e : get(mz.data(), w.mz, nd);
+    e = e != cudaSuccess ? e : get(gc.data(), w.gc, nd);
+    e = e != cudaSuccess ? e : get(gsn.data(), w.gs, nd);
+    e = e != cudaSuccess ? e : get(morig.data(), w.morig, ni);
+    e = e != cudaSuccess ? e : get(amap.data(), w.amap, ni);
+    e = e != cudaSuccess ? e : get(gmark.data(), w.gmark, ni);
+    e = e != cudaSuccess ? e : get(gbase.data(), w.gbase, ni);
+    e = e != cudaSuccess ? e : get(zmap.data(), w.zmap, ni);
+    e = e != cudaSuccess ? e : get(pmap.data(), w.pmap, sizeof(int) * (size_t)L.np);
+    e = e != cudaSuccess ? e : get(nK.data(), w.nK, sizeof(int) * nodes);
+    e = e != cudaSuccess ? e : get(nKz.data(), w.nKz, sizeof(int) * nodes);
+    e = e != cudaSuccess ? e : get(nrho.data(), w.nrho, sizeof(double) * nodes);
+    e = e != cudaSuccess ? e : get(ntol.data(), w.ntol, sizeof(double) * nodes);
+    BRDC_CUDA(h, "brdc.merge_trace.copy", e);
+    BRDC_CUDA(h, "brdc.merge_trace.sync", cudaStreamSynchronize(h->stream));
+    for (int g = 0; g < nodes; ++g) {
+        long long gs = 0, m = 0;
+        walk_node(n, depth, g, &gs, &m);
+        const long long po = (gs + g + 1) & ~1LL;
+        const int K = nK[g], Kz = nKz[g];
+        if (K < 0 || Kz < K || Kz > m) {
+            set_error(h, 0, BRDC_ERROR_SRC_NONE, "brdc.merge_trace: no checkpoint of this level");
+            return BRDC_STATUS_INVALID_VALUE;
+        }
+        node_K[g] = K;
+        node_rho[g] = nrho[g];
+        node_tol[g] = ntol[g];
+        std::vector<int> pole_of_active(Kz, -1);
+        for (int j = 0; j < K; ++j) {
+            const int a = pmap[po + j];
+            if (a >= 0 && a < Kz) {
+                pole_of_active[a] = j;
+            }
+        }
+        for (long long p = 0; p < m; ++p) {
+            d[gs + p] = md[gs + p];
+            z[gs + p] = mz[gs + p];
+            row[gs + p] = morig[gs + p];
+            state[gs + p] = -1;
+            link[gs + p] = -1;
+            c[gs + p] = 0.0;
+            s[gs + p] = 0.0;
+        }
+        for (int a = 0; a < Kz; ++a) {
+            const long long p = gs + amap[gs + a];
+            if (gmark[gs + a]) {
+                state[p] = 2;
+                link[p] = amap[gs + gbase[gs + a]];
+                c[p] = gc[gs + a];
+                s[p] = gsn[gs + a];
+            } else {
+                state[p] = 0;
+                link[p] = pole_of_active[a];
+            }
+        }
+        for (long long q = 0; q < m - Kz; ++q) {
+            state[gs + zmap[gs + q]] = 1;
+        }
     }
     return BRDC_STATUS_SUCCESS;
 }

@@ -42,6 +42,12 @@ constexpr int kWarpMaxK = 2048;     // merges up to this K run one warp per item
 constexpr double kDeflTolScale = 8.0;  // tol = 8*eps*max(max|d|,max|z|)
                                         // (merge_kernels.cuh:9-11,1090-1091)
 constexpr unsigned kWsMagic = 0x42524443u; // "BRDC"
+// z of a merge is the children's boundary row divided by sqrt(2), as a
+// correctly rounded quotient by the correctly rounded sqrt(2), which is how
+// the reference forms it (gpu/src/tridiag_solver_merge_kernels.cuh:
+// 1075-1077): the same rows give the same z bit for bit, so the deflation
+// decisions can be compared with the reference's exactly.
+constexpr double kSqrt2 = 1.4142135623730951;
 
 inline int tree_levels(long long n) {
     if (n <= 16) {

@@ -527,7 +527,6 @@ __global__ void __launch_bounds__(256) k_merge(KArgs a, long long total_n) {
         return;
     }
     const Ws &w = a.w;
-    const double isq2 = 0.70710678118654752440;
     for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x; x < total_n;
          x += (long long)gridDim.x * blockDim.x) {
         int g, m, depth;
@@ -544,14 +543,14 @@ __global__ void __launch_bounds__(256) k_merge(KArgs a, long long total_n) {
         if (e < m1) {
             xv = Ad[e];
             pos = e + lower_bound_d(Bd, m2, xv);
-            z = w.cl[x] * isq2;
+            z = w.cl[x] / kSqrt2;
             f = w.cf[x];
             l = 0.0;
         } else {
             const int j = e - m1;
             xv = Bd[j];
             pos = j + upper_bound_d(Ad, m1, xv);
-            z = w.cf[x] * isq2;
+            z = w.cf[x] / kSqrt2;
             f = 0.0;
             l = w.cl[x];
         }

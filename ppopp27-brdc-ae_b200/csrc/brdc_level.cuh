@@ -330,7 +330,6 @@ __global__ void __launch_bounds__(T, 1) k_level(KArgs a) {
     const int x = threadIdx.x;
     constexpr int chunk = kDeflEPT * T;
     constexpr int B = kLvlBatch;
-    const double isq2 = 0.70710678118654752440;
     double rho, maxd;
     defl_node_scalars(a, G, &rho, &maxd);
 
@@ -351,7 +350,7 @@ __global__ void __launch_bounds__(T, 1) k_level(KArgs a) {
             const bool left = ee < m1;
             v[u] = w.cd[gs + ee];
             const double r = left ? w.cl[gs + ee] : w.cf[gs + ee];
-            z[u] = r * isq2;
+            z[u] = r / kSqrt2;
             f[u] = left ? w.cf[gs + ee] : 0.0;
             l[u] = left ? 0.0 : w.cl[gs + ee];
         }

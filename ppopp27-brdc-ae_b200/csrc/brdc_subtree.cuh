@@ -141,7 +141,6 @@ __global__ void __launch_bounds__(kSubRows, 512 / kSubRows) k_subtree(SubArgs A)
     const int warp = x >> 5, lane = x & 31;
     const double eps = DBL_EPSILON;
     const int max_iter = a.w.hdr->max_iter;
-    const double isq2 = 0.70710678118654752440;
 
     // subtree -> instance, its levels and rows
     int b = 0;
@@ -247,12 +246,12 @@ __global__ void __launch_bounds__(kSubRows, 512 / kSubRows) k_subtree(SubArgs A)
             double z, f, l;
             if (e < m1) {
                 pos = e + lower_bound_d(S.cd + s + m1, m - m1, v);
-                z = S.cl[x] * isq2;
+                z = S.cl[x] / kSqrt2;
                 f = S.cf[x];
                 l = 0.0;
             } else {
                 pos = (e - m1) + upper_bound_d(S.cd + s, m1, v);
-                z = S.cf[x] * isq2;
+                z = S.cf[x] / kSqrt2;
                 f = 0.0;
                 l = S.cl[x];
             }
@@ -657,6 +656,8 @@ __global__ void __launch_bounds__(kSubRows, 512 / kSubRows) k_subtree(SubArgs A)
             const int e = x - s;
             const int ndz = m - Kz, ndg = Kz - K;
             lw.morig[gs + e] = S.morig[x];
+            lw.md[gs + e] = S.md[x];
+            lw.mz[gs + e] = S.mz[x];
             if (e < Kz) {
                 lw.af[gs + e] = S.af[x];
                 lw.al[gs + e] = S.al[x];

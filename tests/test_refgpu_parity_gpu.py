@@ -1,6 +1,15 @@
-"""Per-level deflation counts against the reference CUDA prototype
-(gpu/src, built from source for sm_100a by oracle/build_ref.sh), and
-eigenvalue accuracy of both against the oracle.
+"""Deflation decisions, per-level counts and accuracy against the reference
+CUDA prototype (gpu/src, built from source for sm_100a by
+oracle/build_ref.sh).
+
+Decisions: at every merge of every level of this build's solve, the
+reference's own deflation kernels (oracle/ref_merge.cu: prepare/deflatezero,
+sortd, setcandflags, deflatecount, deflateapply) are handed exactly the
+inputs this build's merge saw -- the children's eigenvalues by row, the
+boundary rows that give this build's z, rho -- and must reach the same
+decisions bit for bit: the same tolerance, the same small-z deflations, the
+same close-pole chains with the same bases and Givens pairs, the same K and
+the same order of the secular poles.
 
 On tie-free inputs -- here random normal tridiagonals of orders where no
 |rho*z| or pole gap falls within rounding of the deflation tolerance --
@@ -13,6 +22,7 @@ import pytest
 
 import oracle
 import ref_gpu
+from brdc import families
 
 pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not ref_gpu.available(), reason="reference prototype not built")]
@@ -38,6 +48,143 @@ def run_both(solver, ref, d, e):
     torch.cuda.synchronize()
     theirs = ref.level_diagnostics()
     return W1.cpu().numpy(), W2.cpu().numpy(), ours, theirs
+
+
+def walk_node(n, depth, idx):
+    """(start, size) of node idx at the given depth of the split tree
+    (left child floor(s/2), right ceil(s/2))."""
+    s, st = n, 0
+    for bit in range(depth - 1, -1, -1):
+        h = s >> 1
+        if (idx >> bit) & 1:
+            st += h
+            s -= h
+        else:
+            s = h
+    return st, s
+
+
+def row_for_z(z):
+    """A boundary-row value r with r / sqrt(2) == z exactly (IEEE division,
+    as the reference forms z), so the reference's kernels see this build's z."""
+    r0 = z * np.sqrt(2.0)
+    out = r0.copy()
+    ok = (r0 / np.sqrt(2.0)) == z
+    for k in (1, -1, 2, -2, 3, -3):
+        cand = r0.copy()
+        for _ in range(abs(k)):
+            cand = np.nextafter(cand, np.inf if k > 0 else -np.inf)
+        hit = (~ok) & ((cand / np.sqrt(2.0)) == z)
+        out[hit] = cand[hit]
+        ok |= hit
+    assert ok.all()
+    return out
+
+
+def compare_level(tr, n, L, k):
+    """Decisions of this build's level-k merges (trace) against the
+    reference's deflation kernels on the same inputs.  Returns the counts
+    (small-z, rotated, poles) checked."""
+    depth = L - 1 - k
+    nodes = 1 << depth
+    D = np.zeros(n)
+    E = np.zeros(n)
+    first = np.zeros(n)
+    last = np.zeros(n)
+    sizes = []
+    geo = []
+    for g in range(nodes):
+        gs, m = walk_node(n, depth, g)
+        m1 = m >> 1
+        sizes += [m1, m - m1]
+        geo.append((gs, m, m1))
+        rows = tr["row"][gs:gs + m]
+        assert sorted(rows) == list(range(m))
+        D[gs + rows] = tr["d"][gs:gs + m]
+        rv = row_for_z(tr["z"][gs:gs + m])
+        left = rows < m1
+        last[gs + rows[left]] = rv[left]
+        first[gs + rows[~left]] = rv[~left]
+        E[gs + m1 - 1] = tr["rho"][g] / 2.0
+    R = ref_gpu.merge_level(sizes, D, E, first, last)
+    counts = [0, 0, 0]
+    for g, (gs, m, m1) in enumerate(geo):
+        rows = tr["row"][gs:gs + m]
+        pos_of_row = np.empty(m, dtype=np.int64)
+        pos_of_row[rows] = np.arange(m)
+        state = tr["state"][gs:gs + m]
+        link = tr["link"][gs:gs + m]
+        # tolerance and rho, bit for bit
+        assert R["tol"][gs] == tr["tol"][g], (k, g)
+        assert R["rho"][gs] == tr["rho"][g], (k, g)
+        # small-z decisions |rho z| <= tol (by row)
+        ours_small = np.zeros(m, dtype=bool)
+        ours_small[rows] = state == 1
+        assert np.array_equal(R["mask0"][gs:gs + m] == 0, ours_small), (k, g)
+        # close-pole chains: member row -> base row
+        ref_rot = {}
+        for q in range(gs, gs + m):
+            cnt = R["dcount"][q]
+            if cnt > 0:
+                base = R["map"][q] - gs
+                for j in range(1, cnt + 1):
+                    ref_rot[int(R["map"][q + j] - gs)] = int(base)
+        ours_rot = {int(rows[p]): int(rows[link[p]]) for p in np.nonzero(state == 2)[0]}
+        assert ref_rot == ours_rot, (k, g)
+        for r in ours_rot:
+            p = pos_of_row[r]
+            assert R["cc"][gs + r] == tr["c"][gs + p] and R["ss"][gs + r] == tr["s"][gs + p], (k, g, r)
+        # K and the order of the secular poles (ascending d)
+        act = np.nonzero(R["mask"][gs:gs + m] == 1)[0]
+        assert len(act) == tr["K"][g], (k, g)
+        ref_order = act[np.argsort(D[gs + act], kind="stable")]
+        ours_order = np.empty(len(act), dtype=np.int64)
+        poles = np.nonzero(state == 0)[0]
+        ours_order[link[poles]] = rows[poles]
+        assert np.array_equal(ref_order, ours_order), (k, g)
+        counts[0] += int(ours_small.sum())
+        counts[1] += len(ours_rot)
+        counts[2] += len(act)
+    return counts
+
+
+def trace_solve(solver, d, e):
+    import torch
+
+    n = len(d)
+    ws = solver.new_checkpoint_workspace(n)
+    solver.dstebr(torch.tensor(d, device="cuda"), torch.tensor(e, device="cuda"), workspace=ws)
+    L = solver.diagnostics(n, ws)["levels"]
+    return ws, L
+
+
+@pytest.mark.skipif(not ref_gpu.merge_available(), reason="reference deflation kernels not built")
+@pytest.mark.parametrize("n", [17, 31, 32, 33, 48, 64, 100, 128, 200, 256, 500, 512, 1000, 1024,
+                               2048, 4096, 8192, 16384])
+def test_decisions_match_reference_kernels_every_level(solver, n):
+    rng = np.random.default_rng(1000 + n)
+    d, e = rng.standard_normal(n), rng.standard_normal(n - 1)
+    ws, L = trace_solve(solver, d, e)
+    tot = np.zeros(3, dtype=np.int64)
+    for k in range(L):
+        tot += compare_level(solver.merge_trace(n, k, ws), n, L, k)
+    assert tot[2] > 0
+
+
+@pytest.mark.skipif(not ref_gpu.merge_available(), reason="reference deflation kernels not built")
+@pytest.mark.parametrize("family,n", [("toeplitz", 1024), ("toeplitz", 4096), ("clustered", 4096),
+                                      ("uniform", 16384)])
+def test_decisions_match_reference_kernels_families(solver, family, n):
+    """Ties (Toeplitz: every inner merge of identical children), heavy
+    small-z deflation (clustered) and a wide uniform spectrum: the rules and
+    their tie-breaks agree too."""
+    d, e = families.generate(family, n)
+    ws, L = trace_solve(solver, d, e)
+    tot = np.zeros(3, dtype=np.int64)
+    for k in range(L):
+        tot += compare_level(solver.merge_trace(n, k, ws), n, L, k)
+    if family == "toeplitz":
+        assert tot[1] > 0  # close-pole chains were exercised
 
 
 @pytest.mark.parametrize("n", [17, 32, 33, 48, 64, 100, 128, 200, 256, 512, 1000])
