@@ -1088,7 +1088,8 @@ def work_model(diag, fused):
     """Algorithmic FP64 work of the solve from the solver's own counters
     (a divide or square root counts as one flop, an FMA as two):
       leaf Jacobi     (12 s + 15) flops per rotation, s(s-1)/2 rotations a
-                      sweep, at the largest sweep count any leaf took
+                      sweep, summed over the leaves with the sweeps each
+                      leaf's half-warp ran
       secular         8 flops per pole-root pair and sweep; sweeps per root
                       = its iterations + the initial midpoint sweep
       Loewner         4 flops per pair (inner merges only)
@@ -1098,7 +1099,8 @@ def work_model(diag, fused):
     nlev = len(levels)
     leaves = diag["leaf_count"]
     s = 16
-    leaf = leaves * diag["leaf_sweeps_max"] * (s * (s - 1) / 2) * (12 * s + 15)
+    sweeps = diag.get("leaf_sweeps_sum") or leaves * diag["leaf_sweeps_max"]
+    leaf = sweeps * (s * (s - 1) / 2) * (12 * s + 15)
     per = []
     for k, lv in enumerate(levels):
         kk = max(lv["dd_after_sum"], 1)

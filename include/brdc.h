@@ -181,6 +181,7 @@ typedef struct brdc_diagnostics {
     int levels;
     int leaf_count;
     int leaf_sweeps_max;     /* Jacobi sweeps of the slowest leaf */
+    int leaf_sweeps_sum;     /* Jacobi sweeps summed over the leaves */
     brdc_level_diagnostics level[BRDC_MAX_LEVELS];
 } brdc_diagnostics;
 
@@ -356,7 +357,6 @@ brdc_status brdc_dstebr_batched_backward(brdc_handle handle, int64_t count,
                                          double *d_gD, double *d_gE, void *workspace,
                                          size_t workspace_size, int keep_forward);
 
-/* Library version string. */
 /* Eigenvalues and eigenvectors: the vector path of the reference's solver
  * (compute_eigenvectors = 1, gpu/src/tridiag_solver.cu:848-1071).  A
  * checkpointing values solve records every merge; each node's eigenvector
@@ -364,20 +364,20 @@ brdc_status brdc_dstebr_batched_backward(brdc_handle handle, int64_t count,
  * are children's eigenvectors (or short rotation combinations of them),
  * the K root eigenvectors blockdiag(Q_left, Q_right) * M_node[:, :K], M
  * built from the recorded permutations, rotations and secular vectors
- * (Loewner weights), the products by library FP64 GEMMs.  W[n] ascending,
- * Z column-major n x n (ld ldz >= n), column j the unit eigenvector of
- * W[j].  The workspace (query below) holds the checkpoints, M, the
- * products and two levels of eigenvector blocks, about 24 n^2 bytes;
- * n <= 32768.  It reads each level's largest K back once (a stream
- * synchronisation) to size the products; inside a graph capture it reads
- * nothing and multiplies every column instead (same result, more flops).
- * The first call on a handle creates its GEMM library handle, so make it
- * outside a capture. */
+ * (Loewner weights), the products by the library's own FP64 tensor-core
+ * kernel, which writes each root eigenvector straight to its place.
+ * W[n] ascending, Z column-major n x n (ld ldz >= n), column j the unit
+ * eigenvector of W[j].  The workspace (query below) holds the checkpoints,
+ * M and two levels of eigenvector blocks, about 16 n^2 bytes; n <= 32768.
+ * It reads each level's largest K back once (a stream synchronisation) to
+ * size the level's M; inside a graph capture it reads nothing and sizes it
+ * by the level's largest node instead (the same result). */
 brdc_status brdc_dstebr_vectors_workspace_size(int64_t n, size_t *bytes);
 brdc_status brdc_dstebr_vectors(brdc_handle handle, int64_t n, const double *d_D,
                                 const double *d_E, double *d_W, double *d_Z,
                                 int64_t ldz, void *workspace, size_t workspace_size);
 
+/* Library version string. */
 const char *brdc_version(void);
 
 #ifdef __cplusplus

@@ -104,6 +104,7 @@ class Diagnostics(ctypes.Structure):
         ("levels", ctypes.c_int),
         ("leaf_count", ctypes.c_int),
         ("leaf_sweeps_max", ctypes.c_int),
+        ("leaf_sweeps_sum", ctypes.c_int),
         ("level", LevelDiag * MAX_LEVELS),
     ]
 
@@ -113,6 +114,7 @@ class Diagnostics(ctypes.Structure):
             "levels": self.levels,
             "leaf_count": self.leaf_count,
             "leaf_sweeps_max": self.leaf_sweeps_max,
+            "leaf_sweeps_sum": self.leaf_sweeps_sum,
             "level": [],
         }
         for k in range(self.levels):

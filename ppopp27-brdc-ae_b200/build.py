@@ -50,7 +50,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     deps = _sources() + [os.path.join(HERE, "..", "include", h) for h in ("brdc.h", "brdc_lapack.h")] + [__file__]
     deps = [d for d in deps if not d.endswith(("host_check.cpp", "brdc_inputs.cpp"))]
     if force or _stale(LIB, deps):
-        cmd = [_nvcc(), *NVCC_FLAGS, "-o", LIB, os.path.join(CSRC, "brdc_capi.cu"), "-lcublas"]
+        cmd = [_nvcc(), *NVCC_FLAGS, "-o", LIB, os.path.join(CSRC, "brdc_capi.cu")]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
         subprocess.run(cmd, check=True)

@@ -8,7 +8,6 @@
 // so a solve can be captured in a CUDA graph.  Data-dependent sizes (deflation counts K) travel from kernel to
 // kernel through the workspace header; that replaces the per-level device
 // to host copy of the reference (gpu/src/tridiag_solver.cu:624-630).
-#include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -63,7 +62,6 @@ struct brdc_handle_struct {
     int timed_levels;
     int has_lowner[BRDC_MAX_LEVELS];
     int fused_levels;
-    cublasHandle_t blas = nullptr; // the eigenvector path's GEMMs, made on first use
 };
 
 namespace {
@@ -236,7 +234,9 @@ Layout plan_workspace(const HostForest &f, bool ckpt, void *base, Ws *w) {
     Layout L{};
     L.nt = f.total_n;
     L.nn0 = f.nn0;
-    L.np = f.total_n + f.nn0 + 4;
+    // even, so that every level's slice of a checkpointing workspace keeps
+    // the pole slices 16-byte aligned for the bulk copies
+    L.np = (f.total_n + f.nn0 + 4 + 1) & ~1LL;
     L.levels = f.max_levels;
     L.ckpt = ckpt;
     size_t cur = align_up(sizeof(WsHeader));
@@ -815,9 +815,6 @@ extern "C" brdc_status brdc_destroy(brdc_handle h) {
             cudaEventDestroy(e);
         }
     }
-    if (h->blas != nullptr) {
-        cublasDestroy(h->blas);
-    }
     if (h->prep_ev != nullptr) {
         cudaEventDestroy(h->prep_ev);
     }
@@ -1040,6 +1037,7 @@ extern "C" brdc_status brdc_get_diagnostics(brdc_handle h, const void *workspace
     out->levels = hd.max_levels;
     out->leaf_count = hd.leaf_count;
     out->leaf_sweeps_max = hd.leaf_sweeps_max;
+    out->leaf_sweeps_sum = hd.leaf_sweeps_sum;
     for (int k = 0; k < hd.max_levels && k < BRDC_MAX_LEVELS; ++k) {
         out->level[k] = hd.diag[k];
         out->level[k].level = k;
@@ -1921,7 +1919,7 @@ namespace {
 // products (n x Kmax each), the GEMM pointer tables, the row signs and the
 // per-level Kmax.
 struct VecLayout {
-    size_t ckpt, qa, qb, mm, cm, ptrs, sgn, kmax, total;
+    size_t ckpt, qa, qb, mm, sgn, kmax, rows, cnt, total;
 };
 
 VecLayout vec_layout(const HostForest &hf, long long n) {
@@ -1931,11 +1929,11 @@ VecLayout vec_layout(const HostForest &hf, long long n) {
     v.qa = align_up(half);
     v.qb = align_up(half);
     v.mm = align_up((size_t)n * (size_t)n * sizeof(double));
-    v.cm = v.mm;
-    v.ptrs = align_up(sizeof(double *) * 6 * (size_t)(hf.nn0 + 1));
     v.sgn = align_up(sizeof(double) * (size_t)n);
     v.kmax = align_up(sizeof(int) * (size_t)(hf.max_levels + 1));
-    v.total = v.ckpt + v.qa + v.qb + v.mm + v.cm + v.ptrs + v.sgn + v.kmax;
+    v.rows = align_up(sizeof(int) * (size_t)n);
+    v.cnt = align_up(sizeof(int) * 2 * (size_t)(hf.nn0 + 1));
+    v.total = v.ckpt + v.qa + v.qb + v.mm + v.sgn + v.kmax + v.rows + v.cnt;
     return v;
 }
 
@@ -1979,14 +1977,6 @@ extern "C" brdc_status brdc_dstebr_vectors(brdc_handle h, int64_t n, const doubl
         return BRDC_STATUS_INVALID_WORKSPACE;
     }
     cudaStream_t s = h->stream;
-    if (h->blas == nullptr) {
-        if (cublasCreate(&h->blas) != CUBLAS_STATUS_SUCCESS) {
-            h->blas = nullptr;
-            set_error(h, (int)cudaErrorUnknown, BRDC_ERROR_SRC_CUDA, "brdc.vectors.cublas_create");
-            return BRDC_STATUS_INTERNAL_ERROR;
-        }
-    }
-    cublasSetStream(h->blas, s);
     const Layout L = make_layout(hf, true);
     const Ws w = carve(workspace, hf, true);
     Forest F{};
@@ -2003,10 +1993,10 @@ extern "C" brdc_status brdc_dstebr_vectors(brdc_handle h, int64_t n, const doubl
     double *qa = reinterpret_cast<double *>(base);
     double *qb = reinterpret_cast<double *>(base + V.qa);
     double *M = reinterpret_cast<double *>(base + V.qa + V.qb);
-    double *Cm = reinterpret_cast<double *>(base + V.qa + V.qb + V.mm);
-    double **ptrs = reinterpret_cast<double **>(base + V.qa + V.qb + V.mm + V.cm);
-    double *sgn = reinterpret_cast<double *>(base + V.qa + V.qb + V.mm + V.cm + V.ptrs);
-    int *dkmax = reinterpret_cast<int *>(base + V.qa + V.qb + V.mm + V.cm + V.ptrs + V.sgn);
+    double *sgn = reinterpret_cast<double *>(base + V.qa + V.qb + V.mm);
+    int *dkmax = reinterpret_cast<int *>(base + V.qa + V.qb + V.mm + V.sgn);
+    int *vrows = reinterpret_cast<int *>(base + V.qa + V.qb + V.mm + V.sgn + V.kmax);
+    int *vcnt = reinterpret_cast<int *>(base + V.qa + V.qb + V.mm + V.sgn + V.kmax + V.rows);
     k_vec_signs<<<1, 1024, 0, s>>>(d_E, n, sgn);
     BRDC_CUDA(h, "brdc.vectors.signs", cudaGetLastError());
     const int Lv = hf.max_levels;
@@ -2047,7 +2037,6 @@ extern "C" brdc_status brdc_dstebr_vectors(brdc_handle h, int64_t n, const doubl
             kmax[k] = std::min(std::max(kmax[k], 0), (int)hf.level_mmax[k]);
         }
     }
-    const double one = 1.0, zero = 0.0;
     double *qprev = nullptr, *qcur = qa;
     long long prev_mmax = 16;
     for (int k = 0; k < Lv; ++k) {
@@ -2071,6 +2060,8 @@ extern "C" brdc_status brdc_dstebr_vectors(brdc_handle h, int64_t n, const doubl
         va.top = top ? 1 : 0;
         va.ldout = ldz;
         va.sgn = sgn;
+        va.rows = vrows;
+        va.cnt = vcnt;
         if (top) {
             k_vec_lowner<<<(unsigned)std::max<long long>(1, std::min<long long>((n + 7) / 8, h->sm_count * 8)),
                            256, 0, s>>>(va);
@@ -2089,66 +2080,19 @@ extern "C" brdc_status brdc_dstebr_vectors(brdc_handle h, int64_t n, const doubl
             prev_mmax = mmax;
             continue;
         }
-        // the roots: C = blockdiag(Q_left, Q_right) * M[:, :Kmax], two GEMMs
-        // per node, batched over the nodes of equal shape (tables built on
-        // the device), then each root column to its place
-        const int depth = Lv - 1 - k;
-        const int nodes = hf.level_nodes[k];
-        int msmall = 0, mlarge = 0, cs = 0, cl = 0;
-        for (int g = 0; g < nodes; ++g) {
-            long long st0 = 0, m = 0;
-            walk_node(n, depth, g, &st0, &m);
-            if (msmall == 0 || m < msmall) {
-                msmall = (int)m;
-            }
-            mlarge = std::max(mlarge, (int)m);
+        // the roots: blockdiag(Q_left, Q_right) * M[:, :K] per node over the
+        // surviving rows of M, each column written to its place (k_vec_gemm,
+        // FP64 tensor cores)
+        k_vec_rows<256><<<(unsigned)hf.level_nodes[k], 256, 0, s>>>(va);
+        BRDC_CUDA(h, "brdc.vectors.rows", cudaGetLastError());
+        {
+            const long long half_rows = (mmax + 1) / 2;
+            const dim3 grid((unsigned)((half_rows + kVgBM - 1) / kVgBM),
+                            (unsigned)((Km + kVgBN - 1) / kVgBN),
+                            (unsigned)(2 * hf.level_nodes[k]));
+            k_vec_gemm<<<grid, kVgThreads, 0, s>>>(va);
+            BRDC_CUDA(h, "brdc.vectors.gemm", cudaGetLastError());
         }
-        for (int g = 0; g < nodes; ++g) {
-            long long st0 = 0, m = 0;
-            walk_node(n, depth, g, &st0, &m);
-            ((int)m == msmall ? cs : cl) += 1;
-        }
-        VecTables vt{};
-        vt.n = n;
-        vt.depth = depth;
-        vt.nodes = nodes;
-        vt.msmall = msmall;
-        vt.cs = cs;
-        vt.cl = cl;
-        vt.off[0] = 0;
-        vt.off[1] = 3LL * cs;
-        vt.off[2] = 6LL * cs;
-        vt.off[3] = 6LL * cs + 3LL * cl;
-        vt.child = va.child;
-        vt.leafchild = va.leafchild;
-        vt.child_stride = prev_mmax;
-        vt.M = M;
-        vt.C = Cm;
-        vt.stride = va.mstride;
-        vt.tab = const_cast<const double **>(ptrs);
-        k_vec_tables<<<1, 1024, 0, s>>>(vt);
-        BRDC_CUDA(h, "brdc.vectors.tables", cudaGetLastError());
-        for (int grp = 0; grp < 4; ++grp) {
-            const int cnt = grp < 2 ? cs : cl;
-            if (cnt == 0) {
-                continue;
-            }
-            const int m = grp < 2 ? msmall : mlarge;
-            const int rows = (grp & 1) ? m - (m >> 1) : (m >> 1);
-            const int lda = (k == 0) ? 16 : rows;
-            double **dev = ptrs + vt.off[grp];
-            const cublasStatus_t bs = cublasDgemmBatched(
-                h->blas, CUBLAS_OP_N, CUBLAS_OP_N, rows, Km, rows, &one,
-                reinterpret_cast<const double *const *>(dev), lda,
-                reinterpret_cast<const double *const *>(dev + cnt), m, &zero, dev + 2 * cnt, m,
-                cnt);
-            if (bs != CUBLAS_STATUS_SUCCESS) {
-                set_error(h, (int)bs, BRDC_ERROR_SRC_CUDA, "brdc.vectors.gemm");
-                return BRDC_STATUS_INTERNAL_ERROR;
-            }
-        }
-        k_vec_scatter<<<(unsigned)eg, 256, 0, s>>>(va, Cm, n);
-        BRDC_CUDA(h, "brdc.vectors.scatter", cudaGetLastError());
         qprev = qcur;
         qcur = (qcur == qa) ? qb : qa;
         prev_mmax = mmax;

@@ -104,6 +104,7 @@ struct WsHeader {
     int leaf_sweeps_max;
     int leaf_count;
     int max_iter;    // iteration cap of one secular root (the handle's limit)
+    int leaf_sweeps_sum; // Jacobi sweeps summed over the leaves
     unsigned long long wait_ns; // bound of every device-side wait, in ns
     LevelCtl lvl[BRDC_MAX_LEVELS];
     brdc_level_diagnostics diag[BRDC_MAX_LEVELS];
@@ -571,6 +572,13 @@ __device__ inline void fence_mbar_init() {
 
 __device__ inline void fence_proxy_async() {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Orders this thread's view of global memory written through ordinary
+// stores (by this CTA or, after a cluster barrier, by its peers) before
+// bulk copies it issues next, which read through the async proxy.
+__device__ inline void fence_proxy_async_global() {
+    asm volatile("fence.proxy.async.global;" ::: "memory");
 }
 
 __device__ inline void mbar_expect_tx(uint64_t *bar, unsigned bytes) {

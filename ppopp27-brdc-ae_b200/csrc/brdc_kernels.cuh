@@ -424,7 +424,7 @@ __global__ void __launch_bounds__(kLeafWarps * 32)
     const int lane = threadIdx.x & 31;
     const int x = lane & 15;
     const int half = lane >> 4;
-    int sweeps_max = 0;
+    int sweeps_max = 0, sweeps_sum = 0;
     const long long pairs = (total_leaves + 1) / 2;
     for (long long pr = (long long)blockIdx.x * kLeafWarps + (threadIdx.x >> 5); pr < pairs;
          pr += (long long)gridDim.x * kLeafWarps) {
@@ -439,6 +439,7 @@ __global__ void __launch_bounds__(kLeafWarps * 32)
         double key, v[16];
         const int sweep = leaf_solve_full(a, G, s, x, &key, v);
         sweeps_max = sweeps_max > sweep ? sweeps_max : sweep;
+        sweeps_sum += (x == 0 && s > 0) ? sweep : 0;
         if (x < s) {
             const long long o = G.gstart + x;
             double vlast = 0.0;
@@ -457,8 +458,10 @@ __global__ void __launch_bounds__(kLeafWarps * 32)
             }
         }
     }
+    sweeps_sum = __reduce_add_sync(kFull, sweeps_sum);
     if (lane == 0 && sweeps_max > 0) {
         atomicMax(&a.w.hdr->leaf_sweeps_max, sweeps_max);
+        atomicAdd(&a.w.hdr->leaf_sweeps_sum, sweeps_sum);
     }
 }
 
@@ -471,7 +474,7 @@ __global__ void __launch_bounds__(kLeafWarps * 32)
     const int lane = threadIdx.x & 31;
     const int x = lane & 15;
     const int half = lane >> 4;
-    int sweeps_max = 0;
+    int sweeps_max = 0, sweeps_sum = 0;
     const long long pairs = (total_leaves + 1) / 2;
     for (long long pr = (long long)blockIdx.x * kLeafWarps + (threadIdx.x >> 5); pr < pairs;
          pr += (long long)gridDim.x * kLeafWarps) {
@@ -486,6 +489,7 @@ __global__ void __launch_bounds__(kLeafWarps * 32)
         double key, v0, v1;
         const int sweep = leaf_solve(a, G, s, x, &key, &v0, &v1);
         sweeps_max = sweeps_max > sweep ? sweeps_max : sweep;
+        sweeps_sum += (x == 0 && s > 0) ? sweep : 0;
         if (x < s) {
             const long long o = G.gstart + x;
             if (G.top) {
@@ -497,8 +501,10 @@ __global__ void __launch_bounds__(kLeafWarps * 32)
             }
         }
     }
+    sweeps_sum = __reduce_add_sync(kFull, sweeps_sum);
     if (lane == 0 && sweeps_max > 0) {
         atomicMax(&a.w.hdr->leaf_sweeps_max, sweeps_max);
+        atomicAdd(&a.w.hdr->leaf_sweeps_sum, sweeps_sum);
     }
 }
 
@@ -2131,6 +2137,7 @@ __global__ void k_init(WsHeader *h, int levels, int B, long long total_n,
         h->status = 0;
         h->nonconv = 0;
         h->leaf_sweeps_max = 0;
+        h->leaf_sweeps_sum = 0;
         h->max_iter = max_iter;
         h->wait_ns = wait_ns;
     }

@@ -43,6 +43,7 @@ struct LvlSmem {
     double s_val;                        // cluster exchange
     int s_cnt;
     int s_last;
+    uint64_t bar;                        // completion of the pole copies
 };
 
 // A sorted list in global memory with every Q-th element staged in shared
@@ -116,13 +117,33 @@ __device__ void level_roots(LvlSmem &S, cooperative_groups::cluster_group &cl, c
     const int x = threadIdx.x, lane = x & 31;
     const double eps = DBL_EPSILON;
     const int max_iter = a.w.hdr->max_iter;
-    for (int i = x; i < K; i += T) {
-        S.pd[i] = w.pd[po + i];
-        S.pz[i] = w.pz[po + i];
-        S.pf[i] = w.pf[po + i];
-        S.pl[i] = w.pl[po + i];
+    // The node's poles, weights and rows into shared memory by four bulk
+    // copies (cp.async.bulk, one thread issues them) completing on one
+    // mbarrier.  The pole slice starts 16-byte aligned; an odd K copies one
+    // element more, which the padded slice holds.  The cluster's deflation
+    // wrote these arrays with ordinary stores just before (released by the
+    // cluster barrier), hence the proxy fence before the copies.  A wait
+    // past the handle's limit is followed by a bounded drain, so the block
+    // never moves on with copies in flight; only a failed drain records an
+    // error.
+    {
+        const unsigned bytes = (unsigned)(((K + 1) & ~1) * sizeof(double));
+        if (x == 0) {
+            mbar_init(&S.bar, 1);
+            fence_mbar_init();
+            fence_proxy_async_global();
+            mbar_expect_tx(&S.bar, 4u * bytes);
+            bulk_g2s(S.pd, w.pd + po, bytes, &S.bar);
+            bulk_g2s(S.pz, w.pz + po, bytes, &S.bar);
+            bulk_g2s(S.pf, w.pf + po, bytes, &S.bar);
+            bulk_g2s(S.pl, w.pl + po, bytes, &S.bar);
+        }
+        __syncthreads();
+        if (!mbar_wait(&S.bar, 0u, w.hdr->wait_ns) && !mbar_wait(&S.bar, 0u, kDrainWaitNs)) {
+            record_error(w.hdr, kErrBarrierTimeout);
+        }
+        __syncthreads();
     }
-    __syncthreads();
     const int P = (K + C - 1) / C;
     const int r0 = min(K, rank * P), r1 = min(K, r0 + P);
     if (K == 1) {

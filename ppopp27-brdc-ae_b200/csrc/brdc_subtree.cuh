@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(kSubRows, 512 / kSubRows) k_subtree(SubArgs A)
             S.cl[r] = a.w.cl[gsub + r];
         }
     } else {
-        int sweeps_max = 0;
+        int sweeps_max = 0, sweeps_sum = 0;
         const int nleaves = 1 << Ls;
         const int xl = lane & 15, half = lane >> 4;
         for (int p0 = 2 * warp; p0 < nleaves; p0 += 2 * kSubWarps) {
@@ -201,6 +201,7 @@ __global__ void __launch_bounds__(kSubRows, 512 / kSubRows) k_subtree(SubArgs A)
             double key, v0, v1;
             const int sw = leaf_solve(a, LG, s, xl, &key, &v0, &v1);
             sweeps_max = sweeps_max > sw ? sweeps_max : sw;
+            sweeps_sum += (xl == 0 && s > 0) ? sw : 0;
             if (xl < s) {
                 const int o = (int)(LG.gstart - gsub) + xl;
                 if (LG.top) {
@@ -212,8 +213,10 @@ __global__ void __launch_bounds__(kSubRows, 512 / kSubRows) k_subtree(SubArgs A)
                 }
             }
         }
+        sweeps_sum = __reduce_add_sync(kFull, sweeps_sum);
         if (lane == 0 && sweeps_max > 0) {
             atomicMax(&a.w.hdr->leaf_sweeps_max, sweeps_max);
+            atomicAdd(&a.w.hdr->leaf_sweeps_sum, sweeps_sum);
         }
     }
     __syncthreads();

@@ -20,7 +20,8 @@
 // columns, which is the chains undone on the rows: the row operations of
 // the adjoint's chain reversal.  Rows map to child coordinates through
 // amap/zmap (list -> merged position) and morig (merged position -> child
-// eigenvalue index).  The two products per node are library FP64 GEMMs.
+// eigenvalue index).  The two products per node run in k_vec_gemm below, on
+// the FP64 tensor cores, each root column written straight to its place.
 #pragma once
 
 #include "brdc_kernels.cuh"
@@ -48,6 +49,11 @@ struct VArgs {
     // the top level writes T's eigenvectors: row i times the sign s_i of
     // T = S |T| S (k_vec_signs)
     const double *sgn;
+    // per node and half: the child eigenvector indices (rows of M) that
+    // survived the small-z test, in ascending order (k_vec_rows), at
+    // rows + gstart + (half ? m1 : 0), and their count at cnt[2 g + half]
+    int *rows;
+    int *cnt;
 };
 
 // Loewner weights of the instance-root merges, which the values solve
@@ -230,35 +236,209 @@ __global__ void __launch_bounds__(256) k_vec_build(VArgs a, long long total_n) {
     }
 }
 
-// Root eigenvectors from the products (node's block of C, columns in root
-// order) to their places in the node's ascending order: one warp per root.
-__global__ void __launch_bounds__(256) k_vec_scatter(VArgs a, const double *C, long long total_n) {
+// ------------------------------------------------------------ products
+// Rows of M that can be nonzero in a root column: the small-z survivors
+// (the secular poles and the members rotated into them), as child
+// eigenvector indices, split by half and kept in ascending order.  One CTA
+// per node.  Every other row of a root column is zero, as LAPACK DLAED3
+// uses the deflation (it multiplies only the non-deflated columns of Q).
+template <int T>
+__global__ void __launch_bounds__(T) k_vec_rows(VArgs a) {
     if (halted(a.w.hdr)) {
         return;
     }
+    __shared__ int iscan[32];
     const Ws &w = a.w;
-    const int lane = threadIdx.x & 31;
-    const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
-    for (long long x = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); x < total_n;
-         x += warps) {
-        int g, m, depth;
-        long long gs;
-        if (!elem_node(a.F, a.k, x, &g, &gs, &m, &depth)) {
+    const int g = blockIdx.x;
+    const NodeGeom G = node_geom(a.F, a.k, g);
+    const long long gs = G.gstart;
+    const int Kz = w.nKz[g];
+    int carry_l = 0, carry_r = 0;
+    for (int base = 0; base < Kz; base += T) {
+        const int i = base + threadIdx.x;
+        const int row = i < Kz ? vec_row_active(w, gs, i) : 0;
+        const bool right = row >= G.m1;
+        int tot;
+        const int ex = block_exscan<T>(i < Kz && !right ? 1 : 0, iscan, &tot);
+        if (i < Kz) {
+            if (!right) {
+                a.rows[gs + carry_l + ex] = row;
+            } else {
+                a.rows[gs + G.m1 + carry_r + (i - base - ex)] = row - G.m1;
+            }
+        }
+        carry_l += tot;
+        carry_r += min(T, Kz - base) - tot;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        a.cnt[2 * g] = carry_l;
+        a.cnt[2 * g + 1] = carry_r;
+    }
+}
+
+// The root eigenvectors of every node of a level, in one launch:
+//   Q_node[:, pos(s)] = blockdiag(Q_left, Q_right) * M_node[:, s],  s < K_node,
+// as two products per node (top rows with the left child's eigenvector
+// block, bottom rows with the right child's), each column written straight
+// to its place pos(s) in the node's ascending order (the top level also
+// applies the signs of E), so no intermediate product or scatter pass
+// exists.  Only the node's own K columns are multiplied, and the inner
+// dimension runs over the half's small-z survivors alone (k_vec_rows: the
+// only rows of M a root column can have nonzero), gathering those columns
+// of the child block and rows of M.  FP64 tensor-core MMA (mma.sync m8n8k4
+// .f64, fed from shared memory), 64 x 64 tiles of the output per CTA of
+// four warps (32 x 32 each), 16-deep slices of the inner dimension staged
+// by cp.async in two buffers.  Grid: x row tiles, y column tiles,
+// z = 2 * node + half; tiles past a node's rows or K return at once.
+constexpr int kVgBM = 64, kVgBN = 64, kVgBK = 16, kVgPad = 4, kVgThreads = 128;
+
+struct VgSmem {
+    // A slice stored k-major (t, r) and B slice (t, s): a warp's fragment
+    // loads then touch 16 distinct 8-byte banks per half-warp (row stride
+    // 68 doubles = 4 mod 16)
+    double A[2][kVgBK][kVgBM + kVgPad];
+    double B[2][kVgBK][kVgBN + kVgPad];
+    double *dst[kVgBN];
+};
+
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem, bool valid) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(smem_u32(smem)),
+                 "l"(gmem), "r"(valid ? 8 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// D = A B + D for one 8x8x4 FP64 tile: lane holds a = A[lane/4][lane%4],
+// b = B[lane%4][lane/4], c = D[lane/4][2(lane%4) + {0, 1}].
+__device__ __forceinline__ void dmma884(double (&c)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(c[0]), "+d"(c[1])
+                 : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(kVgThreads) k_vec_gemm(VArgs a) {
+    if (halted(a.w.hdr)) {
+        return;
+    }
+    const int g = (int)(blockIdx.z >> 1), half = (int)(blockIdx.z & 1);
+    if (g >= a.nodes) {
+        return;
+    }
+    const Ws &w = a.w;
+    const NodeGeom G = node_geom(a.F, a.k, g);
+    const int K = w.nK[g];
+    const int rows = half ? G.m - G.m1 : G.m1;
+    const int r0 = (int)blockIdx.x * kVgBM, s0 = (int)blockIdx.y * kVgBN;
+    if (r0 >= rows || s0 >= K) {
+        return;
+    }
+    const long long gs = G.gstart;
+    const int roff = half ? G.m1 : 0;
+    const double *A = a.leafchild ? a.child + (gs + roff) * 16 : a.child + (gs + roff) * a.child_stride;
+    const long long lda = a.leafchild ? 16 : rows;
+    const double *B = a.M + gs * a.mstride + roff;
+    const long long ldb = G.m;
+    const int *tl = a.rows + gs + roff;   // inner indices: the half's survivors
+    const int nin = a.cnt[2 * g + half];
+    __shared__ __align__(16) VgSmem S;
+    const int tid = threadIdx.x;
+    if (tid < kVgBN) {
+        const int s = s0 + tid;
+        double *d = nullptr;
+        if (s < K) {
+            const int Kz = w.nKz[g];
+            const int pos = vec_pos(w, gs, G.poff, s, K, G.m - Kz, Kz - K);
+            d = a.top ? a.out + (long long)pos * a.ldout + roff
+                      : a.out + gs * a.out_stride + (long long)pos * G.m + roff;
+        }
+        S.dst[tid] = d;
+    }
+    auto load = [&](int st, int j0) {
+#pragma unroll
+        for (int q = 0; q < kVgBK * kVgBM / kVgThreads; ++q) {
+            const int i = tid + q * kVgThreads;
+            const int r = i % kVgBM, j = i / kVgBM;
+            const bool v = (r0 + r < rows) && (j0 + j < nin);
+            const int t = v ? tl[j0 + j] : 0;
+            cp_async8(&S.A[st][j][r], v ? A + (r0 + r) + (long long)t * lda : A, v);
+        }
+#pragma unroll
+        for (int q = 0; q < kVgBK * kVgBN / kVgThreads; ++q) {
+            const int i = tid + q * kVgThreads;
+            const int j = i % kVgBK, c = i / kVgBK;
+            const bool v = (j0 + j < nin) && (s0 + c < K);
+            const int t = v ? tl[j0 + j] : 0;
+            cp_async8(&S.B[st][j][c], v ? B + t + (long long)(s0 + c) * ldb : B, v);
+        }
+        cp_async_commit();
+    };
+    const int lane = tid & 31, wid = tid >> 5;
+    const int wr = (wid >> 1) * 32, wc = (wid & 1) * 32;
+    const int gid = lane >> 2, tig = lane & 3;
+    double acc[4][4][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            acc[i][j][0] = 0.0;
+            acc[i][j][1] = 0.0;
+        }
+    }
+    const int nk = (nin + kVgBK - 1) / kVgBK;
+    if (nk > 0) {
+        load(0, 0);
+    }
+    __syncthreads(); // S.dst, for an empty inner dimension too
+    for (int kt = 0; kt < nk; ++kt) {
+        if (kt + 1 < nk) {
+            load((kt + 1) & 1, (kt + 1) * kVgBK);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const int st = kt & 1;
+#pragma unroll
+        for (int kk = 0; kk < kVgBK; kk += 4) {
+            double af[4], bf[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                af[i] = S.A[st][kk + tig][wr + i * 8 + gid];
+                bf[i] = S.B[st][kk + tig][wc + i * 8 + gid];
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    dmma884(acc[i][j], af[i], bf[j]);
+                }
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int r = r0 + wr + i * 8 + gid;
+        if (r >= rows) {
             continue;
         }
-        const long long po = (gs + g + 1) & ~1LL;
-        const int s = (int)(x - gs);
-        const int K = w.nK[g];
-        if (s >= K) {
-            continue;
-        }
-        const int Kz = w.nKz[g];
-        const int pos = vec_pos(w, gs, po, s, K, m - Kz, Kz - K);
-        const double *src = C + gs * a.mstride + (long long)s * m;
-        double *dst = a.top ? a.out + (long long)pos * a.ldout
-                            : a.out + gs * a.out_stride + (long long)pos * m;
-        for (int r = lane; r < m; r += 32) {
-            dst[r] = a.top ? src[r] * a.sgn[r] : src[r];
+        const double sg = a.top ? a.sgn[roff + r] : 1.0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                double *d = S.dst[wc + j * 8 + 2 * tig + e];
+                if (d != nullptr) {
+                    d[r] = acc[i][j][e] * sg;
+                }
+            }
         }
     }
 }
@@ -274,60 +454,6 @@ __global__ void __launch_bounds__(256) k_vec_kmax(const int *nK, int nodes, int 
     }
     if ((threadIdx.x & 31) == 0) {
         atomicMax(kmax, mx);
-    }
-}
-
-// GEMM pointer tables of one level, written on the device so the level's
-// products need nothing from the host: nodes have at most two sizes per
-// level (the tree splits floor/ceil), so the shapes fall in up to four
-// groups -- (top half, bottom half) x (smaller, larger node) -- each stored
-// as A[cnt], B[cnt], C[cnt] from tab + off[group], a node's slot being its
-// rank among the level's nodes of its size.  B (the node's root columns of
-// M) and C (their products) sit at gstart * stride, ld m.
-struct VecTables {
-    long long n;
-    int depth, nodes;
-    int msmall, cs, cl; // smaller node size, nodes of each size
-    long long off[4];
-    const double *child; // the leaves' eigenvectors (ld 16) or the level below's blocks
-    int leafchild;
-    long long child_stride; // mmax of the level below
-    const double *M;
-    double *C;
-    long long stride;
-    const double **tab;
-};
-
-__global__ void __launch_bounds__(1024) k_vec_tables(VecTables t) {
-    __shared__ int iscan[32];
-    int carry = 0;
-    for (int base = 0; base < t.nodes; base += 1024) {
-        const int g = base + threadIdx.x;
-        long long st = 0, m = 0;
-        if (g < t.nodes) {
-            walk_node(t.n, t.depth, g, &st, &m);
-        }
-        const int small = (g < t.nodes && (int)m == t.msmall) ? 1 : 0;
-        int tot;
-        const int ex = block_exscan<1024>(small, iscan, &tot);
-        if (g < t.nodes) {
-            const int rs = carry + ex;
-            const int idx = small ? rs : g - rs;
-            const int cnt = small ? t.cs : t.cl;
-            const long long h1 = m >> 1;
-            for (int half = 0; half < 2; ++half) {
-                const long long cst = st + (half ? h1 : 0);
-                const double *A = t.leafchild ? t.child + cst * 16 : t.child + cst * t.child_stride;
-                const double *B = t.M + st * t.stride + (half ? h1 : 0);
-                double *C = t.C + st * t.stride + (half ? h1 : 0);
-                const long long o = t.off[(small ? 0 : 2) + half];
-                t.tab[o + idx] = A;
-                t.tab[o + cnt + idx] = B;
-                t.tab[o + 2 * cnt + idx] = C;
-            }
-        }
-        carry += tot;
-        __syncthreads();
     }
 }
 

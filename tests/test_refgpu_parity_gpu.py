@@ -200,6 +200,65 @@ def test_deflation_counts_match_on_tie_free_inputs(solver, ref, n):
         assert lo["dd_after_sum"] == lt["dd_after_sum"], k
 
 
+def near_threshold(tr, n, L, k, band=4.0):
+    """This build's decisions at level k that sit within a factor `band` of
+    the deflation tolerance: small-z tests with tol/band <= |rho z| <=
+    band*tol, and gaps between consecutive small-z survivors with
+    tol/band <= gap <= band*tol.  Only these can flip when the merge inputs
+    move by rounding."""
+    depth = L - 1 - k
+    nz = ng = 0
+    for g in range(1 << depth):
+        gs, m = walk_node(n, depth, g)
+        tol, rho = tr["tol"][g], tr["rho"][g]
+        z = tr["z"][gs:gs + m]
+        r = np.abs(rho * z) / tol
+        nz += int(np.count_nonzero((r >= 1.0 / band) & (r <= band)))
+        st = tr["state"][gs:gs + m]
+        act = np.sort(tr["d"][gs:gs + m][st != 1])
+        gap = np.diff(act) / tol
+        ng += int(np.count_nonzero((gap >= 1.0 / band) & (gap <= band)))
+    return nz, ng
+
+
+@pytest.mark.parametrize("family,n", [("uniform", 4096), ("normal", 4096), ("uniform", 16384),
+                                      ("normal", 16384)])
+def test_counts_differ_only_by_near_threshold_decisions(solver, ref, family, n):
+    """End to end, the two solvers feed their merges slightly different data,
+    so per-level counts may differ -- but only through decisions within
+    rounding of the tolerance.  The prototype's leaves stop at an absolute
+    off-diagonal of 1e-12 (gpu/src/tridiag_solver_leaf.cuh:56-123), which
+    on a matrix of norm ~4 leaves its boundary rows, and so z, wrong by far
+    more than rounding; it is therefore run on the same matrix scaled by
+    2^13 (exactly: every decision of its merges scales with it, its leaves
+    become accurate to rounding).  The remaining differences come from the
+    rows' z mode (this build forms boundary rows from the Loewner weights,
+    the prototype's values path from the original z: SURVEY note N1) and
+    rounding, and every level's difference is bounded by this build's
+    decisions within a factor 4 of tol."""
+    import torch
+
+    d, e = families.generate(family, n)
+    ws, L = trace_solve(solver, d, e)
+    ours = solver.diagnostics(n, ws)
+    sc = 2.0 ** 13
+    D = torch.tensor(d * sc, device="cuda")
+    E = torch.tensor(e * sc, device="cuda")
+    W2 = torch.empty_like(D)
+    ref.solve(D, E, W2, diagnostics=True)
+    torch.cuda.synchronize()
+    theirs = ref.level_diagnostics()
+    assert len(theirs) == L
+    report = []
+    for k, (lo, lt) in enumerate(zip(ours["level"], theirs)):
+        nz, ng = near_threshold(solver.merge_trace(n, k, ws), n, L, k)
+        db = abs(lo["dd_before_sum"] - lt["dd_before_sum"])
+        da = abs(lo["dd_after_sum"] - lt["dd_after_sum"])
+        report.append((k, db, da, nz, ng))
+        assert db <= nz, report
+        assert da <= nz + ng, report
+
+
 @pytest.mark.parametrize("n", [4096, 16384])
 def test_accuracy_not_worse_than_prototype(solver, ref, n):
     rng = np.random.default_rng(n + 7)
@@ -210,6 +269,3 @@ def test_accuracy_not_worse_than_prototype(solver, ref, n):
     err_ours = np.max(np.abs(w1 - r)) / s
     err_ref = np.max(np.abs(w2 - r)) / s
     assert err_ours <= max(err_ref, 1e-14)
-    # near-threshold decisions may flip; the totals stay within 1% per level
-    for lo, lt in zip(ours["level"], theirs):
-        assert abs(lo["dd_after_sum"] - lt["dd_after_sum"]) <= 0.01 * n
