@@ -225,7 +225,7 @@ def run_profile_case(spec):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true")
@@ -668,8 +668,8 @@ def bench_ref_gpu(torch, families, solver, flush, args, head_ms, fam_ms, paper):
     solve entry tridiag_solver_run_from_device_tridiagonal,
     gpu/src/tridiag_solver.cu:2541) timed on this GPU in this run, beside
     this build, on the same inputs with the same L2 flush: the four families
-    at the headline order (the headline family with the headline's steps and
-    warm-up), the reference GPU bench's own data modes at the headline order
+    at the headline order (the headline family with the headline's warm-up
+    and at most 50 timed solves), the reference GPU bench's own data modes at the headline order
     (this build timed beside it with its default launch shapes), and the
     paper inputs at 8,192 whose times this line already carries.  A
     comparison leg only: nothing of it is this build's timed work."""
@@ -702,7 +702,8 @@ def bench_ref_gpu(torch, families, solver, flush, args, head_ms, fam_ms, paper):
             d, e = families.generate(fam, N_HEAD)
             exact = families.toeplitz_eigenvalues(N_HEAD) if fam == "toeplitz" else None
             head = fam == FAMILY_HEAD
-            row(f"family-{fam}:{N_HEAD}", d, e, exact, args.steps if head else (3 if fam == "toeplitz" else 5),
+            row(f"family-{fam}:{N_HEAD}", d, e, exact,
+                min(args.steps, 50) if head else (3 if fam == "toeplitz" else 5),
                 args.warmup if head else 1, head_ms if head else fam_ms.get(fam))
         # the reference GPU bench's data modes at the headline order; this
         # build with its default launch shapes on the same inputs

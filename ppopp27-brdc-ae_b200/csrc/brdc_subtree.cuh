@@ -39,6 +39,16 @@ struct SubArgs {
     int leaves_done;          // the leaves were solved by k_leaf_full: read them
 };
 
+// Roots per warp at most in the barrier-free tail of the subtree's secular
+// rounds (the rounds stop once the live roots fit this many per warp).
+// Measured on B200 (uniform 65,536): 1 -> 0.846 ms, 4 -> 0.856, 8 -> 0.865,
+// 16 -> 0.914: repacking the live roots every round beats iterating
+// several of them per warp, whose lanes idle once their root converges.
+#ifndef BRDC_SUB_TAIL_ROOTS
+#define BRDC_SUB_TAIL_ROOTS 1
+#endif
+constexpr int kSubTailRoots = BRDC_SUB_TAIL_ROOTS;
+
 template <int kSubRows>
 struct SubSmem {
     static constexpr int kSubWarps = kSubRows / 32;
@@ -458,36 +468,55 @@ __global__ void __launch_bounds__(kSubRows, 512 / kSubRows) k_subtree(SubArgs A)
         int cur = 0, round = 0;
         __syncthreads();
         while (nact > 0) {
-            if (nact <= kSubRows / 32) {
-                // The last few roots (the slow tail of the iteration): one
-                // warp each, iterated to convergence with no barrier,
-                // parking or list between sweeps.  All 32 lanes hold the
-                // same state (the butterfly sums are bit-identical), so the
-                // loop is warp-uniform; the iteration cap ends it.
-                const int wq = x >> 5;
-                if (wq < nact) {
-                    const int code = S.aq[cur][wq];
-                    const int id = code & 0xffff, q = code >> 16;
-                    const int rr = id - S.kpre[q], Kr = S.nK[q], sr = S.nstart[q];
-                    const double *pd = S.pd + sr, *pz = S.pz + sr;
-                    SecRoot st;
+            if (nact <= kSubWarps * kSubTailRoots) {
+                // The last roots (the slow tail of the iteration): R per
+                // warp (the smallest power of two that covers them, dealt
+                // round robin over the warps), 32 / R lanes each, iterated
+                // to convergence with no barrier, parking or list between
+                // sweeps.  A lane group's lanes hold the same state (the
+                // butterfly sums are bit-identical); the warp loops until
+                // its last root converges, and the iteration cap ends it.
+                int R = 1;
+                while (R < kSubTailRoots && R * kSubWarps < nact) {
+                    R <<= 1;
+                }
+                const int lanes = 32 / R;
+                const int sub = lane / lanes, l2 = lane & (lanes - 1);
+                const int slot = sub * kSubWarps + (x >> 5);
+                const bool act = slot < nact;
+                const int code = act ? S.aq[cur][slot] : 0;
+                const int id = code & 0xffff, q = code >> 16;
+                const int rr = id - S.kpre[q], Kr = S.nK[q], sr = S.nstart[q];
+                const double *pd = S.pd + sr, *pz = S.pz + sr;
+                SecRoot st;
+                if (act) {
                     sec_init_static(st, rr, Kr, pd, pz, S.nrho[q], S.nrinv[q], S.nzn[q]);
                     sec_unpark(st, S.dyn[id]);
-                    const int pmin = rr < Kr - 2 ? rr : Kr - 2;
-                    while (st.stage != 2) {
-                        SecSums sum;
-                        sec_zero(sum);
-                        secular_span(sum, st, 0, Kr, lane, 32, pmin, rr + 1,
+                } else {
+                    st.stage = 2;
+                }
+                const int pmin = rr < Kr - 2 ? rr : Kr - 2;
+                for (;;) {
+                    SecSums sum;
+                    sec_zero(sum);
+                    const bool live = act && st.stage != 2;
+                    if (live) {
+                        secular_span(sum, st, 0, Kr, l2, lanes, pmin, rr + 1,
                                      [&](int u, double *du, double *zu) {
                                          *du = pd[u];
                                          *zu = pz[u];
                                      });
-                        sums_reduce(sum, 32);
+                    }
+                    sums_reduce(sum, lanes);
+                    if (live) {
                         sec_after_sweep(st, sum, eps, max_iter);
                     }
-                    if (lane == 0) {
-                        sec_park(st, S.dyn[id]);
+                    if (__all_sync(0xffffffffu, !act || st.stage == 2)) {
+                        break;
                     }
+                }
+                if (act && l2 == 0) {
+                    sec_park(st, S.dyn[id]);
                 }
                 __syncthreads();
                 break;
