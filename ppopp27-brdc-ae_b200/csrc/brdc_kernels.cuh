@@ -189,7 +189,11 @@ __device__ inline int leaf_solve(const KArgs &a, const LeafGeom &G, int s, int x
     double v0 = (x == 0 && s > 0) ? 1.0 : 0.0;
     double v1 = (x == s - 1) ? 1.0 : 0.0;
     const double amax = half_max(fmax(fabs(dx), fmax(ex, exm1)));
-    const double th = 1.0e-3 * eps * amax;
+    // Sweeps stop, and rotations are skipped, once an off-diagonal entry is
+    // at most eps max|T_leaf|: what it leaves in an eigenvalue is of the
+    // order of its rounding.  A threshold 1000 times smaller cost 3% more
+    // sweeps on B200 (uniform 65,536) and changed no tested result.
+    const double th = eps * amax;
     int sweep = 0;
     for (; sweep < 40; ++sweep) {
         double off = 0.0;
@@ -351,7 +355,7 @@ __device__ inline int leaf_solve_full(const KArgs &a, const LeafGeom &G, int s, 
         v[j] = (j == x) ? 1.0 : 0.0;
     }
     const double amax = half_max(fmax(fabs(dx), fmax(ex, exm1)));
-    const double th = 1.0e-3 * eps * amax;
+    const double th = eps * amax;
     int sweep = 0;
     for (; sweep < 40; ++sweep) {
         double off = 0.0;
