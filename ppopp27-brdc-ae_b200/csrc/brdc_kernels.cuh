@@ -852,9 +852,11 @@ __device__ int defl_compact_active(const Ws &w, long long gs, int r0, int r1, do
 
 // Close-pole clusters whose run starts at an active index in [i0, i1): one
 // thread walks each run of gaps <= tol (it may read and rotate entries past
-// i1; no other thread touches them).
+// i1; no other thread touches them).  Returns whether this thread rotated
+// any entry out.
 template <int T>
-__device__ void defl_close_walk(const Ws &w, long long gs, int Kz, double tol, int i0, int i1) {
+__device__ bool defl_close_walk(const Ws &w, long long gs, int Kz, double tol, int i0, int i1) {
+    bool rotated = false;
     for (int i = i0 + threadIdx.x; i < i1; i += T) {
         const double di = w.ad[gs + i];
         const bool nxt = (i + 1 < Kz) && (w.ad[gs + i + 1] - di <= tol);
@@ -899,12 +901,14 @@ __device__ void defl_close_walk(const Ws &w, long long gs, int Kz, double tol, i
             w.gs[gs + x] = s;
             w.gr[gs + x] = r;
             w.gbase[gs + x] = base;
+            rotated = true;
             ++x;
         }
         w.az[gs + base] = zb;
         w.af[gs + base] = fb;
         w.al[gs + base] = lb;
     }
+    return rotated;
 }
 
 // Active entries [r0, r1) that remain poles (not rotated out).
@@ -1087,6 +1091,7 @@ __global__ void __launch_bounds__(T) k_merge_deflate_cl(KArgs a) {
     __shared__ int s_last;
     __shared__ double s_val;
     __shared__ int s_cnt;
+    __shared__ int s_rot;
     cg::cluster_group cl = cg::this_cluster();
     const int C = (int)cl.num_blocks();
     const int rank = (int)cl.block_rank();
@@ -1135,22 +1140,35 @@ __global__ void __launch_bounds__(T) k_merge_deflate_cl(KArgs a) {
 
     // close-pole walk over this CTA's share of chain starts
     const int A = (Kz + C - 1) / C;
-    defl_close_walk<T>(w, gs, Kz, tol, min(Kz, rank * A), min(Kz, rank * A + A));
-    cl.sync();
-
-    // compaction 2
-    const int S2 = ((Kz + C - 1) / C + chunk - 1) / chunk * chunk;
-    const int q0 = min(Kz, rank * S2), q1 = min(Kz, q0 + S2);
-    const int np = defl_count_poles<T>(w, gs, q0, q1, iscan);
+    const int rot = __syncthreads_or(
+        defl_close_walk<T>(w, gs, Kz, tol, min(Kz, rank * A), min(Kz, rank * A + A)));
     if (threadIdx.x == 0) {
-        s_cnt = np;
+        s_rot = rot;
     }
     cl.sync();
-    int off_p = 0, K = 0;
+    bool any_rot = false;
     for (int r = 0; r < C; ++r) {
-        const int c = *cl.map_shared_rank(&s_cnt, r);
-        off_p += r < rank ? c : 0;
-        K += c;
+        any_rot |= *cl.map_shared_rank(&s_rot, r) != 0;
+    }
+
+    // compaction 2 (with nothing rotated out, every active entry is a pole
+    // and no count is needed)
+    const int S2 = ((Kz + C - 1) / C + chunk - 1) / chunk * chunk;
+    const int q0 = min(Kz, rank * S2), q1 = min(Kz, q0 + S2);
+    int off_p = q0, K = Kz;
+    if (any_rot) {
+        const int np = defl_count_poles<T>(w, gs, q0, q1, iscan);
+        if (threadIdx.x == 0) {
+            s_cnt = np;
+        }
+        cl.sync();
+        off_p = 0;
+        K = 0;
+        for (int r = 0; r < C; ++r) {
+            const int c = *cl.map_shared_rank(&s_cnt, r);
+            off_p += r < rank ? c : 0;
+            K += c;
+        }
     }
     int end_p;
     double zn = defl_compact_poles<T>(w, gs, G.poff, q0, q1, off_p, q0 - off_p, iscan, &end_p);

@@ -42,6 +42,7 @@ struct LvlSmem {
     int iscan[32];
     double s_val;                        // cluster exchange
     int s_cnt;
+    int s_rot;                           // this CTA rotated close poles out
     int s_last;
     uint64_t bar;                        // completion of the pole copies
 };
@@ -437,21 +438,35 @@ __global__ void __launch_bounds__(T, 1) k_level(KArgs a) {
         defl_compact_active<T>(w, gs, r0, r1, rho, tol, off_a, r0 - off_a, S.iscan);
         cl.sync();
         const int A = (Kz + C - 1) / C;
-        defl_close_walk<T>(w, gs, Kz, tol, min(Kz, rank * A), min(Kz, rank * A + A));
-        cl.sync();
-        const int S2 = ((Kz + C - 1) / C + chunk - 1) / chunk * chunk;
-        const int q0 = min(Kz, rank * S2), q1 = min(Kz, q0 + S2);
-        const int np = defl_count_poles<T>(w, gs, q0, q1, S.iscan);
+        const int rot = __syncthreads_or(
+            defl_close_walk<T>(w, gs, Kz, tol, min(Kz, rank * A), min(Kz, rank * A + A)));
         if (x == 0) {
-            S.s_cnt = np;
+            S.s_rot = rot;
         }
         cl.sync();
-        int off_p = 0;
-        K = 0;
+        bool any_rot = false;
         for (int r = 0; r < C; ++r) {
-            const int cn = *cl.map_shared_rank(&S.s_cnt, r);
-            off_p += r < rank ? cn : 0;
-            K += cn;
+            any_rot |= *cl.map_shared_rank(&S.s_rot, r) != 0;
+        }
+        const int S2 = ((Kz + C - 1) / C + chunk - 1) / chunk * chunk;
+        const int q0 = min(Kz, rank * S2), q1 = min(Kz, q0 + S2);
+        int off_p = q0;
+        K = Kz;
+        if (any_rot) {
+            // some entries were rotated out: count the poles of every
+            // slice (with none, every active entry is a pole)
+            const int np = defl_count_poles<T>(w, gs, q0, q1, S.iscan);
+            if (x == 0) {
+                S.s_cnt = np;
+            }
+            cl.sync();
+            off_p = 0;
+            K = 0;
+            for (int r = 0; r < C; ++r) {
+                const int cn = *cl.map_shared_rank(&S.s_cnt, r);
+                off_p += r < rank ? cn : 0;
+                K += cn;
+            }
         }
         int end_p;
         double zp = defl_compact_poles<T>(w, gs, G.poff, q0, q1, off_p, q0 - off_p, S.iscan,
