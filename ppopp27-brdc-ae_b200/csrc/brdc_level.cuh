@@ -6,7 +6,7 @@
 // level on launches and global round trips -- short chains of dependent
 // latencies.  k_level runs every step of a level for one merge node in a
 // cluster of C CTAs (C = 1 allowed):
-//   rank merge of the two children (sorted lists staged in shared memory),
+//   rank merge of the two children (a merge path through shared memory),
 //   deflation (the phases of k_merge_deflate / k_merge_deflate_cl),
 //   secular roots, Loewner weights and boundary rows of the K <= kLvlMaxK
 //   poles in shared memory, the roots split over the cluster's CTAs and the
@@ -33,19 +33,28 @@ constexpr int kLvlMaxK = 1024;       // poles a node takes through the roots in 
 constexpr int kLvlSamples = 4096;    // samples of a sorted list staged in shared memory
 constexpr int kLvlRowsPerCta = 4096; // merge rows per CTA the launch aims at
 constexpr int kLvlBatch = 4;         // rows a thread moves per pass (loads issued together)
+constexpr int kLvlMergeChunk = 4096; // merged positions per chunk of the merge path
 
 struct LvlSmem {
     double pd[kLvlMaxK], pz[kLvlMaxK], pf[kLvlMaxK], pl[kLvlMaxK], pw[kLvlMaxK];
     double rdo[kLvlMaxK], rtau[kLvlMaxK];
-    double stage[2 * kLvlSamples];       // staged sorted lists (merge, placement)
+    double stage[2 * kLvlSamples];       // staged sorted lists of the placement
     double red[32];
     int iscan[32];
     double s_val;                        // cluster exchange
+    int msplit[2];                       // merge-path splits of the current chunk
     int s_cnt;
     int s_rot;                           // this CTA rotated close poles out
     int s_last;
     uint64_t bar;                        // completion of the pole copies
 };
+
+// The merge uses pd .. stage as one scratch buffer (the poles are staged
+// only after it, the placement lists after the roots).
+static_assert(offsetof(LvlSmem, stage) == offsetof(LvlSmem, pd) + 7 * kLvlMaxK * sizeof(double),
+              "pd .. rtau and stage must be contiguous");
+static_assert(3 * kLvlMergeChunk <= 7 * kLvlMaxK + 2 * kLvlSamples,
+              "the merge scratch must fit in pd .. stage");
 
 // A sorted list in global memory with every Q-th element staged in shared
 // memory.  A bound takes a binary search of the samples, then one scan of
@@ -102,6 +111,124 @@ __device__ inline int staged_fine(const StagedList &L, int c, double v) {
         cnt += UPPER ? (L.g[j] <= v) : (L.g[j] < v);
     }
     return cnt;
+}
+
+// ---------------------------------------------------------------- merge
+// The rank merge of a node's two sorted children as a merge path: CTA r of
+// the cluster writes the merged positions [e0, e1), chunk by chunk.  For a
+// chunk [oc, oe) the CTA finds how many left-child elements precede oc and
+// oe (left wins ties: A[i] goes before B[j] iff A[i] <= B[j]), loads the two
+// child ranges that fill the chunk into shared memory with coalesced loads,
+// and every thread takes merged positions of the chunk by a binary search
+// of the merge path in shared memory.  Each child element is read once and
+// every store is coalesced; the order is exactly the rank merge's.
+
+// Left-child elements among the first o merged elements, by a G-ary search
+// of the merge path (G = T/2 threads, t = this thread's index in its half;
+// the two halves of the CTA search for two positions at once).  Every
+// thread of the CTA calls it; cnt points at 4 ints of shared memory.
+template <int T>
+__device__ inline int merge_split2(const double *A, int m1, const double *B, int m2, int o,
+                                   int *cnt) {
+    constexpr int G = T / 2;
+    const int h = threadIdx.x / G, t = threadIdx.x % G;
+    int lo = max(0, o - m2), hi = min(o, m1);
+    if (threadIdx.x < 4) {
+        cnt[threadIdx.x] = 0;
+    }
+    // invariant: the split (the smallest i with !(A[i] <= B[o-i-1])) lies in
+    // [lo, hi]; at hi the test fails by definition
+    for (int round = 0;; ++round) {
+        if (!__syncthreads_or(lo < hi)) {
+            break;
+        }
+        const int par = round & 1;
+        if (threadIdx.x == 0) {
+            cnt[(par ^ 1) * 2] = 0;
+            cnt[(par ^ 1) * 2 + 1] = 0;
+        }
+        const int step = lo < hi ? (hi - lo + G - 1) / G : 1;
+        const int c = lo + t * step;
+        // c < hi <= min(o, m1), and c >= lo >= o - m2: both reads in range
+        const bool good = lo < hi && c < hi && A[c] <= B[o - c - 1];
+        const unsigned b = __ballot_sync(0xffffffffu, good);
+        if ((threadIdx.x & 31) == 0 && b != 0u) {
+            atomicAdd(&cnt[par * 2 + h], __popc(b));
+        }
+        __syncthreads();
+        const int nt = cnt[par * 2 + h];
+        if (lo < hi) {
+            if (nt == 0) {
+                hi = lo;
+            } else {
+                const int nlo = lo + (nt - 1) * step + 1;
+                hi = min(hi, lo + nt * step);
+                lo = nlo;
+            }
+        }
+    }
+    return lo;
+}
+
+// The merged lists md, mz, mf, ml, morig of positions [e0, e1) of node gs
+// (left child rows [0, m1), right child [m1, m)); returns this thread's
+// max |z|.  buf holds 3 * kLvlMergeChunk doubles of scratch; cnt 4 ints.
+template <int T>
+__device__ double level_merge(const Ws &w, long long gs, int m1, int m, int e0, int e1,
+                              double *buf, int *cnt, int *split) {
+    const int m2 = m - m1;
+    const double *A = w.cd + gs, *B = w.cd + gs + m1;
+    double *bd = buf, *bf = buf + kLvlMergeChunk, *bl = buf + 2 * kLvlMergeChunk;
+    const int x = threadIdx.x;
+    double lz = 0.0;
+    for (int oc = e0; oc < e1; oc += kLvlMergeChunk) {
+        const int oe = min(e1, oc + kLvlMergeChunk);
+        const int s = merge_split2<T>(A, m1, B, m2, x < T / 2 ? oc : oe, cnt);
+        if (x == 0) {
+            split[0] = s;
+        }
+        if (x == T / 2) {
+            split[1] = s;
+        }
+        __syncthreads();
+        const int a0 = split[0], a1 = split[1];
+        const int na = a1 - a0, n = oe - oc;
+        const int b0 = oc - a0;
+        // the two child ranges, left then right, into shared memory
+        for (int u = x; u < n; u += T) {
+            const long long src = u < na ? gs + a0 + u : gs + m1 + b0 + (u - na);
+            bd[u] = w.cd[src];
+            bf[u] = w.cf[src];
+            bl[u] = w.cl[src];
+        }
+        __syncthreads();
+        const int nb = n - na;
+        for (int k = x; k < n; k += T) {
+            int lo = max(0, k - nb), hi = min(k, na);
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (bd[mid] <= bd[na + k - mid - 1]) {
+                    lo = mid + 1;
+                } else {
+                    hi = mid;
+                }
+            }
+            const int i = lo, j = k - lo;
+            const bool left = i < na && (j >= nb || bd[i] <= bd[na + j]);
+            const int u = left ? i : na + j;
+            const double r = left ? bl[u] : bf[u];
+            const double z = r / kSqrt2;
+            const long long o = gs + oc + k;
+            w.md[o] = bd[u];
+            w.mz[o] = z;
+            w.mf[o] = left ? bf[u] : 0.0;
+            w.ml[o] = left ? 0.0 : bl[u];
+            w.morig[o] = left ? a0 + i : m1 + b0 + j;
+            lz = fmax(lz, fabs(z));
+        }
+        __syncthreads();
+    }
+    return lz;
 }
 
 // Roots, Loewner weights and boundary rows of one node with 1 <= K <=
@@ -348,7 +475,7 @@ __global__ void __launch_bounds__(T, 1) k_level(KArgs a) {
     const NodeGeom G = node_geom(a.F, a.k, g);
     const Ws &w = a.w;
     const long long gs = G.gstart;
-    const int m = G.m, m1 = G.m1, m2 = m - m1;
+    const int m = G.m, m1 = G.m1;
     const int x = threadIdx.x;
     constexpr int chunk = kDeflEPT * T;
     constexpr int B = kLvlBatch;
@@ -356,47 +483,10 @@ __global__ void __launch_bounds__(T, 1) k_level(KArgs a) {
     defl_node_scalars(a, G, &rho, &maxd);
 
     // ------------------------------------------------ rank merge
-    // (left wins ties), as k_merge; max|z| on the way
-    const StagedList LA = stage_list<T>(S.stage, w.cd + gs, m1);
-    const StagedList LB = stage_list<T>(S.stage + kLvlSamples, w.cd + gs + m1, m2);
-    __syncthreads();
+    // (left wins ties), as k_merge, by the merge path; max|z| on the way
     const int SE = (m + C - 1) / C;
     const int e0 = min(m, rank * SE), e1 = min(m, e0 + SE);
-    double lz = 0.0;
-    for (int e = e0 + x; e < e1; e += B * T) {
-        double v[B], z[B], f[B], l[B];
-        int c[B];
-#pragma unroll
-        for (int u = 0; u < B; ++u) {
-            const int ee = e + u * T < e1 ? e + u * T : e;
-            const bool left = ee < m1;
-            v[u] = w.cd[gs + ee];
-            const double r = left ? w.cl[gs + ee] : w.cf[gs + ee];
-            z[u] = r / kSqrt2;
-            f[u] = left ? w.cf[gs + ee] : 0.0;
-            l[u] = left ? 0.0 : w.cl[gs + ee];
-        }
-#pragma unroll
-        for (int u = 0; u < B; ++u) {
-            const int ee = e + u * T;
-            c[u] = ee < m1 ? staged_coarse<false>(LB, v[u]) : staged_coarse<true>(LA, v[u]);
-        }
-#pragma unroll
-        for (int u = 0; u < B; ++u) {
-            const int ee = e + u * T;
-            if (ee < e1) {
-                const int pos = ee < m1 ? ee + staged_fine<false>(LB, c[u], v[u])
-                                        : (ee - m1) + staged_fine<true>(LA, c[u], v[u]);
-                const long long o = gs + pos;
-                w.md[o] = v[u];
-                w.mz[o] = z[u];
-                w.mf[o] = f[u];
-                w.ml[o] = l[u];
-                w.morig[o] = ee;
-                lz = fmax(lz, fabs(z[u]));
-            }
-        }
-    }
+    double lz = level_merge<T>(w, gs, m1, m, e0, e1, S.pd, S.iscan, S.msplit);
     lz = block_max<T>(lz, S.red);
     if (x == 0) {
         S.s_val = lz;
