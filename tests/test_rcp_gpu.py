@@ -1,5 +1,5 @@
 """The reciprocal of the pole-root pair loops (brdc_rcp: hardware estimate
-plus two Newton-Raphson steps) against IEEE division on the device, over
+plus one third-order refinement step) against IEEE division on the device, over
 magnitudes from 1e-300 to 1e300 and both signs, including powers of two
 and their neighbours."""
 import ctypes
