@@ -50,11 +50,14 @@ struct LvlSmem {
 };
 
 // The merge uses pd .. stage as one scratch buffer (the poles are staged
-// only after it, the placement lists after the roots).
+// only after it), the placement pz .. stage (after the roots are gathered);
+// the kernel addresses both from the raw shared-memory base.
 static_assert(offsetof(LvlSmem, stage) == offsetof(LvlSmem, pd) + 7 * kLvlMaxK * sizeof(double),
               "pd .. rtau and stage must be contiguous");
 static_assert(3 * kLvlMergeChunk <= 7 * kLvlMaxK + 2 * kLvlSamples,
               "the merge scratch must fit in pd .. stage");
+static_assert(3 * kLvlMergeChunk <= 6 * kLvlMaxK + 2 * kLvlSamples,
+              "the placement scratch must fit in pz .. stage");
 
 // A sorted list in global memory with every Q-th element staged in shared
 // memory.  A bound takes a binary search of the samples, then one scan of
@@ -229,6 +232,68 @@ __device__ double level_merge(const Ws &w, long long gs, int m1, int m, int e0, 
         __syncthreads();
     }
     return lz;
+}
+
+// Placement of a node none of whose poles was rotated out: its ascending
+// order is the merge of the roots (R, in shared memory) and the small-z
+// list (zd, zf, zl), roots first on ties -- the order the three-list rank
+// rule gives -- taken as a merge path like the rank merge: chunk splits by
+// merge_split2, the small-z range loaded coalesced into shared memory
+// (buf: pz .. stage, free once the roots are gathered), every output
+// stored coalesced.  Outputs [e0, e1) of the node; at an instance root the
+// values go to W.
+template <int T>
+__device__ void level_place_merge(const KArgs &a, const Ws &w, LvlSmem &S, double *buf,
+                                  long long gs, long long po, int K, int ndz, int e0, int e1,
+                                  bool top, double wsc) {
+    const double *R = S.pd;
+    const double *Z = w.zd + gs;
+    double *zd = buf, *zf = buf + kLvlMergeChunk, *zl = buf + 2 * kLvlMergeChunk;
+    const int x = threadIdx.x;
+    for (int oc = e0; oc < e1; oc += kLvlMergeChunk) {
+        const int oe = min(e1, oc + kLvlMergeChunk);
+        const int sp = merge_split2<T>(R, K, Z, ndz, x < T / 2 ? oc : oe, S.iscan);
+        if (x == 0) {
+            S.msplit[0] = sp;
+        }
+        if (x == T / 2) {
+            S.msplit[1] = sp;
+        }
+        __syncthreads();
+        const int r0 = S.msplit[0], r1 = S.msplit[1];
+        const int nr = r1 - r0, n = oe - oc, nz = n - nr;
+        const int z0 = oc - r0;
+        for (int u = x; u < nz; u += T) {
+            const long long src = gs + z0 + u;
+            zd[u] = w.zd[src];
+            zf[u] = w.zf[src];
+            zl[u] = w.zl[src];
+        }
+        __syncthreads();
+        for (int k = x; k < n; k += T) {
+            int lo = max(0, k - nz), hi = min(k, nr);
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (R[r0 + mid] <= zd[k - mid - 1]) {
+                    lo = mid + 1;
+                } else {
+                    hi = mid;
+                }
+            }
+            const int i = lo, j = k - lo;
+            const bool root = i < nr && (j >= nz || R[r0 + i] <= zd[j]);
+            const long long o = gs + oc + k;
+            const double val = root ? R[r0 + i] : zd[j];
+            if (top) {
+                a.W[o] = val * wsc;
+            } else {
+                w.nd[o] = val;
+                w.nf[o] = root ? __ldcg(w.rf + po + r0 + i) : zf[j];
+                w.nl[o] = root ? __ldcg(w.rl + po + r0 + i) : zl[j];
+            }
+        }
+        __syncthreads();
+    }
 }
 
 // Roots, Loewner weights and boundary rows of one node with 1 <= K <=
@@ -486,7 +551,9 @@ __global__ void __launch_bounds__(T, 1) k_level(KArgs a) {
     // (left wins ties), as k_merge, by the merge path; max|z| on the way
     const int SE = (m + C - 1) / C;
     const int e0 = min(m, rank * SE), e1 = min(m, e0 + SE);
-    double lz = level_merge<T>(w, gs, m1, m, e0, e1, S.pd, S.iscan, S.msplit);
+    double lz = level_merge<T>(w, gs, m1, m, e0, e1,
+                               reinterpret_cast<double *>(lvl_raw + offsetof(LvlSmem, pd)),
+                               S.iscan, S.msplit);
     lz = block_max<T>(lz, S.red);
     if (x == 0) {
         S.s_val = lz;
@@ -611,73 +678,79 @@ __global__ void __launch_bounds__(T, 1) k_level(KArgs a) {
     for (int i = x; i < K; i += T) {
         S.pd[i] = S.rdo[i] + S.rtau[i]; // = rlam, bit for bit
     }
-    const StagedList LZ = stage_list<T>(S.stage, w.zd + gs, ndz);
-    const StagedList LG = stage_list<T>(S.stage + kLvlSamples, w.gd + gs, ndg);
-    __syncthreads();
     const bool top = (G.depth == 0);
     const double wsc = inst_unscale(w, G.inst);
-    for (int s0 = e0 + x; s0 < e1; s0 += B * T) {
-        double val[B], fo[B], lo[B];
-        int pos[B];
+    if (ndg == 0) {
+        __syncthreads();
+        level_place_merge<T>(a, w, S, reinterpret_cast<double *>(lvl_raw + offsetof(LvlSmem, pz)),
+                             gs, po, K, ndz, e0, e1, top, wsc);
+    } else {
+        const StagedList LZ = stage_list<T>(S.stage, w.zd + gs, ndz);
+        const StagedList LG = stage_list<T>(S.stage + kLvlSamples, w.gd + gs, ndg);
+        __syncthreads();
+        for (int s0 = e0 + x; s0 < e1; s0 += B * T) {
+            double val[B], fo[B], lo[B];
+            int pos[B];
 #pragma unroll
-        for (int u = 0; u < B; ++u) {
-            const int s = s0 + u * T < e1 ? s0 + u * T : s0;
-            if (s < K) {
-                val[u] = S.pd[s];
-                fo[u] = top ? 0.0 : __ldcg(w.rf + po + s);
-                lo[u] = top ? 0.0 : __ldcg(w.rl + po + s);
-            } else if (s < K + ndz) {
-                val[u] = w.zd[gs + s - K];
-                fo[u] = w.zf[gs + s - K];
-                lo[u] = w.zl[gs + s - K];
-            } else {
-                val[u] = w.gd[gs + s - K - ndz];
-                fo[u] = w.gf[gs + s - K - ndz];
-                lo[u] = w.gl[gs + s - K - ndz];
-            }
-        }
-        // each row searches the two lists it is not in (rows of one warp
-        // are consecutive, so the branches split few warps)
-        int cz[B], cgr[B];
-#pragma unroll
-        for (int u = 0; u < B; ++u) {
-            const int s = s0 + u * T;
-            cz[u] = 0;
-            cgr[u] = 0;
-            if (s < K) {
-                cz[u] = staged_coarse<false>(LZ, val[u]);
-                cgr[u] = staged_coarse<false>(LG, val[u]);
-            } else if (s < K + ndz) {
-                cgr[u] = staged_coarse<false>(LG, val[u]);
-            } else {
-                cz[u] = staged_coarse<true>(LZ, val[u]); // rotated out: ties after small-z
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < B; ++u) {
-            const int s = s0 + u * T;
-            if (s < K) {
-                pos[u] = s + staged_fine<false>(LZ, cz[u], val[u]) +
-                         staged_fine<false>(LG, cgr[u], val[u]);
-            } else if (s < K + ndz) {
-                pos[u] = (s - K) + upper_bound_d(S.pd, K, val[u]) +
-                         staged_fine<false>(LG, cgr[u], val[u]);
-            } else {
-                pos[u] = (s - K - ndz) + upper_bound_d(S.pd, K, val[u]) +
-                         staged_fine<true>(LZ, cz[u], val[u]);
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < B; ++u) {
-            const int s = s0 + u * T;
-            if (s < e1) {
-                const long long o = gs + pos[u];
-                if (top) {
-                    a.W[o] = val[u] * wsc;
+            for (int u = 0; u < B; ++u) {
+                const int s = s0 + u * T < e1 ? s0 + u * T : s0;
+                if (s < K) {
+                    val[u] = S.pd[s];
+                    fo[u] = top ? 0.0 : __ldcg(w.rf + po + s);
+                    lo[u] = top ? 0.0 : __ldcg(w.rl + po + s);
+                } else if (s < K + ndz) {
+                    val[u] = w.zd[gs + s - K];
+                    fo[u] = w.zf[gs + s - K];
+                    lo[u] = w.zl[gs + s - K];
                 } else {
-                    w.nd[o] = val[u];
-                    w.nf[o] = fo[u];
-                    w.nl[o] = lo[u];
+                    val[u] = w.gd[gs + s - K - ndz];
+                    fo[u] = w.gf[gs + s - K - ndz];
+                    lo[u] = w.gl[gs + s - K - ndz];
+                }
+            }
+            // each row searches the two lists it is not in (rows of one warp
+            // are consecutive, so the branches split few warps)
+            int cz[B], cgr[B];
+#pragma unroll
+            for (int u = 0; u < B; ++u) {
+                const int s = s0 + u * T;
+                cz[u] = 0;
+                cgr[u] = 0;
+                if (s < K) {
+                    cz[u] = staged_coarse<false>(LZ, val[u]);
+                    cgr[u] = staged_coarse<false>(LG, val[u]);
+                } else if (s < K + ndz) {
+                    cgr[u] = staged_coarse<false>(LG, val[u]);
+                } else {
+                    cz[u] = staged_coarse<true>(LZ, val[u]); // rotated out: ties after small-z
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < B; ++u) {
+                const int s = s0 + u * T;
+                if (s < K) {
+                    pos[u] = s + staged_fine<false>(LZ, cz[u], val[u]) +
+                             staged_fine<false>(LG, cgr[u], val[u]);
+                } else if (s < K + ndz) {
+                    pos[u] = (s - K) + upper_bound_d(S.pd, K, val[u]) +
+                             staged_fine<false>(LG, cgr[u], val[u]);
+                } else {
+                    pos[u] = (s - K - ndz) + upper_bound_d(S.pd, K, val[u]) +
+                             staged_fine<true>(LZ, cz[u], val[u]);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < B; ++u) {
+                const int s = s0 + u * T;
+                if (s < e1) {
+                    const long long o = gs + pos[u];
+                    if (top) {
+                        a.W[o] = val[u] * wsc;
+                    } else {
+                        w.nd[o] = val[u];
+                        w.nf[o] = fo[u];
+                        w.nl[o] = lo[u];
+                    }
                 }
             }
         }
