@@ -44,6 +44,8 @@ struct LvlSmem {
     double s_val;                        // cluster exchange
     int msplit[2];                       // merge-path splits of the current chunk
     int s_cnt;
+    int s_kz;                            // CTA 0's deflation results for its peers
+    double s_zn;                         // (s_val still holds max|z| for their reads)
     int s_rot;                           // this CTA rotated close poles out
     int s_last;
     uint64_t bar;                        // completion of the pole copies
@@ -577,6 +579,27 @@ __global__ void __launch_bounds__(T, 1) k_level(KArgs a) {
         __syncthreads();
         zn = defl_compact_poles<T>(w, gs, G.poff, 0, Kz, 0, 0, S.iscan, &K);
         zn = block_sum<T>(zn, S.red);
+    } else if (m <= ((m + C - 1) / C + chunk - 1) / chunk * chunk) {
+        // the deflation slices are whole chunks, so the node lies in CTA 0's
+        // slice alone: CTA 0 deflates it as one CTA per node does, with no
+        // counts to exchange, and its peers wait at one cluster barrier
+        if (rank == 0) {
+            Kz = defl_compact_active<T>(w, gs, 0, m, rho, tol, 0, 0, S.iscan);
+            __syncthreads();
+            defl_close_walk<T>(w, gs, Kz, tol, 0, Kz);
+            __syncthreads();
+            zn = defl_compact_poles<T>(w, gs, G.poff, 0, Kz, 0, 0, S.iscan, &K);
+            zn = block_sum<T>(zn, S.red);
+            if (x == 0) {
+                S.s_cnt = K;
+                S.s_kz = Kz;
+                S.s_zn = zn;
+            }
+        }
+        cl.sync();
+        K = *cl.map_shared_rank(&S.s_cnt, 0);
+        Kz = *cl.map_shared_rank(&S.s_kz, 0);
+        zn = *cl.map_shared_rank(&S.s_zn, 0);
     } else {
         const int SD = ((m + C - 1) / C + chunk - 1) / chunk * chunk;
         const int r0 = min(m, rank * SD), r1 = min(m, r0 + SD);
