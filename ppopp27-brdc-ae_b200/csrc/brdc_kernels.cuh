@@ -1727,8 +1727,8 @@ __device__ bool sweep_lowner(const KArgs &a, int cta_blocks, double *smem, uint6
             const long long po = G.poff;
             const int i = (item - w.pref_w[g]) * Rw + grp;
             const bool active = i < K;
-            // two interleaved products halve the serial multiply chain
-            double prod = 1.0, prod2 = 1.0;
+            // two factors per step share one reciprocal (lowner_pair)
+            double prod = 1.0;
             if (active) {
                 const double di = w.pd[po + i];
                 const double *rdo = w.rdo + po;
@@ -1740,17 +1740,15 @@ __device__ bool sweep_lowner(const KArgs &a, int cta_blocks, double *smem, uint6
                     const int j2 = j + tpr;
                     const double dl = (di - __ldcg(rdo + j)) - __ldcg(rtau + j);
                     const double dl2 = (di - __ldcg(rdo + j2)) - __ldcg(rtau + j2);
-                    const double q = brdc_rcp(j == i ? 1.0 : di - __ldg(pd + j));
-                    const double q2 = brdc_rcp(j2 == i ? 1.0 : di - __ldg(pd + j2));
-                    prod *= dl * q;
-                    prod2 *= dl2 * q2;
+                    prod *= lowner_pair(dl, j == i ? 1.0 : di - __ldg(pd + j), dl2,
+                                        j2 == i ? 1.0 : di - __ldg(pd + j2));
                 }
                 if (j < K) {
                     const double dl = (di - __ldcg(rdo + j)) - __ldcg(rtau + j);
                     prod *= dl * brdc_rcp(j == i ? 1.0 : di - __ldg(pd + j));
                 }
             }
-            prod = group_prod(prod * prod2, tpr);
+            prod = group_prod(prod, tpr);
             if (active && l == 0) {
                 w.pw[po + i] = lowner_value(w, po, i, prod, w.nrho[g]);
             }
@@ -1773,7 +1771,7 @@ __device__ bool sweep_lowner(const KArgs &a, int cta_blocks, double *smem, uint6
         const int i = (item - w.pref_c[g]) * R + grp;
         const bool active = i < K;
         const double di = active ? w.pd[po + i] : 0.0;
-        double prod = 1.0, prod2 = 1.0;
+        double prod = 1.0;
         TileSet<3> ts;
         const double *srcs[3] = {w.rdo, w.rtau, w.pd};
         tiles_setup<3>(ts, smem, bars, srcs, po, K, w.hdr->wait_ns);
@@ -1786,10 +1784,8 @@ __device__ bool sweep_lowner(const KArgs &a, int cta_blocks, double *smem, uint6
                     const int j = j0 + jj, jj2 = jj + tpr;
                     const double dl = (di - b[0][jj]) - b[1][jj];
                     const double dl2 = (di - b[0][jj2]) - b[1][jj2];
-                    const double q = brdc_rcp(j == i ? 1.0 : di - b[2][jj]);
-                    const double q2 = brdc_rcp(j + tpr == i ? 1.0 : di - b[2][jj2]);
-                    prod *= dl * q;
-                    prod2 *= dl2 * q2;
+                    prod *= lowner_pair(dl, j == i ? 1.0 : di - b[2][jj], dl2,
+                                        j + tpr == i ? 1.0 : di - b[2][jj2]);
                 }
                 if (jj < cnt) {
                     const double dl = (di - b[0][jj]) - b[1][jj];
@@ -1804,7 +1800,7 @@ __device__ bool sweep_lowner(const KArgs &a, int cta_blocks, double *smem, uint6
             record_error(w.hdr, kErrBarrierTimeout);
             return false;
         }
-        prod = group_prod(prod * prod2, tpr);
+        prod = group_prod(prod, tpr);
         if (active && lane == 0) {
             w.pw[po + i] = lowner_value(w, po, i, prod, w.nrho[g]);
         }

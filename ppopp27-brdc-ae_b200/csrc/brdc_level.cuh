@@ -440,7 +440,7 @@ __device__ void level_roots(LvlSmem &S, cooperative_groups::cluster_group &cl, c
     const int per = T / tpr, gl = x & (tpr - 1);
     for (int base = 0; base < nmine; base += per) {
         const int i = r0 + base + x / tpr;
-        double prod = 1.0, prod2 = 1.0;
+        double prod = 1.0;
         if (i < r1) {
             const double di = S.pd[i];
             int q = gl;
@@ -448,15 +448,15 @@ __device__ void level_roots(LvlSmem &S, cooperative_groups::cluster_group &cl, c
                 const int q2 = q + tpr;
                 const double dl = (di - S.rdo[q]) - S.rtau[q];
                 const double dl2 = (di - S.rdo[q2]) - S.rtau[q2];
-                prod *= dl * brdc_rcp(q == i ? 1.0 : di - S.pd[q]);
-                prod2 *= dl2 * brdc_rcp(q2 == i ? 1.0 : di - S.pd[q2]);
+                prod *= lowner_pair(dl, q == i ? 1.0 : di - S.pd[q], dl2,
+                                    q2 == i ? 1.0 : di - S.pd[q2]);
             }
             if (q < K) {
                 const double dl = (di - S.rdo[q]) - S.rtau[q];
                 prod *= dl * brdc_rcp(q == i ? 1.0 : di - S.pd[q]);
             }
         }
-        prod = group_prod(prod * prod2, tpr);
+        prod = group_prod(prod, tpr);
         if (i < r1 && gl == 0) {
             const double zi = S.pz[i];
             const double mag = sqrt(fmax(-prod, 0.0));

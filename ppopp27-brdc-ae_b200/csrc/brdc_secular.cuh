@@ -66,6 +66,19 @@ __host__ __device__ inline double brdc_rcp(double x) {
 #endif
 }
 
+// Two factors of a Loewner product, (d_i - lambda_j) / (d_i - d_j) for two
+// poles j, with one reciprocal of the product of their denominators.  The
+// denominators are distinct poles' differences (or 1 for j = i), of order
+// ||T|| down to the deflation tolerance, and the numerators of order ||T||
+// down to a root's distance from its pole, so neither product comes near
+// the ends of the double range.  The reciprocal is the pair loops' dearest
+// operation (a quarter-rate estimate and three FMAs), and one per two
+// factors takes about a third off the product's cost.
+__host__ __device__ inline double lowner_pair(double num1, double den1, double num2,
+                                              double den2) {
+    return (num1 * num2) * brdc_rcp(den1 * den2);
+}
+
 struct SecSums {
     double psi;   // sum_{j < p} z_j^2 / delta_j
     double dpsi;  // sum_{j < p} z_j^2 / delta_j^2

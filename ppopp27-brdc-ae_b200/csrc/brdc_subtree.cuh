@@ -626,7 +626,7 @@ __global__ void __launch_bounds__(kSubRows, 512 / kSubRows) k_subtree(SubArgs A)
         if (!nodetop) {
             // Loewner weights (sqrt(rho) z), tpr lanes per pole
             {
-                double prod = 1.0, prod2 = 1.0;
+                double prod = 1.0;
                 if (jr >= 0) {
                     const int i = rr;
                     const double di = S.pd[sr + i];
@@ -635,15 +635,15 @@ __global__ void __launch_bounds__(kSubRows, 512 / kSubRows) k_subtree(SubArgs A)
                         const int q2 = q + tpr;
                         const double dl = (di - S.rdo[sr + q]) - S.rtau[sr + q];
                         const double dl2 = (di - S.rdo[sr + q2]) - S.rtau[sr + q2];
-                        prod *= dl * brdc_rcp(q == i ? 1.0 : di - S.pd[sr + q]);
-                        prod2 *= dl2 * brdc_rcp(q2 == i ? 1.0 : di - S.pd[sr + q2]);
+                        prod *= lowner_pair(dl, q == i ? 1.0 : di - S.pd[sr + q], dl2,
+                                            q2 == i ? 1.0 : di - S.pd[sr + q2]);
                     }
                     if (q < Kr) {
                         const double dl = (di - S.rdo[sr + q]) - S.rtau[sr + q];
                         prod *= dl * brdc_rcp(q == i ? 1.0 : di - S.pd[sr + q]);
                     }
                 }
-                prod = group_prod(prod * prod2, tpr);
+                prod = group_prod(prod, tpr);
                 if (jr >= 0 && gl == 0) {
                     const double zi = S.pz[sr + rr];
                     const double mag = sqrt(fmax(-prod, 0.0));
