@@ -1848,8 +1848,21 @@ __device__ bool sweep_rows(const KArgs &a, int cta_blocks, double *smem, uint64_
                 const double *pw = w.pw + po;
                 const double *pf = w.pf + po;
                 const double *pl = w.pl + po;
-#pragma unroll 4
-                for (int i = l; i < K; i += tpr) {
+                int i = l;
+#pragma unroll 2
+                for (; i + tpr < K; i += 2 * tpr) {
+                    const int i2 = i + tpr;
+                    double u, u2;
+                    row_pair(__ldcg(pw + i), (__ldg(pd + i) - dorg) - tau, __ldcg(pw + i2),
+                             (__ldg(pd + i2) - dorg) - tau, &u, &u2);
+                    s2 += u * u;
+                    a1 += __ldg(pf + i) * u;
+                    a2 += __ldg(pl + i) * u;
+                    s2 += u2 * u2;
+                    a1 += __ldg(pf + i2) * u2;
+                    a2 += __ldg(pl + i2) * u2;
+                }
+                if (i < K) {
                     const double dl = (__ldg(pd + i) - dorg) - tau;
                     const double u = (dl != 0.0) ? __ldcg(pw + i) * brdc_rcp(dl) : 0.0;
                     s2 += u * u;
@@ -1893,7 +1906,20 @@ __device__ bool sweep_rows(const KArgs &a, int cta_blocks, double *smem, uint64_
         ts.phase[1] = ph[1];
         const bool ok = tiles_sweep<4>(ts, [&](int j0, int cnt, double *const *b) {
             if (root) {
-                for (int jj = lane; jj < cnt; jj += tpr) {
+                int jj = lane;
+                for (; jj + tpr < cnt; jj += 2 * tpr) {
+                    const int jj2 = jj + tpr;
+                    double u, u2;
+                    row_pair(b[1][jj], (b[0][jj] - dorg) - tau, b[1][jj2],
+                             (b[0][jj2] - dorg) - tau, &u, &u2);
+                    s2 += u * u;
+                    a1 += b[2][jj] * u;
+                    a2 += b[3][jj] * u;
+                    s2 += u2 * u2;
+                    a1 += b[2][jj2] * u2;
+                    a2 += b[3][jj2] * u2;
+                }
+                if (jj < cnt) {
                     const double dl = (b[0][jj] - dorg) - tau;
                     const double u = (dl != 0.0) ? b[1][jj] * brdc_rcp(dl) : 0.0;
                     s2 += u * u;

@@ -483,7 +483,20 @@ __device__ void level_roots(LvlSmem &S, cooperative_groups::cluster_group &cl, c
         double a1 = 0.0, a2 = 0.0, s2 = 0.0;
         if (r < r1) {
             const double dorg = S.rdo[r], tau = S.rtau[r];
-            for (int i = gl; i < K; i += tpr) {
+            int i = gl;
+            for (; i + tpr < K; i += 2 * tpr) {
+                const int i2 = i + tpr;
+                double u, u2;
+                row_pair(S.pw[i], (S.pd[i] - dorg) - tau, S.pw[i2], (S.pd[i2] - dorg) - tau, &u,
+                         &u2);
+                s2 += u * u;
+                a1 += S.pf[i] * u;
+                a2 += S.pl[i] * u;
+                s2 += u2 * u2;
+                a1 += S.pf[i2] * u2;
+                a2 += S.pl[i2] * u2;
+            }
+            if (i < K) {
                 const double dl = (S.pd[i] - dorg) - tau;
                 const double u = (dl != 0.0) ? S.pw[i] * brdc_rcp(dl) : 0.0;
                 s2 += u * u;

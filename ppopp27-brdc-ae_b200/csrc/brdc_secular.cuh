@@ -79,6 +79,19 @@ __host__ __device__ inline double lowner_pair(double num1, double den1, double n
     return (num1 * num2) * brdc_rcp(den1 * den2);
 }
 
+// The secular vector entries u = w / delta of two poles, with one
+// reciprocal of the product of their deltas.  The deltas are distances of
+// one root from distinct poles, so at most one of them is tiny and the
+// product stays inside the double range.  A zero delta (a root on a pole,
+// reachable only through underflow) gives u = 0, as the single form does.
+__host__ __device__ inline void row_pair(double w1, double dl1, double w2, double dl2,
+                                         double *u1, double *u2) {
+    const double e1 = dl1 != 0.0 ? dl1 : 1.0, e2 = dl2 != 0.0 ? dl2 : 1.0;
+    const double inv = brdc_rcp(e1 * e2);
+    *u1 = dl1 != 0.0 ? w1 * (e2 * inv) : 0.0;
+    *u2 = dl2 != 0.0 ? w2 * (e1 * inv) : 0.0;
+}
+
 struct SecSums {
     double psi;   // sum_{j < p} z_j^2 / delta_j
     double dpsi;  // sum_{j < p} z_j^2 / delta_j^2

@@ -660,7 +660,20 @@ __global__ void __launch_bounds__(kSubRows, 512 / kSubRows) k_subtree(SubArgs A)
                 double a1 = 0.0, a2 = 0.0, s2 = 0.0;
                 if (jr >= 0) {
                     const double dorg = S.rdo[sr + rr], tau = S.rtau[sr + rr];
-                    for (int i = gl; i < Kr; i += tpr) {
+                    int i = gl;
+                    for (; i + tpr < Kr; i += 2 * tpr) {
+                        const int i2 = i + tpr;
+                        double u, u2;
+                        row_pair(S.pw[sr + i], (S.pd[sr + i] - dorg) - tau, S.pw[sr + i2],
+                                 (S.pd[sr + i2] - dorg) - tau, &u, &u2);
+                        s2 += u * u;
+                        a1 += S.pf[sr + i] * u;
+                        a2 += S.pl[sr + i] * u;
+                        s2 += u2 * u2;
+                        a1 += S.pf[sr + i2] * u2;
+                        a2 += S.pl[sr + i2] * u2;
+                    }
+                    if (i < Kr) {
                         const double dl = (S.pd[sr + i] - dorg) - tau;
                         const double u = (dl != 0.0) ? S.pw[sr + i] * brdc_rcp(dl) : 0.0;
                         s2 += u * u;
