@@ -34,6 +34,12 @@ constexpr int kLvlSamples = 4096;    // samples of a sorted list staged in share
 constexpr int kLvlRowsPerCta = 4096; // merge rows per CTA the launch aims at
 constexpr int kLvlBatch = 4;         // rows a thread moves per pass (loads issued together)
 constexpr int kLvlMergeChunk = 4096; // merged positions per chunk of the merge path
+// Merges of at most this many rows are deflated by CTA 0 of their cluster
+// alone (two chunks of 2048 rows at most), which measured faster than
+// spreading them over the cluster with its count exchanges and barriers
+// (uniform 65,536, level 7: 53 -> 48 us); 8192 gained nothing more, 16384
+// lost.
+constexpr int kLvlSoloDeflRows = 4096;
 
 struct LvlSmem {
     double pd[kLvlMaxK], pz[kLvlMaxK], pf[kLvlMaxK], pl[kLvlMaxK], pw[kLvlMaxK];
@@ -592,10 +598,11 @@ __global__ void __launch_bounds__(T, 1) k_level(KArgs a) {
         __syncthreads();
         zn = defl_compact_poles<T>(w, gs, G.poff, 0, Kz, 0, 0, S.iscan, &K);
         zn = block_sum<T>(zn, S.red);
-    } else if (m <= ((m + C - 1) / C + chunk - 1) / chunk * chunk) {
-        // the deflation slices are whole chunks, so the node lies in CTA 0's
-        // slice alone: CTA 0 deflates it as one CTA per node does, with no
-        // counts to exchange, and its peers wait at one cluster barrier
+    } else if (m <= kLvlSoloDeflRows || m <= ((m + C - 1) / C + chunk - 1) / chunk * chunk) {
+        // a small merge (or one that lies in CTA 0's deflation slice alone,
+        // the slices being whole chunks): CTA 0 deflates it as one CTA per
+        // node does, with no counts to exchange, and its peers wait at one
+        // cluster barrier
         if (rank == 0) {
             Kz = defl_compact_active<T>(w, gs, 0, m, rho, tol, 0, 0, S.iscan);
             __syncthreads();
