@@ -53,6 +53,7 @@ __device__ inline double sgn(double x) { return (double)((x > 0.0) - (x < 0.0));
 // node's ascending order.  Instance roots read dL/dW and have no row
 // cotangents.
 __global__ void __launch_bounds__(256) k_bw_unplace(BArgs a, long long total_n) {
+    pdl_begin();
     if (halted(a.w.hdr)) {
         return;
     }
@@ -157,6 +158,7 @@ __device__ inline bool warp_item(const Ws &w, const LevelCtl *ctl, int wi, WarpI
 // the origin's dd and dz terms for the pole kernel and its drho term, which
 // k_bw_undeflate sums in a fixed order.
 __global__ void __launch_bounds__(kSweepThreads) k_bw_roots(BArgs a) {
+    pdl_begin();
     if (halted(a.w.hdr)) {
         return;
     }
@@ -253,6 +255,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_bw_roots(BArgs a) {
 // the (at most two) roots j in {i-1, i} with origin i add their stored
 // origin terms instead.
 __global__ void __launch_bounds__(kSweepThreads) k_bw_poles(BArgs a) {
+    pdl_begin();
     if (halted(a.w.hdr)) {
         return;
     }
@@ -372,6 +375,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_bw_poles(BArgs a) {
 // average); the lanes stride over the roots and combine by shuffles.  Every warp runs the same number of trips,
 // so the shuffles stay convergent.
 __global__ void __launch_bounds__(256) k_bw_defl(BArgs a, long long total_n) {
+    pdl_begin();
     if (halted(a.w.hdr)) {
         return;
     }
@@ -512,6 +516,7 @@ __device__ inline bool bw_reverse_chain(const Ws &w, long long gs, int b0, int K
 // sqrt 2), and dL/dE at the cut.
 template <int T>
 __global__ void __launch_bounds__(T) k_bw_undeflate(BArgs a) {
+    pdl_begin();
     if (halted(a.w.hdr)) {
         return;
     }
@@ -612,6 +617,7 @@ __global__ void __launch_bounds__(T) k_bw_undeflate(BArgs a) {
 
 // poles and rotated-out members -> active positions
 __global__ void __launch_bounds__(256) k_bw_ud_active(BArgs a, long long total_n) {
+    pdl_begin();
     if (halted(a.w.hdr)) {
         return;
     }
@@ -647,6 +653,7 @@ __global__ void __launch_bounds__(256) k_bw_ud_active(BArgs a, long long total_n
 
 // Givens chains, one thread per active index (chain bases do the work)
 __global__ void __launch_bounds__(256) k_bw_ud_chains(BArgs a, long long total_n) {
+    pdl_begin();
     if (halted(a.w.hdr)) {
         return;
     }
@@ -668,6 +675,7 @@ __global__ void __launch_bounds__(256) k_bw_ud_chains(BArgs a, long long total_n
 
 // active and small-z lists -> merged positions
 __global__ void __launch_bounds__(256) k_bw_ud_merged(BArgs a, long long total_n) {
+    pdl_begin();
     if (halted(a.w.hdr)) {
         return;
     }
@@ -701,6 +709,7 @@ __global__ void __launch_bounds__(256) k_bw_ud_merged(BArgs a, long long total_n
 // merged positions -> children (z = last row of the left child / first row
 // of the right child, over sqrt 2)
 __global__ void __launch_bounds__(256) k_bw_ud_children(BArgs a, long long total_n) {
+    pdl_begin();
     if (halted(a.w.hdr)) {
         return;
     }
@@ -731,6 +740,7 @@ __global__ void __launch_bounds__(256) k_bw_ud_children(BArgs a, long long total
 // dL/drho of every merge summed over its roots by one warp, in a fixed
 // order, and dL/dE at its cut
 __global__ void __launch_bounds__(256) k_bw_ud_rho(BArgs a) {
+    pdl_begin();
     if (halted(a.w.hdr)) {
         return;
     }
@@ -762,6 +772,7 @@ __global__ void __launch_bounds__(256) k_bw_ud_rho(BArgs a) {
 // of the cuts.
 __global__ void __launch_bounds__(kLeafWarps * 32)
     k_bw_leaf(BArgs a, long long total_leaves) {
+    pdl_begin();
     if (halted(a.w.hdr)) {
         return;
     }
@@ -878,6 +889,7 @@ __global__ void __launch_bounds__(kLeafWarps * 32)
 // 2 sign(E_c) dL/drho stored by k_bw_undeflate.  One thread per leaf (the
 // leaf left of the cut), so the sum has a fixed order.
 __global__ void __launch_bounds__(256) k_bw_cuts(BArgs a, long long total_leaves) {
+    pdl_begin();
     if (halted(a.w.hdr)) {
         return;
     }
@@ -892,6 +904,7 @@ __global__ void __launch_bounds__(256) k_bw_cuts(BArgs a, long long total_leaves
 }
 
 __global__ void k_bw_zero(double *p, long long n) {
+    pdl_begin();
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x) {
         p[i] = 0.0;

@@ -1496,9 +1496,19 @@ extern "C" brdc_status brdc_autotune(brdc_handle h, int64_t count, const int64_t
 // -------------------------------------------------------------- backward
 namespace {
 
+// Every adjoint kernel starts with pdl_begin, so each is launched with the
+// programmatic-serialization attribute: its blocks are scheduled while the
+// kernel before it finishes, and they wait there for its writes.
+template <typename... P, typename... A>
+void launch_pdl(void (*kern)(P...), long long grid, unsigned block, cudaStream_t s, A... args) {
+    cudaLaunchAttribute at[1];
+    cudaLaunchConfig_t cfg = plain_config((unsigned)grid, block, 0, s, at);
+    cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 template <int T>
 void launch_undeflate(const BArgs &b, int grid, cudaStream_t s) {
-    k_bw_undeflate<T><<<grid, T, 0, s>>>(b);
+    launch_pdl(k_bw_undeflate<T>, grid, T, s, b);
 }
 
 void launch_undeflate_sized(const BArgs &b, int mmax, cudaStream_t s) {
@@ -1528,7 +1538,7 @@ brdc_status run_backward(brdc_handle h, const HostForest &hf, const Layout &L,
     // instance unused and returned as 0) for a batch
     const long long ne = hf.B > 1 ? nt : nt - 1;
     if (ne > 0) {
-        k_bw_zero<<<(unsigned)eg, 256, 0, s>>>(gE, ne);
+        launch_pdl(k_bw_zero, eg, 256, s, gE, ne);
         BRDC_CUDA(h, "brdc.bw.zero_ge", cudaGetLastError());
     }
     double *par[3] = {w.bnd, w.bnf, w.bnl};
@@ -1558,20 +1568,20 @@ brdc_status run_backward(brdc_handle h, const HostForest &hf, const Layout &L,
         b.nodes = hf.level_nodes[k];
         b.level_rows = hf.level_rows[k];
         b.lanes_target = h->lanes_target;
-        k_bw_unplace<<<(unsigned)eg, 256, 0, s>>>(b, nt);
-        k_bw_roots<<<wgrid, kSweepThreads, 0, s>>>(b);
-        k_bw_poles<<<wgrid, kSweepThreads, 0, s>>>(b);
+        launch_pdl(k_bw_unplace, eg, 256, s, b, nt);
+        launch_pdl(k_bw_roots, wgrid, kSweepThreads, s, b);
+        launch_pdl(k_bw_poles, wgrid, kSweepThreads, s, b);
         if (k + 1 < hf.max_levels || hf.B > 1) {
             // up to 4 lanes per row (the kernel picks); surplus blocks exit
-            k_bw_defl<<<(unsigned)dgrid, 256, 0, s>>>(b, nt);
+            launch_pdl(k_bw_defl, dgrid, 256, s, b, nt);
         }
         if (hf.level_mmax[k] >= 2 * kDeflEPT * 1024) {
             // large merges: grid-wide passes instead of one CTA per merge
-            k_bw_ud_active<<<(unsigned)eg, 256, 0, s>>>(b, nt);
-            k_bw_ud_chains<<<(unsigned)eg, 256, 0, s>>>(b, nt);
-            k_bw_ud_merged<<<(unsigned)eg, 256, 0, s>>>(b, nt);
-            k_bw_ud_children<<<(unsigned)eg, 256, 0, s>>>(b, nt);
-            k_bw_ud_rho<<<std::max(1, std::min(b.nodes / 8 + 1, h->sm_count * 8)), 256, 0, s>>>(b);
+            launch_pdl(k_bw_ud_active, eg, 256, s, b, nt);
+            launch_pdl(k_bw_ud_chains, eg, 256, s, b, nt);
+            launch_pdl(k_bw_ud_merged, eg, 256, s, b, nt);
+            launch_pdl(k_bw_ud_children, eg, 256, s, b, nt);
+            launch_pdl(k_bw_ud_rho, std::max(1, std::min(b.nodes / 8 + 1, h->sm_count * 8)), 256, s, b);
         } else {
             launch_undeflate_sized(b, hf.level_mmax[k], s);
         }
@@ -1595,11 +1605,11 @@ brdc_status run_backward(brdc_handle h, const HostForest &hf, const Layout &L,
     const long long per = 2LL * kLeafWarps;
     long long grid = (hf.leaves + per - 1) / per;
     grid = std::max<long long>(1, std::min<long long>(grid, (long long)h->sm_count * 16));
-    k_bw_leaf<<<(unsigned)grid, kLeafWarps * 32, 0, s>>>(b, hf.leaves);
+    launch_pdl(k_bw_leaf, grid, kLeafWarps * 32, s, b, hf.leaves);
     BRDC_CUDA(h, "brdc.bw.leaf", cudaGetLastError());
     long long cg = (hf.leaves + 255) / 256;
     cg = std::max<long long>(1, std::min<long long>(cg, (long long)h->sm_count * 8));
-    k_bw_cuts<<<(unsigned)cg, 256, 0, s>>>(b, hf.leaves);
+    launch_pdl(k_bw_cuts, cg, 256, s, b, hf.leaves);
     BRDC_CUDA(h, "brdc.bw.cuts", cudaGetLastError());
     return BRDC_STATUS_SUCCESS;
 }
