@@ -191,6 +191,27 @@ __global__ void __launch_bounds__(256) k_vec_build(VArgs a, long long total_n) {
         const int pos = vec_pos(w, gs, po, s, K, ndz, ndg);
         double *dst = a.top ? a.out + (long long)pos * a.ldout
                             : a.out + gs * a.out_stride + (long long)pos * m;
+        if (s < K + ndz) {
+            // small-z deflated: the child eigenvector in its half, zeros in
+            // the other, written once (no zero pass and read-back)
+            const int e = vec_row_small(w, gs, s - K);
+            const bool left = e < m1;
+            const int r0 = left ? 0 : m1, r1 = left ? m1 : m;
+            const double *c =
+                a.leafchild ? a.child + (gs + e) * 16
+                            : (left ? a.child + gs * a.child_stride + (long long)e * m1
+                                    : a.child + (gs + m1) * a.child_stride +
+                                          (long long)(e - m1) * (m - m1));
+            for (int r = lane; r < m; r += 32) {
+                double v = 0.0;
+                if (r >= r0 && r < r1) {
+                    v = c[r - r0];
+                    v = a.top ? v * a.sgn[r] : v;
+                }
+                dst[r] = v;
+            }
+            continue;
+        }
         for (int r = lane; r < m; r += 32) {
             dst[r] = 0.0;
         }
@@ -215,10 +236,6 @@ __global__ void __launch_bounds__(256) k_vec_build(VArgs a, long long total_n) {
                 }
             }
         };
-        if (s < K + ndz) {
-            add_child(vec_row_small(w, gs, s - K), 1.0);
-            continue;
-        }
         const int act = w.gpos[gs + (s - K - ndz)];
         int b0 = act;
         while (b0 > 0 && w.gmark[gs + b0] != 0) {
