@@ -2077,10 +2077,9 @@ extern "C" brdc_status brdc_dstebr_vectors(brdc_handle h, int64_t n, const doubl
                            256, 0, s>>>(va);
             BRDC_CUDA(h, "brdc.vectors.lowner", cudaGetLastError());
         }
-        if (Km > 0) {
-            BRDC_CUDA(h, "brdc.vectors.zero",
-                      cudaMemsetAsync(M, 0, sizeof(double) * (size_t)n * (size_t)Km, s));
-        }
+        // M needs no clearing: k_vec_build writes every row of a root
+        // column that k_vec_gemm reads (the poles and the members rotated
+        // into them, its listed rows), and nothing else of M is read
         // root columns of M; the deflated eigenvectors straight to the blocks
         k_vec_build<<<(unsigned)eg, 256, 0, s>>>(va, n);
         BRDC_CUDA(h, "brdc.vectors.build", cudaGetLastError());

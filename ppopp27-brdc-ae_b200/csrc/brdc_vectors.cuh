@@ -176,7 +176,8 @@ __global__ void __launch_bounds__(256) k_vec_build(VArgs a, long long total_n) {
                     const long long xg = gs + b0 + kk;
                     const double cc = w.gc[xg], ss = w.gs[xg];
                     const int rx = vec_row_active(w, gs, b0 + kk);
-                    const double vx = col[rx];
+                    // a member is no pole: its row of the column starts at 0
+                    const double vx = 0.0;
                     col[rx] = ss * vb + cc * vx;
                     vb = cc * vb - ss * vx;
                 }
