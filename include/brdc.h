@@ -255,7 +255,7 @@ typedef struct brdc_timings {
  *                       sweep kernel); 0 disables it
  * brdc_autotune picks them by timing; defaults: subtree_levels = -1 (5 for
  * a batch of at least 1024 rows per SM, else by tree height: 3 up to
- * n = 16384, 4 up to 32768, 5 above), 16, 303104,
+ * n = 32768, 5 above), 16, 303104,
  * fused_level_rows = 2^30 (every level). */
 typedef struct brdc_tuning {
     int subtree_levels;
