@@ -80,13 +80,18 @@ __device__ __forceinline__ void leaf_round(double (&a)[16], double &v0,
     const bool isp = x < (x ^ M);
     const double mydiag = a[0];
     const double odiag = __shfl_xor_sync(kFull, mydiag, M);
+    // both lanes of a pair compute the rotation from the same three numbers
+    // (the lower column's off-diagonal entry), so both columns turn by
+    // exactly the same plane rotation without exchanging it
     const double apq_mine = a[M];
+    const double apq_o = __shfl_xor_sync(kFull, apq_mine, M);
+    const double apq = isp ? apq_mine : apq_o;
     const double app = isp ? mydiag : odiag;
     const double aqq = isp ? odiag : mydiag;
     double c = 1.0, sn = 0.0, t = 0.0;
     int rot = 0;
-    if (fabs(apq_mine) > th) {
-        const double theta = (aqq - app) / (2.0 * apq_mine);
+    if (fabs(apq) > th) {
+        const double theta = (aqq - app) / (2.0 * apq);
         if (fabs(theta) > 1.0e150) {
             t = 0.5 / theta;
         } else {
@@ -96,22 +101,6 @@ __device__ __forceinline__ void leaf_round(double (&a)[16], double &v0,
         sn = __dmul_rn(t, c);
         rot = 1;
     }
-    // the lane holding the larger index adopts its partner's rotation, so
-    // both columns of a pair turn by exactly the same plane rotation
-    {
-        const double co = __shfl_xor_sync(kFull, c, M);
-        const double so = __shfl_xor_sync(kFull, sn, M);
-        const double to = __shfl_xor_sync(kFull, t, M);
-        const int ro = __shfl_xor_sync(kFull, rot, M);
-        if (!isp) {
-            c = co;
-            sn = so;
-            t = to;
-            rot = ro;
-        }
-    }
-    const double apq_o = __shfl_xor_sync(kFull, apq_mine, M);
-    const double apq = isp ? apq_mine : apq_o;
     // columns: B = A J  (col p: c*col_p - s*col_q, col q: s*col_p + c*col_q)
     const double sgx = isp ? -1.0 : 1.0;
     double b[16];
@@ -260,13 +249,18 @@ __device__ __forceinline__ void leaf_round_v(double (&a)[16], double (&v)[16],
     const bool isp = x < (x ^ M);
     const double mydiag = a[0];
     const double odiag = __shfl_xor_sync(kFull, mydiag, M);
+    // both lanes of a pair compute the rotation from the same three numbers
+    // (the lower column's off-diagonal entry), so both columns turn by
+    // exactly the same plane rotation without exchanging it
     const double apq_mine = a[M];
+    const double apq_o = __shfl_xor_sync(kFull, apq_mine, M);
+    const double apq = isp ? apq_mine : apq_o;
     const double app = isp ? mydiag : odiag;
     const double aqq = isp ? odiag : mydiag;
     double c = 1.0, sn = 0.0, t = 0.0;
     int rot = 0;
-    if (fabs(apq_mine) > th) {
-        const double theta = (aqq - app) / (2.0 * apq_mine);
+    if (fabs(apq) > th) {
+        const double theta = (aqq - app) / (2.0 * apq);
         if (fabs(theta) > 1.0e150) {
             t = 0.5 / theta;
         } else {
@@ -276,20 +270,6 @@ __device__ __forceinline__ void leaf_round_v(double (&a)[16], double (&v)[16],
         sn = __dmul_rn(t, c);
         rot = 1;
     }
-    {
-        const double co = __shfl_xor_sync(kFull, c, M);
-        const double so = __shfl_xor_sync(kFull, sn, M);
-        const double to = __shfl_xor_sync(kFull, t, M);
-        const int ro = __shfl_xor_sync(kFull, rot, M);
-        if (!isp) {
-            c = co;
-            sn = so;
-            t = to;
-            rot = ro;
-        }
-    }
-    const double apq_o = __shfl_xor_sync(kFull, apq_mine, M);
-    const double apq = isp ? apq_mine : apq_o;
     const double sgx = isp ? -1.0 : 1.0;
     double b[16];
 #pragma unroll
