@@ -74,6 +74,8 @@ EXPORTS = (
     "brdc_get_limits",
     "brdc_dstebr_noalloc_get_info",
     "brdc_get_merge_trace",
+    "brdc_set_graphs",
+    "brdc_get_last_launches",
 )
 
 
@@ -221,6 +223,8 @@ def load() -> ctypes.CDLL:
     lib.brdc_get_merge_trace.argtypes = [vp, vp, sz, i64, ctypes.c_int, dpp, dpp, ip, ip, ip,
                                          dpp, dpp, ip, dpp, dpp]
     lib.brdc_get_limits.argtypes = [vp, ctypes.POINTER(Limits)]
+    lib.brdc_set_graphs.argtypes = [vp, ctypes.c_int]
+    lib.brdc_get_last_launches.argtypes = [vp, ip, ip]
     for f in ("brdc_create", "brdc_destroy", "brdc_set_stream", "brdc_get_stream",
               "brdc_get_last_error", "brdc_dstebr_workspace_size", "brdc_dstebr",
               "brdc_dstebr_backward", "brdc_get_info", "brdc_get_diagnostics",
@@ -229,7 +233,7 @@ def load() -> ctypes.CDLL:
               "brdc_dstebr_batched_checkpoint_workspace_size", "brdc_dstebr_batched_backward",
               "brdc_set_tuning", "brdc_get_tuning", "brdc_autotune",
               "brdc_set_limits", "brdc_get_limits", "brdc_dstebr_noalloc_get_info",
-              "brdc_get_merge_trace"):
+              "brdc_get_merge_trace", "brdc_set_graphs", "brdc_get_last_launches"):
         getattr(lib, f).restype = ctypes.c_int
     _lib = lib
     return lib
@@ -364,6 +368,20 @@ class Solver:
         t = Timings()
         _check(load().brdc_get_last_timings(self.h, ctypes.byref(t)), "get_last_timings", self.h)
         return t.as_dict()
+
+    def set_graphs(self, enable: bool) -> None:
+        """Graph replay of repeated plain solves (brdc_set_graphs; on by
+        default)."""
+        _check(load().brdc_set_graphs(self.h, 1 if enable else 0), "set_graphs", self.h)
+
+    def last_launches(self) -> dict:
+        """Kernels the last plain solve ran, and whether it was a graph
+        replay (brdc_get_last_launches; synchronises the stream)."""
+        n = ctypes.c_int(0)
+        r = ctypes.c_int(0)
+        _check(load().brdc_get_last_launches(self.h, ctypes.byref(n), ctypes.byref(r)),
+               "get_last_launches", self.h)
+        return {"launches": n.value, "replayed": bool(r.value)}
 
     def workspace(self, n: int, flags: int = 0):
         key = ("single", int(n), int(flags))

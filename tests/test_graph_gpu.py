@@ -1,0 +1,141 @@
+"""Graph replay of the plain solve (brdc_set_graphs): a call that repeats
+the previous plain call's arguments is captured as a CUDA graph and
+replayed.  The replay runs the same kernels on the same arguments, so its
+eigenvalues are bit for bit those of ordinary launches."""
+import numpy as np
+import pytest
+
+from brdc import families
+
+pytestmark = pytest.mark.gpu
+
+
+def buffers(d, e):
+    import torch
+
+    n = len(d)
+    D = torch.tensor(d, device="cuda")
+    E = torch.tensor(e if len(e) else np.zeros(1), device="cuda")
+    W = torch.empty(n, dtype=torch.float64, device="cuda")
+    return D, E, W
+
+
+@pytest.mark.parametrize("family,n", [("uniform", 65536), ("normal", 40000),
+                                      ("toeplitz", 16384), ("clustered", 8192)])
+def test_replay_matches_ordinary_launches(family, n):
+    import brdc
+
+    d, e = families.generate(family, n)
+    s = brdc.Solver()
+    try:
+        D, E, W = buffers(d, e)
+        ws = s.workspace(n)
+        s.set_graphs(False)
+        s.dstebr(D, E, W=W, workspace=ws)
+        eager = W.cpu().numpy().copy()
+        eager_launches = s.last_launches()
+        assert not eager_launches["replayed"]
+        s.set_graphs(True)
+        s.dstebr(D, E, W=W, workspace=ws)  # first call of the signature: ordinary
+        assert not s.last_launches()["replayed"]
+        for _ in range(3):  # captured, then replayed
+            W.fill_(0.0)
+            s.dstebr(D, E, W=W, workspace=ws)
+            rec = s.last_launches()
+            assert rec["replayed"]
+            assert s.info(n, ws) == 0
+            assert np.array_equal(W.cpu().numpy(), eager)
+            assert rec["launches"] == eager_launches["launches"]
+    finally:
+        s.close()
+
+
+def test_new_arguments_drop_the_graph():
+    import brdc
+    import torch
+
+    n = 8192
+    d, e = families.generate("normal", n)
+    s = brdc.Solver()
+    try:
+        D, E, W = buffers(d, e)
+        ws = s.workspace(n)
+        for _ in range(3):
+            s.dstebr(D, E, W=W, workspace=ws)
+        assert s.last_launches()["replayed"]
+        ref = W.cpu().numpy().copy()
+        W2 = torch.empty_like(W)
+        s.dstebr(D, E, W=W2, workspace=ws)  # another W: ordinary launches
+        assert not s.last_launches()["replayed"]
+        assert np.array_equal(W2.cpu().numpy(), ref)
+        # same pointers, new values: the replay reads them
+        d2, e2 = families.generate("uniform", n)
+        D.copy_(torch.tensor(d2))
+        E.copy_(torch.tensor(e2))
+        s.dstebr(D, E, W=W2, workspace=ws)
+        s.dstebr(D, E, W=W2, workspace=ws)
+        assert s.last_launches()["replayed"]
+        plain = brdc.Solver()
+        try:
+            plain.set_graphs(False)
+            W3 = plain.dstebr(D, E)
+            assert np.array_equal(W2.cpu().numpy(), W3.cpu().numpy())
+        finally:
+            plain.close()
+        assert not np.array_equal(W2.cpu().numpy(), ref)
+    finally:
+        s.close()
+
+
+def test_caller_capture_uses_ordinary_launches():
+    """Inside the caller's own stream capture the solve is captured as plain
+    launches into the caller's graph."""
+    import brdc
+    import torch
+
+    n = 16384
+    d, e = families.generate("uniform", n)
+    s = brdc.Solver()
+    try:
+        D, E, W = buffers(d, e)
+        ws = s.workspace(n)
+        stream = torch.cuda.Stream()
+        stream.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(stream):
+            s.set_stream(stream)
+            s.dstebr(D, E, W=W, workspace=ws)
+            s.dstebr(D, E, W=W, workspace=ws)
+            stream.synchronize()
+            ref = W.cpu().numpy().copy()
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=stream):
+                s.dstebr(D, E, W=W, workspace=ws)
+            W.fill_(0.0)
+            g.replay()
+            stream.synchronize()
+            assert np.array_equal(W.cpu().numpy(), ref)
+            del g
+        s.set_stream(None)
+    finally:
+        s.close()
+
+
+def test_timing_mode_uses_ordinary_launches():
+    import brdc
+
+    n = 16384
+    d, e = families.generate("uniform", n)
+    s = brdc.Solver()
+    try:
+        D, E, W = buffers(d, e)
+        ws = s.workspace(n)
+        for _ in range(3):
+            s.dstebr(D, E, W=W, workspace=ws)
+        s.set_timing(True)
+        s.dstebr(D, E, W=W, workspace=ws)
+        t = s.last_timings()
+        assert not s.last_launches()["replayed"]
+        assert t["launches"] == s.last_launches()["launches"]
+        s.set_timing(False)
+    finally:
+        s.close()
