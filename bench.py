@@ -9,8 +9,9 @@ and E already resident in HBM; L2 is flushed (256 MiB write) before every
 timed solve, outside the timed interval, and each solve is timed with CUDA
 events on its stream.  value = mean ms per solve (lower is better).
 
-Also reported on the same line: the e2e time through the C ABI with pinned
-host buffers (H2D of D and E, solve, D2H of W inside the timed interval),
+Also reported on the same line: the e2e time through the C ABI's
+host-buffer entry brdc_dstebr_host with pinned buffers (H2D of D and E,
+solve, D2H of W inside the timed interval),
 the per-phase roofline of the dominant kernel (FP64 pipe or HBM), the other
 three families at the same order, accuracy against the oracle, workspace
 bytes, clocks sampled during the timed loop, and the CPU baseline: the
@@ -432,17 +433,37 @@ def bench_config2(torch, families, solver, flush):
 
 
 def measure_e2e(torch, solver, D, E, W, ws, d, e, flush, warmup, steps):
-    """The solve end to end through the C ABI: pinned host D and E copied in,
-    the solve, W copied back, all inside the timed interval.  D and E travel
-    as one pinned buffer [D | E] in one copy; the solve's D and E pointers
-    address the two parts of its device image."""
+    """The solve end to end through the C ABI's host-buffer entry
+    (brdc_dstebr_host): pinned host D and E copied in, the solve, W copied
+    back, all inside the timed interval.  D, E and W are the device-entry
+    arguments of the headline line: their solve is the reference for the
+    host entry's result, and the same end-to-end interval is also timed
+    through the device entry with the copies made by the caller."""
     n = len(d)
+    solver.dstebr(D, E, W=W, workspace=ws)
+    ref = W.cpu().numpy()
+    # one pinned buffer [D | E]: the entry copies it in one piece
     hDE = torch.cat([torch.tensor(d), torch.tensor(e, dtype=torch.float64)]).pin_memory()
-    DE = torch.empty(hDE.numel(), dtype=torch.float64, device=D.device)
-    Dv, Ev = DE[:n], DE[n:]
+    hD, hE = hDE[:n], hDE[n:]
     hW = torch.empty(n, dtype=torch.float64).pin_memory()
+    hws = solver.host_workspace(n)
     stream = torch.cuda.current_stream()
     e2e = []
+    for i in range(warmup + steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        solver.dstebr_host(hD, hE, W=hW, workspace=hws)
+        e1.record(stream)
+        e1.synchronize()
+        if i >= warmup:
+            e2e.append(e0.elapsed_time(e1))
+    err = float(np.max(np.abs(hW.numpy() - ref)))
+    # the same through the device entry, the copies made by the caller
+    DE = torch.empty(n + len(e), dtype=torch.float64, device=D.device)
+    Dv, Ev = DE[:n], DE[n:]
+    dev = []
     for i in range(warmup + steps):
         flush.zero_()
         e0 = torch.cuda.Event(enable_timing=True)
@@ -454,10 +475,13 @@ def measure_e2e(torch, solver, D, E, W, ws, d, e, flush, warmup, steps):
         e1.record(stream)
         e1.synchronize()
         if i >= warmup:
-            e2e.append(e0.elapsed_time(e1))
+            dev.append(e0.elapsed_time(e1))
     return {"value": float(np.mean(e2e)), "unit": "ms",
-            "h2d_bytes_per_step": int(hDE.numel() * 8),
-            "d2h_bytes_per_step": int(hW.numel() * 8)}
+            "h2d_bytes_per_step": int((hD.numel() + hE.numel()) * 8),
+            "d2h_bytes_per_step": int(hW.numel() * 8),
+            "entry": "brdc_dstebr_host (pinned host buffers)",
+            "max_abs_diff_vs_device_entry": err,
+            "device_entry_with_caller_copies_ms": float(np.mean(dev))}
 
 
 def load_workload(input_path, data_spec):

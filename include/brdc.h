@@ -321,6 +321,27 @@ brdc_status brdc_get_last_timings(brdc_handle handle, brdc_timings *out);
 brdc_status brdc_set_graphs(brdc_handle handle, int enable);
 brdc_status brdc_get_last_launches(brdc_handle handle, int *launches, int *replayed);
 
+/* brdc_dstebr on host buffers: D[n], E[n-1] in host memory -> W[n] in host
+ * memory, through device images of D, E and W kept in the caller's
+ * workspace after the solve's own (brdc_dstebr_host_workspace_size; the
+ * workspace takes no checkpoints).  Same checks and statuses as
+ * brdc_dstebr.  The copies in (one when E lies right after D in one host
+ * buffer, h_E == h_D + n; else two), the solve and the copy out are
+ * enqueued on the handle's stream; W is valid once the stream has
+ * synchronised.  With
+ * page-locked buffers (cudaMallocHost, cudaHostAlloc, cudaHostRegister)
+ * the call does not block the host; pageable buffers are staged by the
+ * runtime, which blocks it.  The solve itself is brdc_dstebr's on the
+ * device images, so a repeated call with the same workspace replays its
+ * graph.  No reference counterpart: the reference's LAPACK-style host
+ * entry allocates and frees device memory on every call
+ * (cpu/src/dstedc_dc_br.f:7-75 has the interface; brdc_dstedc_dc_br_ below
+ * keeps that behaviour). */
+brdc_status brdc_dstebr_host_workspace_size(int64_t n, size_t *bytes);
+brdc_status brdc_dstebr_host(brdc_handle handle, int64_t n, const double *h_D,
+                             const double *h_E, double *h_W, void *workspace,
+                             size_t workspace_size);
+
 /* LAPACK-style host entry with the argument list and workspace-query
  * semantics of DSTEDC_DC_BR (cpu/src/dstedc_dc_br.f:7-75): LWORK = -1 or
  * LIWORK = -1 returns LWMIN = max(1,(16+2*NTHR)*N) in WORK(1) and

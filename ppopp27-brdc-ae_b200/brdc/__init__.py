@@ -76,6 +76,8 @@ EXPORTS = (
     "brdc_get_merge_trace",
     "brdc_set_graphs",
     "brdc_get_last_launches",
+    "brdc_dstebr_host_workspace_size",
+    "brdc_dstebr_host",
 )
 
 
@@ -225,6 +227,8 @@ def load() -> ctypes.CDLL:
     lib.brdc_get_limits.argtypes = [vp, ctypes.POINTER(Limits)]
     lib.brdc_set_graphs.argtypes = [vp, ctypes.c_int]
     lib.brdc_get_last_launches.argtypes = [vp, ip, ip]
+    lib.brdc_dstebr_host_workspace_size.argtypes = [i64, ctypes.POINTER(sz)]
+    lib.brdc_dstebr_host.argtypes = [vp, i64, vp, vp, vp, vp, sz]
     for f in ("brdc_create", "brdc_destroy", "brdc_set_stream", "brdc_get_stream",
               "brdc_get_last_error", "brdc_dstebr_workspace_size", "brdc_dstebr",
               "brdc_dstebr_backward", "brdc_get_info", "brdc_get_diagnostics",
@@ -233,7 +237,8 @@ def load() -> ctypes.CDLL:
               "brdc_dstebr_batched_checkpoint_workspace_size", "brdc_dstebr_batched_backward",
               "brdc_set_tuning", "brdc_get_tuning", "brdc_autotune",
               "brdc_set_limits", "brdc_get_limits", "brdc_dstebr_noalloc_get_info",
-              "brdc_get_merge_trace", "brdc_set_graphs", "brdc_get_last_launches"):
+              "brdc_get_merge_trace", "brdc_set_graphs", "brdc_get_last_launches",
+              "brdc_dstebr_host_workspace_size", "brdc_dstebr_host"):
         getattr(lib, f).restype = ctypes.c_int
     _lib = lib
     return lib
@@ -409,6 +414,40 @@ class Solver:
             ctypes.c_void_p(W.data_ptr()), ctypes.c_void_p(ws.data_ptr()), ws.numel(),
         )
         _check(st, "brdc_dstebr", self.h)
+        return W
+
+    def host_workspace(self, n: int):
+        """Device workspace of dstebr_host (brdc_dstebr_host_workspace_size)."""
+        key = ("host", int(n))
+        ws = self._ws.get(key)
+        if ws is None:
+            nb = ctypes.c_size_t(0)
+            _check(load().brdc_dstebr_host_workspace_size(int(n), ctypes.byref(nb)),
+                   "brdc_dstebr_host_workspace_size")
+            ws = self._torch.empty(nb.value, dtype=self._torch.uint8, device="cuda")
+            self._ws[key] = ws
+        return ws
+
+    def dstebr_host(self, D, E, W=None, workspace=None):
+        """dstebr on host (CPU) float64 tensors: D and E are copied in, the
+        eigenvalues copied back into W (allocated pinned when None).  The call
+        only enqueues; W is valid once the handle's stream has synchronised.
+        Pinned tensors (pin_memory()) keep it from blocking the host
+        (brdc_dstebr_host)."""
+        torch = self._torch
+        n = D.shape[0]
+        if D.dtype != torch.float64 or D.is_cuda or not D.is_contiguous():
+            raise TypeError("D must be a contiguous float64 CPU tensor")
+        if n > 1 and (E is None or E.dtype != torch.float64 or E.is_cuda or not E.is_contiguous()):
+            raise TypeError("E must be a contiguous float64 CPU tensor")
+        if W is None:
+            W = torch.empty(n, dtype=torch.float64).pin_memory()
+        ws = self.host_workspace(n) if workspace is None else workspace
+        e_ptr = E.data_ptr() if n > 1 else None
+        st = load().brdc_dstebr_host(self.h, n, ctypes.c_void_p(D.data_ptr()),
+                                     ctypes.c_void_p(e_ptr), ctypes.c_void_p(W.data_ptr()),
+                                     ctypes.c_void_p(ws.data_ptr()), ws.numel())
+        _check(st, "brdc_dstebr_host", self.h)
         return W
 
     def dstebr_vectors(self, D, E, workspace=None):

@@ -950,6 +950,21 @@ brdc_status solve_graph(brdc_handle h, const HostForest &hf, const Layout &L, co
     return BRDC_STATUS_SUCCESS;
 }
 
+// brdc_dstebr after its checks: a graph replay where solve_graph takes the
+// call, else the stream launches.
+brdc_status plain_solve(brdc_handle h, const HostForest &hf, const Layout &L, const Forest &F,
+                        const Ws &w, const double *D, const double *E, double *W, void *ws,
+                        size_t ws_size, bool ckpt) {
+    if (!ckpt && h->graphs && !h->timing) {
+        bool done = false;
+        const brdc_status st = solve_graph(h, hf, L, F, w, D, E, W, ws, ws_size, &done);
+        if (done) {
+            return st;
+        }
+    }
+    return run_forest(h, hf, L, F, w, D, E, W);
+}
+
 } // namespace
 
 // ------------------------------------------------------------------ C ABI
@@ -1166,15 +1181,115 @@ extern "C" brdc_status brdc_dstebr(brdc_handle h, int64_t n, const double *d_D,
     F.max_levels = hf.max_levels;
     F.n0 = n;
     F.L0 = hf.max_levels;
-    if (!ckpt && h->graphs && !h->timing) {
-        bool done = false;
-        const brdc_status st = solve_graph(h, hf, L, F, w, d_D, d_E, d_W, workspace,
-                                           workspace_size, &done);
-        if (done) {
-            return st;
+    return plain_solve(h, hf, L, F, w, d_D, d_E, d_W, workspace, workspace_size, ckpt);
+}
+
+namespace {
+
+// Workspace of brdc_dstebr_host: the plain solve's, then the device images
+// [D | E] back to back (so that a host buffer holding E right after D is
+// one copy) and W, each part 256-byte aligned.
+struct HostLayout {
+    size_t d, e, w, bytes;
+};
+
+HostLayout host_layout(long long n, const HostForest &hf) {
+    HostLayout H;
+    H.d = align_up(make_layout(hf, false).bytes);
+    H.e = H.d + sizeof(double) * n;
+    H.w = align_up(H.e + sizeof(double) * std::max(n - 1, 1LL));
+    H.bytes = H.w + align_up(sizeof(double) * n);
+    return H;
+}
+
+} // namespace
+
+extern "C" brdc_status brdc_dstebr_host_workspace_size(int64_t n, size_t *bytes) {
+    if (bytes == nullptr) {
+        return BRDC_STATUS_INVALID_POINTER;
+    }
+    if (n <= 0 || n > (1LL << 30)) {
+        return BRDC_STATUS_INVALID_VALUE;
+    }
+    const long long off[2] = {0, (long long)n};
+    HostForest hf;
+    if (!build_forest(1, off, &hf)) {
+        return BRDC_STATUS_INVALID_VALUE;
+    }
+    *bytes = host_layout(n, hf).bytes;
+    return BRDC_STATUS_SUCCESS;
+}
+
+extern "C" brdc_status brdc_dstebr_host(brdc_handle h, int64_t n, const double *h_D,
+                                        const double *h_E, double *h_W, void *workspace,
+                                        size_t workspace_size) {
+    if (h == nullptr) {
+        return BRDC_STATUS_INVALID_HANDLE;
+    }
+    if (h_D == nullptr || h_W == nullptr || (n > 1 && h_E == nullptr)) {
+        return BRDC_STATUS_INVALID_POINTER;
+    }
+    if (n <= 0 || n > (1LL << 30)) {
+        return BRDC_STATUS_INVALID_VALUE;
+    }
+    const long long off[2] = {0, (long long)n};
+    HostForest hf;
+    if (!build_forest(1, off, &hf)) {
+        return BRDC_STATUS_INVALID_VALUE;
+    }
+    const HostLayout H = host_layout(n, hf);
+    if (workspace == nullptr || workspace_size < H.bytes) {
+        return BRDC_STATUS_INVALID_WORKSPACE;
+    }
+    char *base = static_cast<char *>(workspace);
+    double *dD = reinterpret_cast<double *>(base + H.d);
+    double *dE = reinterpret_cast<double *>(base + H.e);
+    double *dW = reinterpret_cast<double *>(base + H.w);
+    const Layout L = make_layout(hf, false);
+    const Ws w = carve(workspace, hf, false);
+    Forest F{};
+    F.B = 1;
+    F.max_levels = hf.max_levels;
+    F.n0 = n;
+    F.L0 = hf.max_levels;
+    // stream copies around the device entry's solve (a graph replay from
+    // the second call with this workspace on)
+    // E right after D in the caller's memory: one copy of [D | E].  Two
+    // separate page-locked allocations can also lie back to back, and the
+    // runtime refuses a copy across them (an error it returns at once, with
+    // nothing enqueued): then the two copies below.  Inside the caller's
+    // stream capture a refused call would end the capture, so there the
+    // copies are always two.
+    bool joint = false;
+    if (n > 1 && h_E == h_D + n) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusActive;
+        if (cudaStreamIsCapturing(h->stream, &cs) == cudaSuccess &&
+            cs == cudaStreamCaptureStatusNone) {
+            joint = cudaMemcpyAsync(dD, h_D, sizeof(double) * (2 * n - 1),
+                                    cudaMemcpyHostToDevice, h->stream) == cudaSuccess;
+        }
+        if (!joint) {
+            cudaGetLastError();
         }
     }
-    return run_forest(h, hf, L, F, w, d_D, d_E, d_W);
+    if (!joint) {
+        BRDC_CUDA(h, "brdc.host.copy_d",
+                  cudaMemcpyAsync(dD, h_D, sizeof(double) * n, cudaMemcpyHostToDevice,
+                                  h->stream));
+        if (n > 1) {
+            BRDC_CUDA(h, "brdc.host.copy_e",
+                      cudaMemcpyAsync(dE, h_E, sizeof(double) * (n - 1), cudaMemcpyHostToDevice,
+                                      h->stream));
+        }
+    }
+    const brdc_status st = plain_solve(h, hf, L, F, w, dD, dE, dW, workspace, workspace_size,
+                                       false);
+    if (st != BRDC_STATUS_SUCCESS) {
+        return st;
+    }
+    BRDC_CUDA(h, "brdc.host.copy_w",
+              cudaMemcpyAsync(h_W, dW, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+    return BRDC_STATUS_SUCCESS;
 }
 
 namespace {

@@ -139,3 +139,64 @@ def test_timing_mode_uses_ordinary_launches():
         s.set_timing(False)
     finally:
         s.close()
+
+
+@pytest.mark.parametrize("layout", ["pinned", "pageable", "joint"])
+def test_host_entry_matches_device_entry(layout):
+    """brdc_dstebr_host: the copies in, the solve and the copy out give the
+    device entry's eigenvalues bit for bit, with pinned or pageable buffers;
+    from the second call on the solve is a graph replay."""
+    import brdc
+    import torch
+
+    n = 32768
+    d, e = families.generate("normal", n)
+    s = brdc.Solver()
+    try:
+        D, E, W = buffers(d, e)
+        s.dstebr(D, E, W=W, workspace=s.workspace(n))
+        ref = W.cpu().numpy().copy()
+        hD = torch.tensor(d)
+        hE = torch.tensor(e)
+        hW = torch.empty(n, dtype=torch.float64)
+        if layout == "pinned":
+            hD, hE, hW = hD.pin_memory(), hE.pin_memory(), hW.pin_memory()
+        elif layout == "joint":  # E right after D in one buffer: one copy in
+            hDE = torch.cat([hD, hE]).pin_memory()
+            hD, hE, hW = hDE[:n], hDE[n:], hW.pin_memory()
+        for i in range(4):
+            hW.fill_(0.0)
+            s.dstebr_host(hD, hE, W=hW)
+            torch.cuda.current_stream().synchronize()
+            s.stream.synchronize()
+            assert np.array_equal(hW.numpy(), ref)
+            assert s.last_launches()["replayed"] == (i >= 1)
+        # new values in the same pinned buffers reach the replay
+        d2, e2 = families.generate("uniform", n)
+        hD.copy_(torch.tensor(d2))
+        hE.copy_(torch.tensor(e2))
+        s.dstebr_host(hD, hE, W=hW)
+        s.stream.synchronize()
+        D.copy_(torch.tensor(d2))
+        E.copy_(torch.tensor(e2))
+        s.dstebr(D, E, W=W, workspace=s.workspace(n))
+        assert np.array_equal(hW.numpy(), W.cpu().numpy())
+    finally:
+        s.close()
+
+
+def test_host_entry_argument_checks():
+    import brdc
+    import torch
+
+    s = brdc.Solver()
+    try:
+        with pytest.raises(brdc.BrdcError) as ei:
+            s.dstebr_host(torch.zeros(8, dtype=torch.float64), torch.zeros(7, dtype=torch.float64),
+                          workspace=torch.empty(16, dtype=torch.uint8, device="cuda"))
+        assert ei.value.status == brdc.INVALID_WORKSPACE
+        w = s.dstebr_host(torch.tensor([3.0], dtype=torch.float64), None)
+        s.stream.synchronize()
+        assert w.numpy().tolist() == [3.0]
+    finally:
+        s.close()
