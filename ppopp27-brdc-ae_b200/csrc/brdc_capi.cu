@@ -497,7 +497,7 @@ void mark(brdc_handle h, int slot) {
 // Subtree depth of a solve: the handle's setting, or by default the depth
 // measured fastest on B200: 5 for a batch with at least two 512-row
 // subtrees per SM (the subtrees fill the GPU), otherwise by the forest's
-// tallest instance (3 up to 10 levels, i.e. n <= 16384; 4 at 11; 5 above).
+// tallest instance (3 up to 11 levels, i.e. n <= 32768; 5 above).
 int effective_sub_levels(brdc_handle h, const HostForest &hf) {
     if (h->sub_levels >= 0) {
         return h->sub_levels;
