@@ -200,3 +200,45 @@ def test_host_entry_argument_checks():
         assert w.numpy().tolist() == [3.0]
     finally:
         s.close()
+
+
+def test_replay_reports_failure_statuses():
+    """The status words work in a replay as in stream launches: a NaN put
+    into the same buffers between replays gives info = -4 from the replayed
+    k_norm, the next clean values solve again on the same graph, and an
+    iteration cap of 1 (a new signature: stream launches, then a new graph)
+    reports unconverged roots."""
+    import brdc
+    import torch
+
+    n = 16384
+    d, e = families.generate("normal", n)
+    s = brdc.Solver()
+    try:
+        D, E, W = buffers(d, e)
+        ws = s.workspace(n)
+        for _ in range(3):
+            s.dstebr(D, E, W=W, workspace=ws)
+        assert s.last_launches()["replayed"]
+        ref = W.cpu().numpy().copy()
+        D[n // 3] = float("nan")
+        s.dstebr(D, E, W=W, workspace=ws)
+        assert s.last_launches()["replayed"]
+        assert s.info_status(n, ws) == (-4, brdc.INTERNAL_ERROR)
+        D.copy_(torch.tensor(d))
+        s.dstebr(D, E, W=W, workspace=ws)
+        assert s.last_launches()["replayed"]
+        assert s.info_status(n, ws) == (0, brdc.SUCCESS)
+        assert np.array_equal(W.cpu().numpy(), ref)
+        s.set_limits(secular_max_iter=1)
+        for i in range(3):
+            s.dstebr(D, E, W=W, workspace=ws)
+            assert s.last_launches()["replayed"] == (i >= 1)
+            info, st = s.info_status(n, ws)
+            assert info > 0 and st == brdc.NOT_CONVERGED
+        s.set_limits(secular_max_iter=64)
+        s.dstebr(D, E, W=W, workspace=ws)
+        assert not s.last_launches()["replayed"]
+        assert np.array_equal(W.cpu().numpy(), ref)
+    finally:
+        s.close()
