@@ -242,3 +242,28 @@ def test_replay_reports_failure_statuses():
         assert np.array_equal(W.cpu().numpy(), ref)
     finally:
         s.close()
+
+
+@pytest.mark.parametrize("n", [1, 2, 16, 17, 33, 1000])
+def test_replay_small_orders(n):
+    """Orders whose tree is one leaf, one merge or a few levels replay like
+    the rest: the same bits as stream launches, call after call."""
+    import brdc
+
+    rng = np.random.default_rng(77 + n)
+    d, e = rng.standard_normal(n), rng.standard_normal(max(n - 1, 1))
+    s = brdc.Solver()
+    try:
+        D, E, W = buffers(d, e[: n - 1] if n > 1 else e)
+        ws = s.workspace(n)
+        s.set_graphs(False)
+        s.dstebr(D, E, W=W, workspace=ws)
+        ref = W.cpu().numpy().copy()
+        s.set_graphs(True)
+        for i in range(3):
+            W.fill_(0.0)
+            s.dstebr(D, E, W=W, workspace=ws)
+            assert s.last_launches()["replayed"] == (i >= 1)
+            assert np.array_equal(W.cpu().numpy(), ref)
+    finally:
+        s.close()
