@@ -305,19 +305,23 @@ brdc_status brdc_autotune(brdc_handle handle, int64_t count, const int64_t *offs
 brdc_status brdc_set_timing(brdc_handle handle, int enable);
 brdc_status brdc_get_last_timings(brdc_handle handle, brdc_timings *out);
 
-/* Graph replay of brdc_dstebr (on by default).  A plain call (no
- * checkpoints, timing off, the stream not being captured by the caller)
- * that repeats the previous plain call's signature -- order, D, E, W,
- * workspace and its size, tuning and limits -- is captured as a CUDA graph
- * on that second call and replayed from then on: the same kernels with the
- * same arguments, less launch processing.  New values in the same buffers
- * are read by the replay; any other change of the signature drops the
- * graph.  A failed capture falls back to ordinary launches for that
- * signature.  brdc_set_graphs(handle, 0) turns it off and drops the graph.
- * brdc_get_last_launches: kernels the last plain solve ran, and whether it
- * was a graph replay (replayed may be NULL).  No reference counterpart: the
- * reference launches every kernel from the host and synchronises on each
- * level's deflation count (gpu/src/tridiag_solver.cu:624-630). */
+/* Graph replay of repeated solves (on by default).  A call of brdc_dstebr
+ * or brdc_dstebr_backward (timing off, the stream not being captured by the
+ * caller) that repeats the previous call's signature for that entry --
+ * order, D, E, W (G, gD, gE and keep_forward for the adjoint), workspace and
+ * its size, tuning and limits -- is captured as a CUDA graph on that second
+ * call and replayed from then on: the same kernels with the same
+ * arguments, less launch processing.  One graph is kept for the forwards
+ * (plain, checkpointing, and the solve of brdc_dstebr_host) and one for the
+ * adjoint, so a loop of forward and adjoint replays both.  New values in
+ * the same buffers are read by the replay; any other change of the
+ * signature drops that graph.  A failed capture falls back to ordinary
+ * launches for that signature.  brdc_set_graphs(handle, 0) turns replay off
+ * and drops the graphs.  brdc_get_last_launches: kernels the last forward
+ * ran, and whether the last solve was a graph replay (replayed may be
+ * NULL).  No reference counterpart: the reference launches every kernel
+ * from the host and synchronises on each level's deflation count
+ * (gpu/src/tridiag_solver.cu:624-630). */
 brdc_status brdc_set_graphs(brdc_handle handle, int enable);
 brdc_status brdc_get_last_launches(brdc_handle handle, int *launches, int *replayed);
 

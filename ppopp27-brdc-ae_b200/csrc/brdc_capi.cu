@@ -26,39 +26,41 @@
 
 using namespace brdc;
 
-// A plain solve captured as a CUDA graph.  The graph holds every pointer and
+// A solve captured as a CUDA graph.  The graph holds every pointer and
 // launch shape of one call, so it is replayed only for calls with the same
 // signature.
 struct SolveSig {
+    int kind = 0; // 0: forward (plain or checkpointing), 1: adjoint
     long long n = 0;
     const double *D = nullptr, *E = nullptr;
     double *W = nullptr;
     void *ws = nullptr;
     size_t ws_size = 0;
+    const double *G = nullptr; // adjoint: G, gD, gE and keep_forward
+    double *gD = nullptr, *gE = nullptr;
+    int keep_forward = 0;
     int sub_levels = 0, defl_cluster = 0, lanes_target = 0, lvl_rows = 0, max_iter = 0;
     unsigned long long wait_ns = 0;
     bool operator==(const SolveSig &o) const {
-        return n == o.n && D == o.D && E == o.E && W == o.W && ws == o.ws &&
-               ws_size == o.ws_size && sub_levels == o.sub_levels &&
+        return kind == o.kind && n == o.n && D == o.D && E == o.E && W == o.W && ws == o.ws &&
+               ws_size == o.ws_size && G == o.G && gD == o.gD && gE == o.gE &&
+               keep_forward == o.keep_forward && sub_levels == o.sub_levels &&
                defl_cluster == o.defl_cluster && lanes_target == o.lanes_target &&
                lvl_rows == o.lvl_rows && max_iter == o.max_iter && wait_ns == o.wait_ns;
     }
 };
 
 struct SolveGraph {
-    SolveSig seen;                  // the last plain call's signature
+    SolveSig seen;                  // the last call's signature (of this kind)
     bool seen_valid = false;
     bool failed = false;            // capturing `seen` failed: no retry
     cudaGraph_t graph = nullptr;    // captured for `seen` on its second call
     cudaGraphExec_t exec = nullptr;
-    cudaStream_t cap = nullptr;     // captures the solve (the caller's stream
-                                    // may be the legacy stream, which cannot)
-    // what run_forest leaves on the host, restored by a replay
+    // what the enqueue leaves on the host, restored by a replay
     int launches = 0;
     int fused_levels = 0;
     int timed_levels = 0;
     int has_lowner[BRDC_MAX_LEVELS] = {};
-    bool replayed = false;          // the last plain call was a replay
 };
 
 struct brdc_handle_struct {
@@ -97,9 +99,14 @@ struct brdc_handle_struct {
     int timed_levels;
     int has_lowner[BRDC_MAX_LEVELS];
     int fused_levels;
-    // replay of the plain solve from a CUDA graph (brdc_set_graphs)
+    // graph replay of repeated solves (brdc_set_graphs): one graph for the
+    // forwards, one for the adjoints, so that a forward-and-adjoint loop
+    // replays both; the stream they are captured on (the caller's may be
+    // the legacy stream, which cannot be captured)
     int graphs = 1;
-    SolveGraph g;
+    SolveGraph gf, gb;
+    cudaStream_t gcap = nullptr;
+    bool replayed = false;          // the last solve was a replay
 };
 
 namespace {
@@ -658,7 +665,7 @@ brdc_status run_forest(brdc_handle h, const HostForest &hf, const Layout &L,
                        const double *E, double *W) {
     cudaStream_t s = h->stream;
     BRDC_CUDA(h, "brdc.set_attributes", set_attrs());
-    h->g.replayed = false;
+    h->replayed = false;
     h->ev_used = 0;
     h->launches = 0;
     h->timed_levels = hf.max_levels;
@@ -819,8 +826,7 @@ brdc_status run_forest(brdc_handle h, const HostForest &hf, const Layout &L,
     return BRDC_STATUS_SUCCESS;
 }
 
-void drop_graph(brdc_handle h) {
-    SolveGraph &g = h->g;
+void drop_graph(SolveGraph &g) {
     if (g.exec != nullptr) {
         cudaGraphExecDestroy(g.exec);
     }
@@ -829,15 +835,13 @@ void drop_graph(brdc_handle h) {
     }
     g.exec = nullptr;
     g.graph = nullptr;
-    g.replayed = false;
 }
 
-// Capture the plain solve into h->g and instantiate it.  On any failure nothing is
-// kept, the handle's error state is as before, and the caller launches the
-// solve as usual.
-bool capture_graph(brdc_handle h, const HostForest &hf, const Layout &L, const Forest &F,
-                   const Ws &w, const double *D, const double *E, double *W) {
-    SolveGraph &g = h->g;
+// Capture what enqueue() launches into g and instantiate it.  On any
+// failure nothing is kept, the handle's error state is as before, and the
+// caller launches the solve as usual.
+template <class Enqueue>
+bool capture_graph(brdc_handle h, SolveGraph &g, Enqueue enqueue) {
     const int code = h->last_code;
     const brdc_error_source src = h->last_src;
     const char *site = h->last_site;
@@ -851,15 +855,16 @@ bool capture_graph(brdc_handle h, const HostForest &hf, const Layout &L, const F
     if (set_attrs() != cudaSuccess) {
         return fail();
     }
-    if (g.cap == nullptr && cudaStreamCreateWithFlags(&g.cap, cudaStreamNonBlocking) != cudaSuccess) {
-        g.cap = nullptr;
+    if (h->gcap == nullptr &&
+        cudaStreamCreateWithFlags(&h->gcap, cudaStreamNonBlocking) != cudaSuccess) {
+        h->gcap = nullptr;
         return fail();
     }
     cudaGraph_t graph = nullptr;
     if (cudaGraphCreate(&graph, 0) != cudaSuccess) {
         return fail();
     }
-    if (cudaStreamBeginCaptureToGraph(g.cap, graph, nullptr, nullptr, 0,
+    if (cudaStreamBeginCaptureToGraph(h->gcap, graph, nullptr, nullptr, 0,
                                       cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
         cudaGraphDestroy(graph);
         return fail();
@@ -867,12 +872,11 @@ bool capture_graph(brdc_handle h, const HostForest &hf, const Layout &L, const F
     // the graph records kernels only, so the stream it is captured on does
     // not matter for its replays on the caller's stream
     cudaStream_t user = h->stream;
-    h->stream = g.cap;
-    g.graph = graph;
-    const brdc_status st = run_forest(h, hf, L, F, w, D, E, W);
+    h->stream = h->gcap;
+    const brdc_status st = enqueue();
     h->stream = user;
     cudaGraph_t out = nullptr;
-    const cudaError_t ec = cudaStreamEndCapture(g.cap, &out);
+    const cudaError_t ec = cudaStreamEndCapture(h->gcap, &out);
     cudaGraphExec_t exec = nullptr;
     if (st != BRDC_STATUS_SUCCESS || ec != cudaSuccess || out != graph ||
         cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
@@ -880,9 +884,9 @@ bool capture_graph(brdc_handle h, const HostForest &hf, const Layout &L, const F
             cudaGraphExecDestroy(exec);
         }
         cudaGraphDestroy(graph);
-        g.graph = nullptr;
         return fail();
     }
+    g.graph = graph;
     g.exec = exec;
     g.launches = h->launches;
     g.fused_levels = h->fused_levels;
@@ -891,19 +895,23 @@ bool capture_graph(brdc_handle h, const HostForest &hf, const Layout &L, const F
     return true;
 }
 
-// The plain solve as a graph replay, when this call repeats the previous
-// plain call's signature (pointers, order, workspace, tuning and limits):
+// A solve as a graph replay, when this call repeats the previous call's
+// signature of its kind (pointers, order, workspace, tuning and limits):
 // captured on that second call, replayed from then on.  A replay runs the
 // same kernels with the same arguments and programmatic edges, and saves
-// the launch processing of each (uniform 65,536 on B200: 0.742 -> 0.725 ms
-// in a probe with a caller-side graph).  *done = false hands the call to the
-// ordinary launches: the first call of a signature, a stream the caller is
-// capturing (its own graph then holds the launches), or a failed capture.
-brdc_status solve_graph(brdc_handle h, const HostForest &hf, const Layout &L, const Forest &F,
-                        const Ws &w, const double *D, const double *E, double *W, void *ws,
-                        size_t ws_size, bool *done) {
+// the launch processing of each (uniform 65,536 on B200: 0.742 -> 0.725 ms).
+// *done = false hands the call to the ordinary launches: replay switched
+// off, phase timing on, a stream the caller is capturing (its own graph
+// then holds the launches), the first call of a signature, or a failed
+// capture.
+template <class Enqueue>
+brdc_status graph_call(brdc_handle h, SolveGraph &g, SolveSig sig, Enqueue enqueue,
+                       bool *done) {
     *done = false;
-    SolveGraph &g = h->g;
+    h->replayed = false;
+    if (!h->graphs || h->timing) {
+        return BRDC_STATUS_SUCCESS;
+    }
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     if (cudaStreamIsCapturing(h->stream, &cs) != cudaSuccess) {
         cudaGetLastError();
@@ -912,13 +920,6 @@ brdc_status solve_graph(brdc_handle h, const HostForest &hf, const Layout &L, co
     if (cs != cudaStreamCaptureStatusNone) {
         return BRDC_STATUS_SUCCESS;
     }
-    SolveSig sig;
-    sig.n = hf.total_n;
-    sig.D = D;
-    sig.E = E;
-    sig.W = W;
-    sig.ws = ws;
-    sig.ws_size = ws_size;
     sig.sub_levels = h->sub_levels;
     sig.defl_cluster = h->defl_cluster;
     sig.lanes_target = h->lanes_target;
@@ -926,7 +927,7 @@ brdc_status solve_graph(brdc_handle h, const HostForest &hf, const Layout &L, co
     sig.max_iter = h->max_iter;
     sig.wait_ns = h->wait_ns;
     if (!(g.seen_valid && g.seen == sig)) {
-        drop_graph(h);
+        drop_graph(g);
         g.seen = sig;
         g.seen_valid = true;
         g.failed = false;
@@ -935,7 +936,7 @@ brdc_status solve_graph(brdc_handle h, const HostForest &hf, const Layout &L, co
     if (g.failed) {
         return BRDC_STATUS_SUCCESS;
     }
-    if (g.exec == nullptr && !capture_graph(h, hf, L, F, w, D, E, W)) {
+    if (g.exec == nullptr && !capture_graph(h, g, enqueue)) {
         g.failed = true;
         return BRDC_STATUS_SUCCESS;
     }
@@ -946,23 +947,27 @@ brdc_status solve_graph(brdc_handle h, const HostForest &hf, const Layout &L, co
     h->timed_levels = g.timed_levels;
     std::copy(g.has_lowner, g.has_lowner + BRDC_MAX_LEVELS, h->has_lowner);
     BRDC_CUDA(h, "brdc.graph_launch", cudaGraphLaunch(g.exec, h->stream));
-    g.replayed = true;
+    h->replayed = true;
     return BRDC_STATUS_SUCCESS;
 }
 
-// brdc_dstebr after its checks: a graph replay where solve_graph takes the
+// brdc_dstebr after its checks: a graph replay where graph_call takes the
 // call, else the stream launches.
 brdc_status plain_solve(brdc_handle h, const HostForest &hf, const Layout &L, const Forest &F,
                         const Ws &w, const double *D, const double *E, double *W, void *ws,
-                        size_t ws_size, bool ckpt) {
-    if (!ckpt && h->graphs && !h->timing) {
-        bool done = false;
-        const brdc_status st = solve_graph(h, hf, L, F, w, D, E, W, ws, ws_size, &done);
-        if (done) {
-            return st;
-        }
-    }
-    return run_forest(h, hf, L, F, w, D, E, W);
+                        size_t ws_size) {
+    SolveSig sig;
+    sig.kind = 0;
+    sig.n = hf.total_n;
+    sig.D = D;
+    sig.E = E;
+    sig.W = W;
+    sig.ws = ws;
+    sig.ws_size = ws_size;
+    auto enqueue = [&]() { return run_forest(h, hf, L, F, w, D, E, W); };
+    bool done = false;
+    const brdc_status st = graph_call(h, h->gf, sig, enqueue, &done);
+    return done ? st : enqueue();
 }
 
 } // namespace
@@ -1006,9 +1011,10 @@ extern "C" brdc_status brdc_destroy(brdc_handle h) {
     if (h->prep_ev != nullptr) {
         cudaEventDestroy(h->prep_ev);
     }
-    drop_graph(h);
-    if (h->g.cap != nullptr) {
-        cudaStreamDestroy(h->g.cap);
+    drop_graph(h->gf);
+    drop_graph(h->gb);
+    if (h->gcap != nullptr) {
+        cudaStreamDestroy(h->gcap);
     }
     if (h->own_stream != nullptr) {
         cudaStreamDestroy(h->own_stream);
@@ -1181,7 +1187,7 @@ extern "C" brdc_status brdc_dstebr(brdc_handle h, int64_t n, const double *d_D,
     F.max_levels = hf.max_levels;
     F.n0 = n;
     F.L0 = hf.max_levels;
-    return plain_solve(h, hf, L, F, w, d_D, d_E, d_W, workspace, workspace_size, ckpt);
+    return plain_solve(h, hf, L, F, w, d_D, d_E, d_W, workspace, workspace_size);
 }
 
 namespace {
@@ -1282,8 +1288,7 @@ extern "C" brdc_status brdc_dstebr_host(brdc_handle h, int64_t n, const double *
                                       h->stream));
         }
     }
-    const brdc_status st = plain_solve(h, hf, L, F, w, dD, dE, dW, workspace, workspace_size,
-                                       false);
+    const brdc_status st = plain_solve(h, hf, L, F, w, dD, dE, dW, workspace, workspace_size);
     if (st != BRDC_STATUS_SUCCESS) {
         return st;
     }
@@ -1467,8 +1472,10 @@ extern "C" brdc_status brdc_set_graphs(brdc_handle h, int enable) {
     }
     h->graphs = enable ? 1 : 0;
     if (!h->graphs) {
-        drop_graph(h);
-        h->g.seen_valid = false;
+        for (SolveGraph *g : {&h->gf, &h->gb}) {
+            drop_graph(*g);
+            g->seen_valid = false;
+        }
     }
     return BRDC_STATUS_SUCCESS;
 }
@@ -1481,7 +1488,7 @@ extern "C" brdc_status brdc_get_last_launches(brdc_handle h, int *launches, int 
         return BRDC_STATUS_INVALID_POINTER;
     }
     if (replayed != nullptr) {
-        *replayed = h->g.replayed ? 1 : 0;
+        *replayed = h->replayed ? 1 : 0;
     }
     *launches = h->launches;
     return BRDC_STATUS_SUCCESS;
@@ -1973,13 +1980,29 @@ extern "C" brdc_status brdc_dstebr_backward(brdc_handle h, int64_t n,
     F.max_levels = hf.max_levels;
     F.n0 = n;
     F.L0 = hf.max_levels;
-    if (!keep_forward) {
-        const brdc_status st = run_forest(h, hf, L, F, w, d_D, d_E, w.wtmp);
-        if (st != BRDC_STATUS_SUCCESS) {
-            return st;
+    auto enqueue = [&]() {
+        if (!keep_forward) {
+            const brdc_status st = run_forest(h, hf, L, F, w, d_D, d_E, w.wtmp);
+            if (st != BRDC_STATUS_SUCCESS) {
+                return st;
+            }
         }
-    }
-    return run_backward(h, hf, L, F, w, d_D, d_E, d_G, d_gD, d_gE);
+        return run_backward(h, hf, L, F, w, d_D, d_E, d_G, d_gD, d_gE);
+    };
+    SolveSig sig;
+    sig.kind = 1;
+    sig.n = n;
+    sig.D = d_D;
+    sig.E = d_E;
+    sig.ws = workspace;
+    sig.ws_size = workspace_size;
+    sig.G = d_G;
+    sig.gD = d_gD;
+    sig.gE = d_gE;
+    sig.keep_forward = keep_forward ? 1 : 0;
+    bool done = false;
+    const brdc_status st = graph_call(h, h->gb, sig, enqueue, &done);
+    return done ? st : enqueue();
 }
 
 extern "C" brdc_status brdc_dstebr_batched_backward(brdc_handle h, int64_t count,

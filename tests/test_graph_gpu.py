@@ -267,3 +267,48 @@ def test_replay_small_orders(n):
             assert np.array_equal(W.cpu().numpy(), ref)
     finally:
         s.close()
+
+
+@pytest.mark.parametrize("keep_forward", [True, False])
+def test_adjoint_replay_matches_ordinary_launches(keep_forward):
+    """A loop of checkpointing forward and adjoint: both replay their graphs
+    from the second step on, with gradients bit for bit those of stream
+    launches."""
+    import brdc
+    import torch
+
+    n = 16384
+    d, e = families.generate("normal", n)
+    g = np.random.default_rng(5).standard_normal(n)
+    s = brdc.Solver()
+    try:
+        D, E, W = buffers(d, e)
+        G = torch.tensor(g, device="cuda")
+        gD = torch.empty(n, dtype=torch.float64, device="cuda")
+        gE = torch.empty(n, dtype=torch.float64, device="cuda")
+        wsc = s.new_checkpoint_workspace(n)
+
+        def step():
+            if keep_forward:
+                s.dstebr(D, E, W=W, workspace=wsc)
+                fwd = s.last_launches()["replayed"]
+            else:
+                fwd = None
+            s.dstebr_backward(D, E, G, workspace=wsc, keep_forward=keep_forward, gD=gD, gE=gE)
+            return fwd, s.last_launches()["replayed"]
+
+        s.set_graphs(False)
+        step()
+        ref = (gD.cpu().numpy().copy(), gE.cpu().numpy()[: n - 1].copy())
+        s.set_graphs(True)
+        for i in range(4):
+            gD.fill_(0.0)
+            gE.fill_(0.0)
+            fwd, bwd = step()
+            assert bwd == (i >= 1)
+            if keep_forward:
+                assert fwd == (i >= 1)
+            assert np.array_equal(gD.cpu().numpy(), ref[0])
+            assert np.array_equal(gE.cpu().numpy()[: n - 1], ref[1])
+    finally:
+        s.close()
