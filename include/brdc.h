@@ -329,10 +329,13 @@ brdc_status brdc_get_last_launches(brdc_handle handle, int *launches, int *repla
  * memory, through device images of D, E and W kept in the caller's
  * workspace after the solve's own (brdc_dstebr_host_workspace_size; the
  * workspace takes no checkpoints).  Same checks and statuses as
- * brdc_dstebr.  The copies in (one when E lies right after D in one host
- * buffer, h_E == h_D + n; else two), the solve and the copy out are
- * enqueued on the handle's stream; W is valid once the stream has
- * synchronised.  With
+ * brdc_dstebr.  Page-locked D and E are read by the solve's first kernel
+ * through their device addresses (it writes the device images as it takes
+ * the norm); others are copied in first (one copy when E lies right after
+ * D in one host buffer, h_E == h_D + n; else two).  A page-locked W is
+ * written by the solve itself through its device address, any other W by
+ * a copy out after it.  Everything is enqueued on the handle's stream; W
+ * is valid once the stream has synchronised.  With
  * page-locked buffers (cudaMallocHost, cudaHostAlloc, cudaHostRegister)
  * the call does not block the host; pageable buffers are staged by the
  * runtime, which blocks it.  The solve itself is brdc_dstebr's on the

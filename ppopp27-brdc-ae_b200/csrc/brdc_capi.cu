@@ -36,6 +36,7 @@ struct SolveSig {
     double *W = nullptr;
     void *ws = nullptr;
     size_t ws_size = 0;
+    const double *srcD = nullptr, *srcE = nullptr; // host entry: mapped D, E
     const double *G = nullptr; // adjoint: G, gD, gE and keep_forward
     double *gD = nullptr, *gE = nullptr;
     int keep_forward = 0;
@@ -43,7 +44,8 @@ struct SolveSig {
     unsigned long long wait_ns = 0;
     bool operator==(const SolveSig &o) const {
         return kind == o.kind && n == o.n && D == o.D && E == o.E && W == o.W && ws == o.ws &&
-               ws_size == o.ws_size && G == o.G && gD == o.gD && gE == o.gE &&
+               ws_size == o.ws_size && srcD == o.srcD && srcE == o.srcE && G == o.G &&
+               gD == o.gD && gE == o.gE &&
                keep_forward == o.keep_forward && sub_levels == o.sub_levels &&
                defl_cluster == o.defl_cluster && lanes_target == o.lanes_target &&
                lvl_rows == o.lvl_rows && max_iter == o.max_iter && wait_ns == o.wait_ns;
@@ -662,7 +664,8 @@ int launch_level_fused(brdc_handle h, const HostForest &hf, const KArgs &a0, boo
 // Enqueue the whole forward solve.
 brdc_status run_forest(brdc_handle h, const HostForest &hf, const Layout &L,
                        const Forest &F, const Ws &w, const double *D,
-                       const double *E, double *W) {
+                       const double *E, double *W, const double *srcD = nullptr,
+                       const double *srcE = nullptr) {
     cudaStream_t s = h->stream;
     BRDC_CUDA(h, "brdc.set_attributes", set_attrs());
     h->replayed = false;
@@ -678,7 +681,9 @@ brdc_status run_forest(brdc_handle h, const HostForest &hf, const Layout &L,
         ng = std::max<long long>(1, std::min<long long>(ng, (long long)h->sm_count * 4));
         cudaLaunchAttribute at[1];
         cudaLaunchConfig_t cfg = plain_config((unsigned)ng, 256, 0, s, at);
-        cudaLaunchKernelEx(&cfg, k_norm, F, D, E, w.f_norm, w.hdr);
+        cudaLaunchKernelEx(&cfg, k_norm, F, srcD ? srcD : D, srcD ? srcE : E, w.f_norm, w.hdr,
+                           srcD ? const_cast<double *>(D) : (double *)nullptr,
+                           srcD ? const_cast<double *>(E) : (double *)nullptr);
         BRDC_CUDA(h, "brdc.norm", cudaGetLastError());
     }
     h->launches += 2;
@@ -955,7 +960,8 @@ brdc_status graph_call(brdc_handle h, SolveGraph &g, SolveSig sig, Enqueue enque
 // call, else the stream launches.
 brdc_status plain_solve(brdc_handle h, const HostForest &hf, const Layout &L, const Forest &F,
                         const Ws &w, const double *D, const double *E, double *W, void *ws,
-                        size_t ws_size) {
+                        size_t ws_size, const double *srcD = nullptr,
+                        const double *srcE = nullptr) {
     SolveSig sig;
     sig.kind = 0;
     sig.n = hf.total_n;
@@ -964,7 +970,9 @@ brdc_status plain_solve(brdc_handle h, const HostForest &hf, const Layout &L, co
     sig.W = W;
     sig.ws = ws;
     sig.ws_size = ws_size;
-    auto enqueue = [&]() { return run_forest(h, hf, L, F, w, D, E, W); };
+    sig.srcD = srcD;
+    sig.srcE = srcE;
+    auto enqueue = [&]() { return run_forest(h, hf, L, F, w, D, E, W, srcD, srcE); };
     bool done = false;
     const brdc_status st = graph_call(h, h->gf, sig, enqueue, &done);
     return done ? st : enqueue();
@@ -1258,38 +1266,64 @@ extern "C" brdc_status brdc_dstebr_host(brdc_handle h, int64_t n, const double *
     F.max_levels = hf.max_levels;
     F.n0 = n;
     F.L0 = hf.max_levels;
-    // stream copies around the device entry's solve (a graph replay from
-    // the second call with this workspace on)
-    // E right after D in the caller's memory: one copy of [D | E].  Two
-    // separate page-locked allocations can also lie back to back, and the
-    // runtime refuses a copy across them (an error it returns at once, with
-    // nothing enqueued): then the two copies below.  Inside the caller's
-    // stream capture a refused call would end the capture, so there the
-    // copies are always two.
-    bool joint = false;
-    if (n > 1 && h_E == h_D + n) {
-        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusActive;
-        if (cudaStreamIsCapturing(h->stream, &cs) == cudaSuccess &&
-            cs == cudaStreamCaptureStatusNone) {
-            joint = cudaMemcpyAsync(dD, h_D, sizeof(double) * (2 * n - 1),
-                                    cudaMemcpyHostToDevice, h->stream) == cudaSuccess;
+    // Page-locked D and E: k_norm reads them through their device addresses
+    // and writes the device images as it takes the norm, so no copy in
+    // precedes the solve (on B200, against the copies below: uniform 16,384
+    // end to end 0.479 -> 0.473 ms, normal 65,536 0.678 -> 0.674 ms).
+    // Otherwise the copies in on the stream.  Then the device entry's solve,
+    // a graph replay from the second call with these buffers on.
+    void *mD = nullptr, *mE = nullptr;
+    if (cudaHostGetDevicePointer(&mD, const_cast<double *>(h_D), 0) != cudaSuccess ||
+        (n > 1 && cudaHostGetDevicePointer(&mE, const_cast<double *>(h_E), 0) != cudaSuccess)) {
+        cudaGetLastError();
+        mD = mE = nullptr;
+    }
+    if (mD == nullptr) {
+        // E right after D in the caller's memory: one copy of [D | E].  Two
+        // separate page-locked allocations can also lie back to back, and the
+        // runtime refuses a copy across them (an error it returns at once, with
+        // nothing enqueued): then the two copies below.  Inside the caller's
+        // stream capture a refused call would end the capture, so there the
+        // copies are always two.
+        bool joint = false;
+        if (n > 1 && h_E == h_D + n) {
+            cudaStreamCaptureStatus cs = cudaStreamCaptureStatusActive;
+            if (cudaStreamIsCapturing(h->stream, &cs) == cudaSuccess &&
+                cs == cudaStreamCaptureStatusNone) {
+                joint = cudaMemcpyAsync(dD, h_D, sizeof(double) * (2 * n - 1),
+                                        cudaMemcpyHostToDevice, h->stream) == cudaSuccess;
+            }
+            if (!joint) {
+                cudaGetLastError();
+            }
         }
         if (!joint) {
-            cudaGetLastError();
-        }
-    }
-    if (!joint) {
-        BRDC_CUDA(h, "brdc.host.copy_d",
-                  cudaMemcpyAsync(dD, h_D, sizeof(double) * n, cudaMemcpyHostToDevice,
-                                  h->stream));
-        if (n > 1) {
-            BRDC_CUDA(h, "brdc.host.copy_e",
-                      cudaMemcpyAsync(dE, h_E, sizeof(double) * (n - 1), cudaMemcpyHostToDevice,
+            BRDC_CUDA(h, "brdc.host.copy_d",
+                      cudaMemcpyAsync(dD, h_D, sizeof(double) * n, cudaMemcpyHostToDevice,
                                       h->stream));
+            if (n > 1) {
+                BRDC_CUDA(h, "brdc.host.copy_e",
+                          cudaMemcpyAsync(dE, h_E, sizeof(double) * (n - 1), cudaMemcpyHostToDevice,
+                                          h->stream));
+            }
         }
     }
-    const brdc_status st = plain_solve(h, hf, L, F, w, dD, dE, dW, workspace, workspace_size);
-    if (st != BRDC_STATUS_SUCCESS) {
+    // W page-locked: the solve stores the eigenvalues through W's device
+    // address straight into host memory as its last level places them, so
+    // no copy out follows the solve (on B200, uniform 65,536 end to end
+    // 0.776 -> 0.753 ms, 16,384 0.483 -> 0.477 ms, the medians of three
+    // processes).  Otherwise they land in the device image and are copied.
+    void *mW = nullptr;
+    if (cudaHostGetDevicePointer(&mW, h_W, 0) != cudaSuccess) {
+        cudaGetLastError();
+        mW = nullptr;
+    }
+    double *Wd = mW != nullptr ? static_cast<double *>(mW) : dW;
+    const double *sD = mD != nullptr ? static_cast<const double *>(mD) : nullptr;
+    const double *sE = mD != nullptr ? (n > 1 ? static_cast<const double *>(mE) : sD) : nullptr;
+    const brdc_status st = plain_solve(h, hf, L, F, w, dD, dE, Wd, workspace, workspace_size,
+                                       sD, sE);
+    if (st != BRDC_STATUS_SUCCESS || mW != nullptr) {
         return st;
     }
     BRDC_CUDA(h, "brdc.host.copy_w",

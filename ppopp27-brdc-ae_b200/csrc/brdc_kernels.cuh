@@ -2087,11 +2087,14 @@ __global__ void __launch_bounds__(kSweepThreads)
 // Max-norm max(|D|, |E|) of every instance, as the bits of a non-negative
 // double (which order like the integers): grid-wide with one
 // atomic per block for a single matrix, one warp per instance for a batch.
+// For a single matrix read from host memory (brdc_dstebr_host), cD and cE
+// receive the device images of D and E that the rest of the solve reads.
 // A NaN or an infinity anywhere in D or E (the ignored E slot at the end
 // of each instance excepted) sets kErrNonFinite: nothing after k_norm runs,
 // and brdc_get_info reports it.  (fmax would drop a NaN silently.)
 __global__ void __launch_bounds__(256) k_norm(Forest F, const double *D, const double *E,
-                                              long long *out, WsHeader *h) {
+                                              long long *out, WsHeader *h, double *cD,
+                                              double *cE) {
     pdl_begin();
     const int lane = threadIdx.x & 31;
     bool bad = false;
@@ -2100,11 +2103,19 @@ __global__ void __launch_bounds__(256) k_norm(Forest F, const double *D, const d
         double mx = 0.0;
         for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
              i += (long long)gridDim.x * blockDim.x) {
-            const double dv = fabs(D[i]);
+            const double dr = D[i];
+            if (cD != nullptr) {
+                cD[i] = dr;
+            }
+            const double dv = fabs(dr);
             bad |= !(dv <= DBL_MAX);
             mx = fmax(mx, dv);
             if (i + 1 < n) {
-                const double ev = fabs(E[i]);
+                const double er = E[i];
+                if (cE != nullptr) {
+                    cE[i] = er;
+                }
+                const double ev = fabs(er);
                 bad |= !(ev <= DBL_MAX);
                 mx = fmax(mx, ev);
             }
