@@ -112,19 +112,43 @@ def stop_clock_sampler(proc, path, device_index):
             "samples": len(sm)}
 
 
+class quiet_host:
+    """The events of a timed loop made beforehand, and Python's garbage
+    collector paused while it runs: every timed interval opens with an
+    event and then waits for the host to submit the work, so a collection
+    pass or an allocation on the host would be timed as solve time."""
+
+    def __init__(self, torch, steps):
+        self.ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                   for _ in range(steps)]
+
+    def __enter__(self):
+        import gc
+
+        self.was = gc.isenabled()
+        gc.disable()
+        return self.ev
+
+    def __exit__(self, *exc):
+        import gc
+
+        if self.was:
+            gc.enable()
+        return False
+
+
 def time_solves(torch, solver, D, E, W, ws, steps, flush):
     """Per-solve device times (ms) with an L2 flush before each solve."""
     stream = torch.cuda.current_stream()
     times = []
-    for _ in range(steps):
-        flush.zero_()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        solver.dstebr(D, E, W=W, workspace=ws)
-        e1.record(stream)
-        e1.synchronize()
-        times.append(e0.elapsed_time(e1))
+    with quiet_host(torch, steps) as ev:
+        for e0, e1 in ev:
+            flush.zero_()
+            e0.record(stream)
+            solver.dstebr(D, E, W=W, workspace=ws)
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
     return times
 
 
@@ -459,35 +483,33 @@ def measure_e2e(torch, solver, D, E, W, ws, d, e, flush, warmup, steps):
     argv = (solver.h, n, ctypes.c_void_p(hD.data_ptr()), ctypes.c_void_p(hE.data_ptr()),
             ctypes.c_void_p(hW.data_ptr()), ctypes.c_void_p(hws.data_ptr()), hws.numel())
     e2e = []
-    for i in range(warmup + steps):
-        flush.zero_()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        st = call(*argv)
-        e1.record(stream)
-        e1.synchronize()
-        if st != 0:
-            raise RuntimeError(f"brdc_dstebr_host returned {st}")
-        if i >= warmup:
-            e2e.append(e0.elapsed_time(e1))
+    with quiet_host(torch, warmup + steps) as ev:
+        for i, (e0, e1) in enumerate(ev):
+            flush.zero_()
+            e0.record(stream)
+            st = call(*argv)
+            e1.record(stream)
+            e1.synchronize()
+            if st != 0:
+                raise RuntimeError(f"brdc_dstebr_host returned {st}")
+            if i >= warmup:
+                e2e.append(e0.elapsed_time(e1))
     err = float(np.max(np.abs(hW.numpy() - ref)))
     # the same through the device entry, the copies made by the caller
     DE = torch.empty(n + len(e), dtype=torch.float64, device=D.device)
     Dv, Ev = DE[:n], DE[n:]
     dev = []
-    for i in range(warmup + steps):
-        flush.zero_()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        DE.copy_(hDE, non_blocking=True)
-        solver.dstebr(Dv, Ev, W=W, workspace=ws)
-        hW.copy_(W, non_blocking=True)
-        e1.record(stream)
-        e1.synchronize()
-        if i >= warmup:
-            dev.append(e0.elapsed_time(e1))
+    with quiet_host(torch, warmup + steps) as ev:
+        for i, (e0, e1) in enumerate(ev):
+            flush.zero_()
+            e0.record(stream)
+            DE.copy_(hDE, non_blocking=True)
+            solver.dstebr(Dv, Ev, W=W, workspace=ws)
+            hW.copy_(W, non_blocking=True)
+            e1.record(stream)
+            e1.synchronize()
+            if i >= warmup:
+                dev.append(e0.elapsed_time(e1))
     return {"value": float(np.mean(e2e)), "unit": "ms",
             "h2d_bytes_per_step": int((hD.numel() + hE.numel()) * 8),
             "d2h_bytes_per_step": int(hW.numel() * 8),
