@@ -1760,6 +1760,10 @@ __device__ bool sweep_lowner(const KArgs &a, int cta_blocks, double *smem, uint6
         const bool ok = tiles_sweep<3>(ts, [&](int j0, int cnt, double *const *b) {
             if (active) {
                 int jj = lane;
+                // unrolled so that the next pair's shared-memory loads issue
+                // under this pair's product (Toeplitz 65,536: 21.03 ->
+                // 20.75 ms with the rows loop below, the same bits)
+#pragma unroll 4
                 for (; jj + tpr < cnt; jj += 2 * tpr) {
                     const int j = j0 + jj, jj2 = jj + tpr;
                     const double dl = (di - b[0][jj]) - b[1][jj];
@@ -1887,6 +1891,7 @@ __device__ bool sweep_rows(const KArgs &a, int cta_blocks, double *smem, uint64_
         const bool ok = tiles_sweep<4>(ts, [&](int j0, int cnt, double *const *b) {
             if (root) {
                 int jj = lane;
+#pragma unroll 4
                 for (; jj + tpr < cnt; jj += 2 * tpr) {
                     const int jj2 = jj + tpr;
                     double u, u2;
