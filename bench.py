@@ -893,15 +893,14 @@ def collect_extras(torch, brdc, families, solver, D, E, W, ws, d, e, flush, args
 def _event_ms(torch, fn, reps, flush, stream=None):
     stream = stream or torch.cuda.current_stream()
     out = []
-    for _ in range(reps):
-        flush.zero_()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        fn()
-        e1.record(stream)
-        e1.synchronize()
-        out.append(e0.elapsed_time(e1))
+    with quiet_host(torch, reps) as ev:
+        for e0, e1 in ev:
+            flush.zero_()
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            out.append(e0.elapsed_time(e1))
     return float(np.mean(out))
 
 
@@ -934,14 +933,19 @@ def bench_fwd_bwd(torch, families, solver, flush, args):
             fwd_c()
             bwd()
 
-        for _ in range(3):
-            both()
-            fwd()
-        torch.cuda.synchronize()
-        reps = 10
-        t_f = _event_ms(torch, fwd, reps, flush)
-        t_fc = _event_ms(torch, fwd_c, reps, flush)
-        t_fb = _event_ms(torch, both, reps, flush)
+        reps = 20
+
+        def timed(fn):
+            # each pattern warmed right before its timing, so that the
+            # library captures its graphs (forward, adjoint) outside it
+            for _ in range(3):
+                fn()
+            torch.cuda.synchronize()
+            return _event_ms(torch, fn, reps, flush)
+
+        t_f = timed(fwd)
+        t_fc = timed(fwd_c)
+        t_fb = timed(both)
         res[str(n)] = {"fwd_ms": t_f, "fwd_checkpointed_ms": t_fc, "fwd_bwd_ms": t_fb,
                        "bwd_ms": t_fb - t_fc, "ratio_fwd_bwd_to_fwd": t_fb / t_f,
                        "workspace_bytes": ws.numel(), "checkpoint_workspace_bytes": wsc.numel()}
