@@ -232,9 +232,10 @@ def test_counts_differ_only_by_near_threshold_decisions(solver, ref, family, n):
     more than rounding; it is therefore run on the same matrix scaled by
     2^13 (exactly: every decision of its merges scales with it, its leaves
     become accurate to rounding).  The remaining differences come from the
-    rows' z mode (this build forms boundary rows from the Loewner weights,
-    the prototype's values path from the original z: SURVEY note N1) and
-    rounding, and every level's difference is bounded by this build's
+    rows' z mode (this build forms boundary rows from the Loewner weights;
+    the prototype's values path reads the unrescaled z when it forms them,
+    gpu/src/tridiag_solver.cu:1660-1664 and merge_kernels.cuh:1215,1229,
+    so its Loewner result is unused) and rounding, and every level's difference is bounded by this build's
     decisions within a factor 4 of tol."""
     import torch
 
