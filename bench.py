@@ -513,7 +513,9 @@ def measure_e2e(torch, solver, D, E, W, ws, d, e, flush, warmup, steps):
     return {"value": float(np.mean(e2e)), "unit": "ms",
             "h2d_bytes_per_step": int((hD.numel() + hE.numel()) * 8),
             "d2h_bytes_per_step": int(hW.numel() * 8),
-            "entry": "brdc_dstebr_host (pinned host buffers)",
+            "entry": ("brdc_dstebr_host on pinned host buffers: k_norm reads D and E and the "
+                      "top level writes W through their mapped addresses, over PCIe inside "
+                      "the timed interval"),
             "max_abs_diff_vs_device_entry": err,
             "device_entry_with_caller_copies_ms": float(np.mean(dev))}
 
